@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""op_H throughput of the B200 path on the Si64 microbenchmark.
+
+Workload (the op_H + LOBPCG microbenchmark configuration): Si 64-atom cubic
+supercell (2x2x2 conventional diamond cells, a = 20.5262 bohr), Gamma only,
+GTH-Pade Si-q4, ecutwfc = 15 Ha -> 75^3 grid (the reference's grid rule),
+Ngw = 23,871, 160 bands, NbetaNL = 320.  psi: seeded complex Gaussian,
+Cholesky-orthonormalised; V_loc = V_Ps_loc + a seeded smooth random field
+(|G|^2 <= 4, max 0.01 Ha).  Synthetic inputs, generated here.
+
+One step = one full op_H (K + V_loc + V_Ps_nloc) over all 160 bands.
+  value        mixed precision (complex64, FP32 FFTs) op_H, inputs resident
+               in HBM, device time (CUDA events), L2 flushed between steps
+  e2e          the reference-facing host call pw_op_H_host on pinned host
+               ComplexF64 arrays: H2D copy + op_H + D2H copy every step
+  fp64_*       the same step on the FP64 path (complex128)
+  roofline     the pruned-FFT op_V_loc round trip (K-zinv + K-plane + K-zfwd),
+               timed alone, against the HBM copy peak
+Unit: GB/s of algorithmic bytes, the FP32 byte model of the op_V_loc round
+trip, c*(3*Ngw + 4*P) + 4*N/Nb per band with c = 8 B and P = Nx_active*N2*N3,
+applied to every arm so that ratios between arms are throughput ratios.
+
+--impl reference times the reference algorithm on the host CPU: the FP64
+NumPy/SciPy restatement of PWDFT.jl's op_H (the Julia reference cannot run
+in this image), all host threads, a bounded sample of bands per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "pwdft.jl_b200")
+for p in (ROOT, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import numpy as np
+
+METRIC = "SCF time-to-1e-6 Ha/atom & op_H GB/s: mixed-prec batched vs FP64 on 1 B200"
+A_SI = 10.2631
+NBANDS = 160
+SEED = 20261203
+PSP = os.path.join(ROOT, "tests", "golden", "psp", "Si-q4.gth")
+DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                    [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def si64_geometry():
+    frac = np.array([(b + np.array([i, j, k])) / 2.0 for i in range(2) for j in range(2) for k in range(2)
+                     for b in DIAMOND]).T
+    LL = 2 * A_SI * np.eye(3)
+    return LL, LL @ frac
+
+
+def smooth_field(Ns, G2, idx_g2r, rng):
+    """Seeded random field with Fourier components only at |G|^2 <= 4,
+    normalised to max |dV| = 1 (G2, idx_g2r: the density sphere)."""
+    N1, N2, N3 = Ns
+    sel = G2 <= 4.0
+    c = np.zeros(N1 * N2 * N3, dtype=np.complex128)
+    c[idx_g2r[sel]] = rng.standard_normal(sel.sum()) + 1j * rng.standard_normal(sel.sum())
+    f = np.fft.ifftn(c.reshape(N3, N2, N1)).real.ravel()
+    return f / np.abs(f).max()
+
+
+def orthonormal_psi(ngw, nb, rng):
+    psi = rng.standard_normal((ngw, nb)) + 1j * rng.standard_normal((ngw, nb))
+    L = np.linalg.cholesky(psi.conj().T @ psi)
+    return np.linalg.solve(L.conj(), psi.T).T  # psi * inv(L^H)
+
+
+def byte_model(Ns, idx_gw2r, nb):
+    """Algorithmic bytes per band of the op_V_loc round trip, FP32 (c = 8)."""
+    N1, N2, N3 = Ns
+    nxa = len(np.unique(np.asarray(idx_gw2r) % N1))
+    P = nxa * N2 * N3
+    return 8 * (3 * len(idx_gw2r) + 4 * P) + 4 * N1 * N2 * N3 / nb, nxa
+
+
+def peaks():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[0]) for r in self.rows if num(r[0]) is not None]
+        mx = [num(r[1]) for r in self.rows if num(r[1]) is not None]
+        busy = [num(r[0]) for r in self.rows if num(r[6]) is not None and num(r[6]) > 0]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[2 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(busy or sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def build_workload(device):
+    import pwb200
+    LL, pos = si64_geometry()
+    sysm = pwb200.System(["Si"] * pos.shape[1], pos, LL)
+    H = pwb200.Hamiltonian(sysm, [PSP], 15.0, device=device)
+    rng = np.random.default_rng(SEED)
+    b = H.basis
+    H.update_vloc(H.V_Ps_loc + 0.01 * smooth_field(b.Ns, b.G2, b.idx_g2r, rng))
+    psi = orthonormal_psi(H.basis.Ngw[0], NBANDS, rng)
+    return H, psi
+
+
+def time_device(ctx, x, y, ops, steps, warmup, flush):
+    import torch
+    for _ in range(warmup):
+        ctx.apply(0, 0, x, y, ops)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    stream = torch.cuda.current_stream()
+    for s, e in ev:
+        flush.add_(1)               # write 256 MB: evicts L2 between steps (untimed)
+        s.record(stream)
+        ctx.apply(0, 0, x, y, ops)
+        e.record(stream)
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in ev]
+
+
+def cpu_reference(psi, steps, warmup, budget_s):
+    """The FP64 oracle op_H on the host cores: bounded band sample per step."""
+    from oracle import systems, ops
+    H = systems.Ham_Si64(Nstates=NBANDS)
+    rng = np.random.default_rng(SEED)
+    # same V_loc as the device arm: V_Ps_loc + the same seeded smooth field
+    g = H.pw.gvec
+    H.V_Total = H.V_Ps_loc + 0.01 * smooth_field(H.pw.Ns, g.G2, g.idx_g2r, rng)
+    nsamp = 16
+    x = psi[:, :nsamp].copy()
+    ops.op_H(H, x, 0)  # warm FFT plans
+    t0 = time.perf_counter()
+    ops.op_H(H, x, 0)
+    t_one = time.perf_counter() - t0
+    reps = max(1, min(steps, int(budget_s / max(t_one, 1e-3))))
+    for _ in range(min(warmup, 1)):
+        ops.op_H(H, x, 0)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ops.op_H(H, x, 0)
+    dt = (time.perf_counter() - t0) / reps
+    return dt, nsamp, reps
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rng = np.random.default_rng(SEED)
+        from oracle import pwgrid
+        LL, _ = si64_geometry()
+        pw = pwgrid.PWGrid(15.0, LL)
+        psi = orthonormal_psi(pw.gvecw.Ngw[0], NBANDS, np.random.default_rng(SEED + 1))
+        dt, nsamp, reps = cpu_reference(psi, args.steps, args.warmup, args.cpu_budget)
+        bpb, _ = byte_model(pw.Ns, pw.gvecw.idx_gw2r[0], NBANDS)
+        val = nsamp * bpb / dt / 1e9
+        out = {"impl": "reference", "metric": METRIC, "value": val, "unit": "GB/s", "n_gpus": args.gpus,
+               "steps": reps, "warmup": args.warmup, "ms_per_step": dt * 1e3 * NBANDS / nsamp,
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+               "data": "synthetic",
+               "config": {"workload": "Si64 Gamma op_H, 160 bands, 75^3 grid (CPU sample of %d bands)" % nsamp,
+                          "global_batch": NBANDS, "seq_len": 0, "parallelism": "cpu"},
+               "cpu_baseline": {"value": val, "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": "%d of 160 bands per step, %d steps" % (nsamp, reps)},
+               "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return
+
+    import torch
+    import pwb200
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    H, psi = build_workload(local)
+    ctx = H.ctx
+    bpb, nxa = byte_model(H.basis.Ns, H.basis.idx_gw2r[0], NBANDS)
+    step_bytes = bpb * NBANDS
+    x32 = torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{local}").to(torch.complex64).contiguous()
+    x64 = torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{local}").contiguous()
+    y32, y64 = torch.empty_like(x32), torch.empty_like(x64)
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    OPS = pwb200.PW_OP_H
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = ctx._L.pw_launch_count(ctx.h)
+    with ClockSampler(local) as clk:
+        t_mixed = time_device(ctx, x32, y32, OPS, args.steps, args.warmup, flush)
+    n1 = ctx._L.pw_launch_count(ctx.h)
+    launches = (n1 - n0) * args.steps // (args.steps + args.warmup)
+    t_fft = time_device(ctx, x32, y32, pwb200.PW_OP_VLOC, args.steps, args.warmup, flush)
+    t_fp64 = time_device(ctx, x64, y64, OPS, max(10, args.steps // 4), args.warmup, flush)
+    torch.cuda.synchronize()
+    ms = sum(t_mixed) / len(t_mixed)
+    ms_fft = sum(t_fft) / len(t_fft)
+    ms64 = sum(t_fp64) / len(t_fp64)
+    if dist:
+        t = torch.tensor([ms, ms_fft, ms64], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_fft, ms64 = [float(v) for v in t.tolist()]
+
+    # end to end through the host drop-in, pinned host buffers
+    pin_in = torch.from_numpy(np.ascontiguousarray(psi.T)).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    a_in = pin_in.numpy().T     # (Ngw, nb) Fortran view of the pinned buffer
+    a_out = pin_out.numpy().T
+    for _ in range(args.warmup):
+        ctx.op_H_host(0, 0, a_in, a_out, OPS, pwb200.PW_C64)
+    e2e_steps = max(5, args.steps // 10)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.op_H_host(0, 0, a_in, a_out, OPS, pwb200.PW_C64)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    hbm, peak_kind = peaks()
+    fft_gbs = step_bytes / (ms_fft * 1e-3) / 1e9
+    out = {
+        "metric": METRIC,
+        "value": world * step_bytes / (ms * 1e-3) / 1e9,
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "c64",
+        "data": "synthetic",
+        "config": {"workload": "Si64 Gamma op_H (K+V_loc+V_Ps_nloc), 160 bands, 75^3 grid, Ngw 23871, "
+                               "NbetaNL 320", "global_batch": NBANDS * world, "seq_len": 0,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed between steps (256 MB write)", "bytes_per_band": bpb, "nx_active": nxa},
+        "fp64_ms_per_step": ms64,
+        "fp64_value": world * step_bytes / (ms64 * 1e-3) / 1e9,
+        "gpu_launches": int(launches),
+        "e2e": {"value": world * step_bytes / e2e_s / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": int(psi.size * 16), "d2h_bytes_per_step": int(psi.size * 16),
+                "ms_per_step": e2e_s * 1e3},
+        "roofline": {"bound": "hbm", "achieved": fft_gbs, "peak": hbm, "unit": "GB/s", "frac": fft_gbs / hbm,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "op_V_loc pruned-FFT round trip (K-zinv+K-plane+K-zfwd), %.4f ms" % ms_fft},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and os.environ.get("PW_BENCH_NO_CPU") != "1":
+        dt, nsamp, reps = cpu_reference(psi, 1000, 1, args.cpu_budget)
+        v = nsamp * bpb / dt / 1e9
+        out["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": "%d of 160 bands per op_H, %d repetitions, FP64 NumPy/SciPy" % (nsamp, reps)}
+    if rank == 0:
+        print(json.dumps(out))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

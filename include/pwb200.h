@@ -1,0 +1,163 @@
+/*
+ * pwb200.h -- C ABI of libpwb200.so, the B200 (sm_100a) implementation of
+ * PWDFT.jl's Hamiltonian-application / density / eigensolver hot path.
+ *
+ * Every entry point returns an int status (PW_OK = 0); on failure the
+ * message is available from pw_last_error(ctx).  No torch, Julia or C++
+ * types cross this boundary: plain pointers, sizes and int flags only.
+ *
+ * Conventions shared with the reference (PWDFT.jl):
+ *   - wavefunctions are column-major (Ngw x Nstates) complex arrays, the
+ *     layout of Julia's Matrix{ComplexF64} (interleaved re, im);
+ *   - grid linear index ip = i + N1*(j + N2*k), x fastest (PWGrid.jl:212);
+ *   - G_to_R is the 1/N-normalised backward FFT, R_to_G the unnormalised
+ *     forward FFT (wrappers_fft.jl:42-62);
+ *   - op_* entry points ACCUMULATE into Hpsi when PW_ACCUMULATE is set
+ *     (the reference's op_K!/op_V_loc!/op_V_Ps_nloc! semantics), and
+ *     overwrite otherwise (op_H!, which zero-fills first, op_H.jl:53-63).
+ *
+ * Device entry points take device pointers and are ordered on the
+ * context's stream (pw_set_stream); host entry points (suffix _host) take
+ * host pointers to the reference's FP64 arrays and copy in and out.
+ */
+#ifndef PWB200_H
+#define PWB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PWB200_ABI_VERSION 1
+
+/* ---- status codes --------------------------------------------------- */
+#define PW_OK               0
+#define PW_ERR_ARG          1   /* invalid argument (size, index, pointer) */
+#define PW_ERR_CUDA         2   /* a CUDA runtime call failed */
+#define PW_ERR_NOMEM        3   /* device allocation failed */
+#define PW_ERR_NOT_POSDEF   4   /* Cholesky of an overlap matrix failed */
+#define PW_ERR_NAN          5   /* non-finite value in a reduction */
+#define PW_ERR_STATE        6   /* call out of order (e.g. no V_loc set) */
+#define PW_ERR_UNSUPPORTED  7   /* grid size with a prime factor > 5, ... */
+#define PW_ERR_TIMEOUT      8   /* a bounded device-side wait gave up */
+
+/* ---- element types of wavefunction buffers -------------------------- */
+#define PW_C128  0   /* ComplexF64: the reference's type (FP64 path)   */
+#define PW_C64   1   /* ComplexF32: mixed-precision path (FP32 FFTs)   */
+
+/* ---- operator selection for pw_apply / pw_op_H_host ----------------- */
+#define PW_OP_K        1u   /* op_K!        op_K.jl:44-75          */
+#define PW_OP_VLOC     2u   /* op_V_loc!    op_V_loc.jl:108-167    */
+#define PW_OP_VNL      4u   /* op_V_Ps_nloc! op_V_Ps_nloc.jl:39-78 */
+#define PW_OP_H        7u   /* op_H!        op_H.jl:53-63          */
+#define PW_ACCUMULATE  0x100u
+
+typedef struct pw_ctx pw_ctx;
+
+/* Basis description handed over once per Hamiltonian (PWGrid.gvecw). */
+typedef struct pw_grid_desc {
+    int32_t Ns[3];                  /* FFT grid (PWGrid.Ns)                     */
+    int32_t Nkpt;                   /* number of k-points                        */
+    int32_t Nspin;                  /* spin channels of V_loc (1 or 2)           */
+    int32_t index_base;             /* 1: idx_gw2r is Julia 1-based, 0: 0-based  */
+    double  CellVolume;             /* PWGrid.CellVolume (bohr^3)                */
+    const int64_t *Ngw;             /* [Nkpt]            GVectorsW.Ngw           */
+    const int64_t *const *idx_gw2r; /* [Nkpt][Ngw[k]]    GVectorsW.idx_gw2r      */
+    const double *const *Gk2;       /* [Nkpt][Ngw[k]]    |G+k|^2 (op_K.jl:70)    */
+} pw_grid_desc;
+
+/* ---- library and context -------------------------------------------- */
+int         pw_abi_version(void);
+
+/* Replaces the FFTW plans and index maps carried by PWGrid
+ * (PWGrid.jl:62-152): builds the pruned-FFT column tables on the host and
+ * uploads them to `device`. */
+int         pw_create(int device, const pw_grid_desc *desc, pw_ctx **out);
+void        pw_destroy(pw_ctx *ctx);
+const char *pw_last_error(const pw_ctx *ctx);
+int         pw_set_stream(pw_ctx *ctx, void *cuda_stream);   /* cudaStream_t */
+int         pw_synchronize(pw_ctx *ctx);
+/* Number of kernels this context has launched so far (for launch
+ * accounting in benchmarks; no counterpart in the reference). */
+int64_t     pw_launch_count(const pw_ctx *ctx);
+
+/* V_loc(r) = Ham.potentials.Total[:, ispin] (Hamiltonian.jl:542), host
+ * FP64, N x nspin column-major.  Replaces the potential read by
+ * op_V_loc.jl:127. */
+int pw_set_vloc(pw_ctx *ctx, const double *V, int nspin);
+int pw_set_vloc_device(pw_ctx *ctx, const double *V_dev, int nspin);
+
+/* betaNL[ik] (PsPotNL.jl:39-69): host ComplexF64 Ngw x nbeta column-major. */
+int pw_set_nonlocal(pw_ctx *ctx, int ik, const double *betaNL, int nbeta);
+/* The (ibeta, jbeta, h_ij) pairs visited by op_V_Ps_nloc.jl:59-76
+ * (0-based ibeta/jbeta; duplicates add). */
+int pw_set_nonlocal_coef(pw_ctx *ctx, int nnz, const int32_t *ibeta,
+                         const int32_t *jbeta, const double *hij);
+
+/* ---- device entry points (device pointers, context stream) ---------- */
+
+/* Hpsi (+)= H psi restricted to `ops` for k-point ik (0-based), spin
+ * ispin (0-based); psi/Hpsi are Ngw[ik] x nb with leading dimension ld.
+ * dtype PW_C128 computes in FP64, PW_C64 in FP32 (mixed precision).
+ * Replaces op_H!/op_K!/op_V_loc!/op_V_Ps_nloc! (op_H.jl:53-63). */
+int pw_apply(pw_ctx *ctx, int ik, int ispin, int dtype, const void *psi,
+             void *Hpsi, int64_t ld, int nb, unsigned ops);
+
+/* out = in / (1 + |G+k|^2)  (Kprec.jl:97-111; in == out allowed). */
+int pw_kprec(pw_ctx *ctx, int ik, int dtype, const void *in, void *out,
+             int64_t ld, int nb);
+
+/* rhoe[ip] (+)= sum_b w[b] |(N/sqrt(Omega)) G_to_R(psi_b)|^2
+ * (calc_rhoe.jl:51-78); w (host, nb) = wk[ik]*Focc[b, ikspin]; rhoe is a
+ * device FP64 array of N points (one spin channel).  accumulate = 0
+ * overwrites. */
+int pw_calc_rhoe(pw_ctx *ctx, int ik, int dtype, const void *psi, int64_t ld,
+                 int nb, const double *w, double *rhoe, int accumulate);
+
+/* Rayleigh-Ritz contractions (diag_LOBPCG.jl:85,144,152-153,183-184):
+ * C (m x n, device ComplexF64, ldc) (+)= A^H B, A is K x m, B is K x n,
+ * both of element type dtype. */
+int pw_gram(pw_ctx *ctx, int dtype, int64_t K, int m, int n, const void *A,
+            int64_t lda, const void *B, int64_t ldb, double *C, int64_t ldc,
+            int accumulate);
+/* C (M x n, dtype, ldc) (+)= A (M x k, dtype, lda) * U (k x n, device
+ * ComplexF64, ldu)  (diag_LOBPCG.jl:188-194). */
+int pw_rotate(pw_ctx *ctx, int dtype, int64_t M, int n, int k, const void *A,
+              int64_t lda, const double *U, int64_t ldu, void *C, int64_t ldc,
+              int accumulate);
+
+/* ---- host drop-ins (the reference's Julia arrays) ------------------- */
+
+/* op_H!(Ham, psi, Hpsi) and friends on host ComplexF64 arrays; compute
+ * precision chosen by dtype (PW_C128 = reference FP64, PW_C64 = mixed). */
+int pw_op_H_host(pw_ctx *ctx, int ik, int ispin, const double *psi,
+                 double *Hpsi, int64_t ld, int nb, unsigned ops, int dtype);
+/* calc_rhoe! inner loop for one k-point on host arrays; rhoe is host FP64
+ * (N), accumulated when accumulate != 0. */
+int pw_calc_rhoe_host(pw_ctx *ctx, int ik, const double *psi, int64_t ld,
+                      int nb, const double *w, double *rhoe, int accumulate,
+                      int dtype);
+
+/* ---- host-side basis construction (no device) ----------------------- */
+
+/* good_fft_order (fft_support.jl:48-72). */
+int pw_good_fft_order(int n);
+/* Number of G with 0.5|G|^2 <= ecutrho (PWGrid.jl:169-189); recvecs is
+ * the 3x3 RecVecs matrix in Julia column-major order. */
+int pw_gvec_count(const int32_t *Ns, const double *recvecs, double ecutrho,
+                  int64_t *Ng);
+/* init_gvec (PWGrid.jl:199-242): G (3 x Ng), G2, idx_g2r (0-based),
+ * sorted by a stable sort on G2, bit-identical to the reference. */
+int pw_gvec_build(const int32_t *Ns, const double *recvecs, double ecutrho,
+                  int64_t Ng, double *G, double *G2, int64_t *idx_g2r);
+/* init_gvecw for one k-point (PWGrid.jl:306-316): returns Ngw and fills
+ * idx_gw2g / idx_gw2r (0-based) and Gk2 (capacity Ng each). */
+int pw_gvecw_build(int64_t Ng, const double *G, const int64_t *idx_g2r,
+                   const double *kpt, double ecutwfc, int64_t *Ngw,
+                   int64_t *idx_gw2g, int64_t *idx_gw2r, double *Gk2);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PWB200_H */

@@ -1,0 +1,669 @@
+// Context, set-up and the C ABI of libpwb200.so (declared in include/pwb200.h).
+//
+// The context replaces what PWDFT.jl keeps in Ham.pw (FFTW plans, index
+// maps), Ham.potentials.Total and Ham.pspotNL for the operators; the
+// kernels themselves live in pw_fft_kernels.cu and pw_gemm.cu.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pwb200.h"
+#include "pw_launch.h"
+
+using namespace pwk;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+struct KData {
+    int Ngw = 0, Ncol = 0, Nxa = 0;
+    int *d_col_ptr = nullptr, *d_ent_igw = nullptr, *d_ent_kz = nullptr, *d_ent_col = nullptr;
+    int *d_col_ia = nullptr, *d_col_j = nullptr, *d_xa = nullptr;
+    double *d_Gk2 = nullptr;
+    float *d_Gk2f = nullptr;
+    double2 *d_beta64 = nullptr;
+    float2 *d_beta32 = nullptr;
+};
+
+constexpr int kMaxV64 = 8;  // complex values per thread per round in the FP64 FFT stages
+constexpr int kFftThreads = 256;
+
+bool make_plan(int n, FftDim &d) {
+    d.n = n;
+    d.nstage = 0;
+    int m = n;
+    const int radices[5] = {8, 4, 2, 3, 5};
+    for (int r : radices) {
+        while (m % r == 0) {
+            if (d.nstage >= 12) return false;
+            const int maxb = std::max(1, kMaxV64 / r);
+            if (n / r > kFftThreads * maxb) return false;
+            d.radix[d.nstage++] = r;
+            m /= r;
+        }
+    }
+    return m == 1;
+}
+
+}  // namespace
+
+struct pw_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    int N1 = 0, N2 = 0, N3 = 0;
+    size_t N = 0;
+    int Nkpt = 0, Nspin = 1;
+    double CellVolume = 0;
+    FftDim dx{}, dy{}, dz{};
+    double2 *tw64[3] = {nullptr, nullptr, nullptr};
+    float2 *tw32[3] = {nullptr, nullptr, nullptr};
+    std::vector<KData> k;
+    double *d_V64 = nullptr;
+    float *d_V32 = nullptr;
+    int vloc_nspin = 0;
+    int nbeta = 0;
+    int *d_Drow = nullptr, *d_Dcol = nullptr;
+    double *d_Dval = nullptr;
+    bool have_D = false;
+    DevBuf A, P, P2, gemm_ws, rho_part, w, st_in, st_out, st_in32, st_out32, st_rho;
+    std::vector<void *> allocs;
+    size_t a_chunk_bytes = 48ull << 20;
+    int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
+};
+
+namespace {
+
+int fail(pw_ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c)
+        c->err = buf;
+    else
+        g_create_error = buf;
+    return code;
+}
+
+#define CK(ctx, x)                                                                                    \
+    do {                                                                                              \
+        cudaError_t e_ = (x);                                                                         \
+        if (e_ != cudaSuccess) return fail(ctx, PW_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+int dalloc(pw_ctx *c, T **p, size_t n) {
+    void *q = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) return fail(c, PW_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    c->allocs.push_back(q);
+    *p = (T *)q;
+    return PW_OK;
+}
+
+template <typename T>
+int upload(pw_ctx *c, T **p, const std::vector<T> &v) {
+    int s = dalloc(c, p, v.size());
+    if (s) return s;
+    CK(c, cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PW_OK;
+}
+
+void dfree(pw_ctx *c, void *p) {
+    if (!p) return;
+    auto it = std::find(c->allocs.begin(), c->allocs.end(), p);
+    if (it != c->allocs.end()) c->allocs.erase(it);
+    cudaFree(p);
+}
+
+int ensure(pw_ctx *c, DevBuf &b, size_t bytes) {
+    if (b.bytes >= bytes) return PW_OK;
+    if (b.p) {
+        cudaStreamSynchronize(c->stream);
+        dfree(c, b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    void *q = nullptr;
+    int s = dalloc(c, (unsigned char **)&q, bytes);
+    if (s) return s;
+    b.p = q;
+    b.bytes = bytes;
+    return PW_OK;
+}
+
+int build_twiddles(pw_ctx *c, int n, int slot) {
+    std::vector<double2> t64(n);
+    std::vector<float2> t32(n);
+    for (int m = 0; m < n; ++m) {
+        const double a = -2.0 * M_PI * (double)m / (double)n;
+        t64[m] = make_double2(std::cos(a), std::sin(a));
+        t32[m] = make_float2((float)t64[m].x, (float)t64[m].y);
+    }
+    int s = upload(c, &c->tw64[slot], t64);
+    if (s) return s;
+    return upload(c, &c->tw32[slot], t32);
+}
+
+// Builds the pruned-FFT tables of one k-point from its sphere -> grid map.
+int build_kdata(pw_ctx *c, KData &kd, int64_t Ngw, const int64_t *idx, int base, const double *Gk2) {
+    const int N1 = c->N1, N2 = c->N2, N3 = c->N3;
+    const int64_t N = (int64_t)c->N;
+    if (Ngw <= 0 || Ngw > (int64_t)INT32_MAX) return fail(c, PW_ERR_ARG, "Ngw out of range: %lld", (long long)Ngw);
+    kd.Ngw = (int)Ngw;
+    std::vector<int> ent_i(Ngw), ent_j(Ngw), ent_k(Ngw);
+    std::vector<unsigned char> seen(N, 0);
+    for (int64_t g = 0; g < Ngw; ++g) {
+        const int64_t ip = idx[g] - base;
+        if (ip < 0 || ip >= N) return fail(c, PW_ERR_ARG, "idx_gw2r[%lld] = %lld outside the grid", (long long)g, (long long)idx[g]);
+        if (seen[ip]) return fail(c, PW_ERR_ARG, "idx_gw2r maps two G-vectors onto grid point %lld", (long long)ip);
+        seen[ip] = 1;
+        ent_i[g] = (int)(ip % N1);
+        ent_j[g] = (int)((ip / N1) % N2);
+        ent_k[g] = (int)(ip / ((int64_t)N1 * N2));
+    }
+    // active columns, x-major (all columns of one x are adjacent)
+    std::vector<int> colid((size_t)N1 * N2, -1);
+    for (int64_t g = 0; g < Ngw; ++g) colid[(size_t)ent_i[g] * N2 + ent_j[g]] = 0;
+    std::vector<int> col_i, col_j;
+    for (int i = 0; i < N1; ++i)
+        for (int j = 0; j < N2; ++j)
+            if (colid[(size_t)i * N2 + j] == 0) {
+                colid[(size_t)i * N2 + j] = (int)col_i.size();
+                col_i.push_back(i);
+                col_j.push_back(j);
+            }
+    const int Ncol = (int)col_i.size();
+    std::vector<int> col_ptr(Ncol + 1, 0);
+    std::vector<int> ecol(Ngw);
+    for (int64_t g = 0; g < Ngw; ++g) {
+        ecol[g] = colid[(size_t)ent_i[g] * N2 + ent_j[g]];
+        col_ptr[ecol[g] + 1]++;
+    }
+    for (int cc = 0; cc < Ncol; ++cc) col_ptr[cc + 1] += col_ptr[cc];
+    std::vector<int> order(Ngw);
+    for (int64_t g = 0; g < Ngw; ++g) order[g] = (int)g;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return ecol[a] != ecol[b] ? ecol[a] < ecol[b] : ent_k[a] < ent_k[b];
+    });
+    std::vector<int> e_igw(Ngw), e_kz(Ngw), e_col(Ngw);
+    for (int64_t e = 0; e < Ngw; ++e) {
+        e_igw[e] = order[e];
+        e_kz[e] = ent_k[order[e]];
+        e_col[e] = ecol[order[e]];
+    }
+    std::vector<int> xa, col_ia(Ncol);
+    for (int cc = 0; cc < Ncol; ++cc) {
+        if (xa.empty() || xa.back() != col_i[cc]) xa.push_back(col_i[cc]);
+        col_ia[cc] = (int)xa.size() - 1;
+    }
+    kd.Ncol = Ncol;
+    kd.Nxa = (int)xa.size();
+    int s;
+    if ((s = upload(c, &kd.d_col_ptr, col_ptr))) return s;
+    if ((s = upload(c, &kd.d_ent_igw, e_igw))) return s;
+    if ((s = upload(c, &kd.d_ent_kz, e_kz))) return s;
+    if ((s = upload(c, &kd.d_ent_col, e_col))) return s;
+    if ((s = upload(c, &kd.d_col_ia, col_ia))) return s;
+    if ((s = upload(c, &kd.d_col_j, col_j))) return s;
+    if ((s = upload(c, &kd.d_xa, xa))) return s;
+    std::vector<double> g2(Gk2, Gk2 + Ngw);
+    std::vector<float> g2f(Ngw);
+    for (int64_t g = 0; g < Ngw; ++g) g2f[g] = (float)g2[g];
+    if ((s = upload(c, &kd.d_Gk2, g2))) return s;
+    if ((s = upload(c, &kd.d_Gk2f, g2f))) return s;
+    (void)N3;
+    return PW_OK;
+}
+
+template <typename T>
+FftLaunch make_launch(const pw_ctx *c, int ik) {
+    const KData &kd = c->k[ik];
+    FftLaunch L;
+    L.kp.N1 = c->N1;
+    L.kp.N2 = c->N2;
+    L.kp.N3 = c->N3;
+    L.kp.Ngw = kd.Ngw;
+    L.kp.Ncol = kd.Ncol;
+    L.kp.Nxa = kd.Nxa;
+    L.kp.col_ptr = kd.d_col_ptr;
+    L.kp.ent_igw = kd.d_ent_igw;
+    L.kp.ent_kz = kd.d_ent_kz;
+    L.kp.ent_col = kd.d_ent_col;
+    L.kp.col_ia = kd.d_col_ia;
+    L.kp.col_j = kd.d_col_j;
+    L.kp.xa = kd.d_xa;
+    L.kp.Gk2 = kd.d_Gk2;
+    L.kp.Gk2f = kd.d_Gk2f;
+    L.dx = c->dx;
+    L.dy = c->dy;
+    L.dz = c->dz;
+    const bool dbl = sizeof(T) == 8;
+    L.twx = dbl ? (const void *)c->tw64[0] : (const void *)c->tw32[0];
+    L.twy = dbl ? (const void *)c->tw64[1] : (const void *)c->tw32[1];
+    L.twz = dbl ? (const void *)c->tw64[2] : (const void *)c->tw32[2];
+    const size_t es = 2 * sizeof(T);
+    // z passes: ~48 KB of shared memory per CTA
+    int Cg = (int)((48 * 1024 / es - c->N3) / c->N3);
+    L.Cg = std::max(1, std::min(64, Cg));
+    // plane passes: a 100 KB budget (two CTAs per SM) when it holds at
+    // least 16 full x lines, otherwise up to 220 KB
+    const size_t fixed = (size_t)c->N1 + c->N2 + (size_t)kd.Nxa * c->N2;
+    size_t budget = 100 * 1024 / es;
+    if (budget < fixed + (size_t)std::min(16, c->N2) * c->N1) budget = 220 * 1024 / es;
+    long Jc = budget > fixed ? (long)((budget - fixed) / c->N1) : 0;
+    L.Jc = (int)std::max(1L, std::min((long)c->N2, Jc));
+    return L;
+}
+
+size_t plane_smem_bytes(const pw_ctx *c, const FftLaunch &L, size_t es) {
+    return ((size_t)c->N1 + c->N2 + (size_t)L.kp.Nxa * c->N2 + (size_t)L.Jc * c->N1) * es;
+}
+
+int check_k(pw_ctx *c, int ik) {
+    if (ik < 0 || ik >= c->Nkpt) return fail(c, PW_ERR_ARG, "k-point index %d outside [0, %d)", ik, c->Nkpt);
+    return PW_OK;
+}
+
+int band_chunk(const pw_ctx *c, int ik, size_t es, int nb) {
+    const size_t per_band = (size_t)c->N3 * c->k[ik].Ncol * es;
+    size_t ch = c->a_chunk_bytes / std::max<size_t>(per_band, 1);
+    if (ch < 1) ch = 1;
+    return (int)std::min<size_t>(ch, (size_t)nb);
+}
+
+template <typename T>
+int apply_T(pw_ctx *c, int ik, int ispin, const void *psi, void *Hpsi, int64_t ld, int nb, unsigned ops) {
+    const KData &kd = c->k[ik];
+    const unsigned o = ops & PW_OP_H;
+    const int acc = (ops & PW_ACCUMULATE) ? 1 : 0;
+    const size_t es = 2 * sizeof(T);
+    cudaStream_t st = c->stream;
+    const void *beta = sizeof(T) == 8 ? (const void *)kd.d_beta64 : (const void *)kd.d_beta32;
+    if (o & PW_OP_VNL) {
+        if (c->nbeta <= 0 || !beta || !c->have_D)
+            return fail(c, PW_ERR_STATE, "op_V_Ps_nloc requested but the projectors of k-point %d are not set", ik);
+        int s;
+        const size_t pb = (size_t)c->nbeta * nb * sizeof(double2);
+        if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb)) ||
+            (s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb))))
+            return s;
+        CK(c, (gemm_tn<T>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+        CK(c, apply_dcsr(c->nbeta, nb, c->d_Drow, c->d_Dcol, c->d_Dval, (const double2 *)c->P.p, (double2 *)c->P2.p, st));
+        c->launches += 3;
+    }
+    if (o & PW_OP_VLOC) {
+        if (c->vloc_nspin <= 0) return fail(c, PW_ERR_STATE, "op_V_loc requested before pw_set_vloc");
+        if (ispin < 0 || ispin >= c->vloc_nspin) return fail(c, PW_ERR_ARG, "spin index %d outside [0, %d)", ispin, c->vloc_nspin);
+        FftLaunch L = make_launch<T>(c, ik);
+        const int nbc = band_chunk(c, ik, es, nb);
+        int s;
+        if ((s = ensure(c, c->A, (size_t)nbc * c->N3 * kd.Ncol * es))) return s;
+        const void *V = sizeof(T) == 8 ? (const void *)(c->d_V64 + (size_t)ispin * c->N)
+                                       : (const void *)(c->d_V32 + (size_t)ispin * c->N);
+        const int flags = ((o & PW_OP_K) ? 2 : 0) | (acc ? 4 : 0);
+        for (int b0 = 0; b0 < nb; b0 += nbc) {
+            const int cnt = std::min(nbc, nb - b0);
+            const char *pin = (const char *)psi + (size_t)b0 * ld * es;
+            char *pout = (char *)Hpsi + (size_t)b0 * ld * es;
+            CK(c, launch_zinv<T>(L, pin, ld, cnt, c->A.p, st));
+            CK(c, launch_plane_vloc<T>(L, V, c->A.p, cnt, st));
+            CK(c, launch_zfwd<T>(L, c->A.p, pin, pout, ld, cnt, flags, st));
+            c->launches += 3;
+        }
+    } else if (o & PW_OP_K) {
+        CK(c, launch_opK<T>(kd.Ngw, nb, kd.d_Gk2, psi, Hpsi, ld, acc, st));
+        c->launches += 1;
+    } else if (!acc) {
+        CK(c, launch_zero<T>(Hpsi, kd.Ngw, nb, ld, st));
+        c->launches += 1;
+    }
+    if (o & PW_OP_VNL) {
+        CK(c, gemm_nn<T>(kd.Ngw, nb, c->nbeta, beta, kd.Ngw, (const double2 *)c->P2.p, c->nbeta, Hpsi, ld, 1, st));
+        c->launches += 1;
+    }
+    return PW_OK;
+}
+
+template <typename T>
+int rhoe_T(pw_ctx *c, int ik, const void *psi, int64_t ld, int nb, const double *w_host, double *rhoe, int accumulate) {
+    const KData &kd = c->k[ik];
+    const size_t es = 2 * sizeof(T);
+    cudaStream_t st = c->stream;
+    FftLaunch L = make_launch<T>(c, ik);
+    const int nbc = band_chunk(c, ik, es, nb);
+    int s;
+    if ((s = ensure(c, c->A, (size_t)nbc * c->N3 * kd.Ncol * es))) return s;
+    // band groups: enough CTAs (N3 * G) to fill the GPU twice
+    int G = std::max(1, std::min(nbc, (2 * 148 + c->N3 - 1) / c->N3));
+    if ((s = ensure(c, c->rho_part, (size_t)G * c->N * sizeof(T)))) return s;
+    if ((s = ensure(c, c->w, (size_t)nb * sizeof(double)))) return s;
+    std::vector<double> wv(w_host, w_host + nb);
+    for (auto &x : wv) x /= c->CellVolume;
+    CK(c, cudaMemcpyAsync(c->w.p, wv.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    for (int b0 = 0; b0 < nb; b0 += nbc) {
+        const int cnt = std::min(nbc, nb - b0);
+        const int Gc = std::min(G, cnt);
+        const int Bg = (cnt + Gc - 1) / Gc;
+        const int Gu = (cnt + Bg - 1) / Bg;
+        const char *pin = (const char *)psi + (size_t)b0 * ld * es;
+        CK(c, launch_zinv<T>(L, pin, ld, cnt, c->A.p, st));
+        CK(c, launch_plane_rho<T>(L, c->A.p, cnt, Gu, Bg, (const double *)c->w.p + b0, c->rho_part.p, st));
+        CK(c, launch_rho_reduce<T>(c->rho_part.p, Gu, c->N, rhoe, (b0 == 0) ? accumulate : 1, st));
+        c->launches += 3;
+    }
+    // the weights live in a pageable host vector: finish before it goes away
+    CK(c, cudaStreamSynchronize(st));
+    return PW_OK;
+}
+
+int check_dtype(pw_ctx *c, int dtype) {
+    if (dtype != PW_C128 && dtype != PW_C64) return fail(c, PW_ERR_ARG, "unknown dtype %d", dtype);
+    return PW_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+
+extern "C" int pw_abi_version(void) { return PWB200_ABI_VERSION; }
+
+extern "C" const char *pw_last_error(const pw_ctx *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+extern "C" int pw_create(int device, const pw_grid_desc *d, pw_ctx **out) {
+    if (!out) return fail(nullptr, PW_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!d) return fail(nullptr, PW_ERR_ARG, "desc is NULL");
+    if (d->Ns[0] <= 0 || d->Ns[1] <= 0 || d->Ns[2] <= 0 || d->Nkpt <= 0 || d->Nspin < 1 || d->Nspin > 2 ||
+        !(d->CellVolume > 0) || !d->Ngw || !d->idx_gw2r || !d->Gk2 || (d->index_base != 0 && d->index_base != 1))
+        return fail(nullptr, PW_ERR_ARG, "invalid grid description");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(nullptr, PW_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(nullptr, PW_ERR_ARG, "device %d outside [0, %d)", device, ndev);
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, PW_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    pw_ctx *c = new pw_ctx();
+    c->device = device;
+    c->N1 = d->Ns[0];
+    c->N2 = d->Ns[1];
+    c->N3 = d->Ns[2];
+    c->N = (size_t)c->N1 * c->N2 * c->N3;
+    c->Nkpt = d->Nkpt;
+    c->Nspin = d->Nspin;
+    c->CellVolume = d->CellVolume;
+    if (const char *s = getenv("PW_A_CHUNK_MB")) c->a_chunk_bytes = (size_t)std::max(1, atoi(s)) << 20;
+    int st = PW_OK;
+    if (!make_plan(c->N1, c->dx) || !make_plan(c->N2, c->dy) || !make_plan(c->N3, c->dz)) {
+        st = fail(nullptr, PW_ERR_UNSUPPORTED, "grid %dx%dx%d: every dimension must factor into 2,3,5 and be <= 512",
+                  c->N1, c->N2, c->N3);
+    }
+    if (!st) {
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) st = fail(nullptr, PW_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        c->own_stream = true;
+    }
+    for (int s = 0; s < 3 && !st; ++s) st = build_twiddles(c, d->Ns[s], s);
+    if (!st) {
+        c->k.resize(c->Nkpt);
+        for (int ik = 0; ik < c->Nkpt && !st; ++ik) {
+            if (!d->idx_gw2r[ik] || !d->Gk2[ik]) {
+                st = fail(c, PW_ERR_ARG, "k-point %d: NULL idx_gw2r or Gk2", ik);
+                break;
+            }
+            st = build_kdata(c, c->k[ik], d->Ngw[ik], d->idx_gw2r[ik], d->index_base, d->Gk2[ik]);
+        }
+    }
+    if (st) {
+        if (!c->err.empty()) g_create_error = c->err;
+        pw_destroy(c);
+        return st;
+    }
+    *out = c;
+    return PW_OK;
+}
+
+extern "C" void pw_destroy(pw_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" int pw_set_stream(pw_ctx *c, void *stream) {
+    if (!c) return PW_ERR_ARG;
+    if (c->own_stream && c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
+    c->own_stream = false;
+    c->stream = (cudaStream_t)stream;
+    return PW_OK;
+}
+
+extern "C" int64_t pw_launch_count(const pw_ctx *c) { return c ? c->launches : -1; }
+
+extern "C" int pw_synchronize(pw_ctx *c) {
+    if (!c) return PW_ERR_ARG;
+    CK(c, cudaStreamSynchronize(c->stream));
+    return PW_OK;
+}
+
+static int set_vloc_common(pw_ctx *c, const double *V, int nspin, bool on_device) {
+    if (!c || !V) return c ? fail(c, PW_ERR_ARG, "V is NULL") : PW_ERR_ARG;
+    if (nspin < 1 || nspin > 2) return fail(c, PW_ERR_ARG, "nspin %d not in {1, 2}", nspin);
+    CK(c, cudaSetDevice(c->device));
+    const size_t n = c->N * nspin;
+    if (c->vloc_nspin < nspin) {
+        dfree(c, c->d_V64);
+        dfree(c, c->d_V32);
+        c->d_V64 = nullptr;
+        c->d_V32 = nullptr;
+        int s;
+        if ((s = dalloc(c, &c->d_V64, n)) || (s = dalloc(c, &c->d_V32, n))) return s;
+    }
+    CK(c, cudaMemcpyAsync(c->d_V64, V, n * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                          c->stream));
+    // fold the 1/N of G_to_R into the potential: fft(V .* ifft(x)) = fft((V/N) .* bfft(x))
+    const double inv = 1.0 / (double)c->N;
+    CK(c, convert_d_to_f(c->d_V64, c->d_V32, n, inv, c->stream));
+    CK(c, scale_d(c->d_V64, c->d_V64, n, inv, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->vloc_nspin = nspin;
+    return PW_OK;
+}
+
+extern "C" int pw_set_vloc(pw_ctx *c, const double *V, int nspin) { return set_vloc_common(c, V, nspin, false); }
+extern "C" int pw_set_vloc_device(pw_ctx *c, const double *V, int nspin) { return set_vloc_common(c, V, nspin, true); }
+
+extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik))) return s;
+    if (!beta || nbeta <= 0) return fail(c, PW_ERR_ARG, "empty betaNL");
+    if (c->nbeta != 0 && c->nbeta != nbeta) return fail(c, PW_ERR_ARG, "nbeta %d differs from %d", nbeta, c->nbeta);
+    CK(c, cudaSetDevice(c->device));
+    KData &kd = c->k[ik];
+    const size_t n = (size_t)kd.Ngw * nbeta;
+    if (!kd.d_beta64) {
+        if ((s = dalloc(c, &kd.d_beta64, n)) || (s = dalloc(c, &kd.d_beta32, n))) return s;
+    }
+    CK(c, cudaMemcpyAsync(kd.d_beta64, beta, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    CK(c, convert_c128_to_c64(kd.d_beta64, kd.d_beta32, n, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->nbeta = nbeta;
+    return PW_OK;
+}
+
+extern "C" int pw_set_nonlocal_coef(pw_ctx *c, int nnz, const int32_t *ib, const int32_t *jb, const double *h) {
+    if (!c) return PW_ERR_ARG;
+    if (c->nbeta <= 0) return fail(c, PW_ERR_STATE, "call pw_set_nonlocal before pw_set_nonlocal_coef");
+    if (nnz < 0 || (nnz > 0 && (!ib || !jb || !h))) return fail(c, PW_ERR_ARG, "invalid coefficient list");
+    std::vector<std::vector<std::pair<int, double>>> rows(c->nbeta);
+    for (int e = 0; e < nnz; ++e) {
+        if (ib[e] < 0 || ib[e] >= c->nbeta || jb[e] < 0 || jb[e] >= c->nbeta)
+            return fail(c, PW_ERR_ARG, "coefficient %d: index outside [0, %d)", e, c->nbeta);
+        bool merged = false;
+        for (auto &pr : rows[ib[e]])
+            if (pr.first == jb[e]) {
+                pr.second += h[e];
+                merged = true;
+            }
+        if (!merged) rows[ib[e]].push_back({jb[e], h[e]});
+    }
+    std::vector<int> rp(c->nbeta + 1, 0), col;
+    std::vector<double> val;
+    for (int i = 0; i < c->nbeta; ++i) {
+        for (auto &pr : rows[i]) {
+            col.push_back(pr.first);
+            val.push_back(pr.second);
+        }
+        rp[i + 1] = (int)col.size();
+    }
+    CK(c, cudaSetDevice(c->device));
+    dfree(c, c->d_Drow);
+    dfree(c, c->d_Dcol);
+    dfree(c, c->d_Dval);
+    int s;
+    if ((s = upload(c, &c->d_Drow, rp)) || (s = upload(c, &c->d_Dcol, col)) || (s = upload(c, &c->d_Dval, val))) return s;
+    c->have_D = true;
+    return PW_OK;
+}
+
+extern "C" int pw_apply(pw_ctx *c, int ik, int ispin, int dtype, const void *psi, void *Hpsi, int64_t ld, int nb,
+                        unsigned ops) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (!psi || !Hpsi) return fail(c, PW_ERR_ARG, "NULL wavefunction pointer");
+    if (psi == Hpsi) return fail(c, PW_ERR_ARG, "psi and Hpsi must not alias");
+    if (nb <= 0 || ld < c->k[ik].Ngw) return fail(c, PW_ERR_ARG, "bad shape: nb=%d ld=%lld Ngw=%d", nb, (long long)ld, c->k[ik].Ngw);
+    if (ops & ~(PW_OP_H | PW_ACCUMULATE)) return fail(c, PW_ERR_ARG, "unknown op flags 0x%x", ops);
+    CK(c, cudaSetDevice(c->device));
+    return dtype == PW_C128 ? apply_T<double>(c, ik, ispin, psi, Hpsi, ld, nb, ops)
+                            : apply_T<float>(c, ik, ispin, psi, Hpsi, ld, nb, ops);
+}
+
+extern "C" int pw_kprec(pw_ctx *c, int ik, int dtype, const void *in, void *out, int64_t ld, int nb) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (!in || !out || nb <= 0 || ld < c->k[ik].Ngw) return fail(c, PW_ERR_ARG, "bad Kprec arguments");
+    CK(c, cudaSetDevice(c->device));
+    const KData &kd = c->k[ik];
+    if (dtype == PW_C128)
+        CK(c, launch_kprec<double>(kd.Ngw, nb, kd.d_Gk2, in, out, ld, c->stream));
+    else
+        CK(c, launch_kprec<float>(kd.Ngw, nb, kd.d_Gk2, in, out, ld, c->stream));
+    return PW_OK;
+}
+
+extern "C" int pw_calc_rhoe(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, int nb, const double *w,
+                            double *rhoe, int accumulate) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (!psi || !w || !rhoe || nb <= 0 || ld < c->k[ik].Ngw) return fail(c, PW_ERR_ARG, "bad calc_rhoe arguments");
+    CK(c, cudaSetDevice(c->device));
+    return dtype == PW_C128 ? rhoe_T<double>(c, ik, psi, ld, nb, w, rhoe, accumulate)
+                            : rhoe_T<float>(c, ik, psi, ld, nb, w, rhoe, accumulate);
+}
+
+extern "C" int pw_gram(pw_ctx *c, int dtype, int64_t K, int m, int n, const void *A, int64_t lda, const void *B,
+                       int64_t ldb, double *C, int64_t ldc, int accumulate) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_dtype(c, dtype))) return s;
+    if (!A || !B || !C || K <= 0 || m <= 0 || n <= 0 || lda < K || ldb < K || ldc < m)
+        return fail(c, PW_ERR_ARG, "bad gram arguments");
+    CK(c, cudaSetDevice(c->device));
+    if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(K, m, n)))) return s;
+    if (dtype == PW_C128)
+        CK(c, gemm_tn<double>(K, m, n, A, lda, B, ldb, (double2 *)C, ldc, accumulate, c->gemm_ws.p, c->stream));
+    else
+        CK(c, gemm_tn<float>(K, m, n, A, lda, B, ldb, (double2 *)C, ldc, accumulate, c->gemm_ws.p, c->stream));
+    return PW_OK;
+}
+
+extern "C" int pw_rotate(pw_ctx *c, int dtype, int64_t M, int n, int k, const void *A, int64_t lda, const double *U,
+                         int64_t ldu, void *C, int64_t ldc, int accumulate) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_dtype(c, dtype))) return s;
+    if (!A || !U || !C || M <= 0 || n <= 0 || k <= 0 || lda < M || ldu < k || ldc < M)
+        return fail(c, PW_ERR_ARG, "bad rotate arguments");
+    if (A == C) return fail(c, PW_ERR_ARG, "A and C must not alias");
+    CK(c, cudaSetDevice(c->device));
+    if (dtype == PW_C128)
+        CK(c, gemm_nn<double>(M, n, k, A, lda, (const double2 *)U, ldu, C, ldc, accumulate, c->stream));
+    else
+        CK(c, gemm_nn<float>(M, n, k, A, lda, (const double2 *)U, ldu, C, ldc, accumulate, c->stream));
+    return PW_OK;
+}
+
+extern "C" int pw_op_H_host(pw_ctx *c, int ik, int ispin, const double *psi, double *Hpsi, int64_t ld, int nb,
+                            unsigned ops, int dtype) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (!psi || !Hpsi || nb <= 0 || ld < c->k[ik].Ngw) return fail(c, PW_ERR_ARG, "bad op_H arguments");
+    CK(c, cudaSetDevice(c->device));
+    const size_t n = (size_t)ld * nb;
+    const bool acc = (ops & PW_ACCUMULATE) != 0;
+    if ((s = ensure(c, c->st_in, n * sizeof(double2))) || (s = ensure(c, c->st_out, n * sizeof(double2)))) return s;
+    CK(c, cudaMemcpyAsync(c->st_in.p, psi, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (acc) CK(c, cudaMemcpyAsync(c->st_out.p, Hpsi, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (dtype == PW_C128) {
+        if ((s = apply_T<double>(c, ik, ispin, c->st_in.p, c->st_out.p, ld, nb, ops))) return s;
+    } else {
+        if ((s = ensure(c, c->st_in32, n * sizeof(float2))) || (s = ensure(c, c->st_out32, n * sizeof(float2)))) return s;
+        CK(c, convert_c128_to_c64((const double2 *)c->st_in.p, (float2 *)c->st_in32.p, n, c->stream));
+        if (acc) CK(c, convert_c128_to_c64((const double2 *)c->st_out.p, (float2 *)c->st_out32.p, n, c->stream));
+        if ((s = apply_T<float>(c, ik, ispin, c->st_in32.p, c->st_out32.p, ld, nb, ops))) return s;
+        CK(c, convert_c64_to_c128((const float2 *)c->st_out32.p, (double2 *)c->st_out.p, n, c->stream));
+    }
+    CK(c, cudaMemcpyAsync(Hpsi, c->st_out.p, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return PW_OK;
+}
+
+extern "C" int pw_calc_rhoe_host(pw_ctx *c, int ik, const double *psi, int64_t ld, int nb, const double *w,
+                                 double *rhoe, int accumulate, int dtype) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (!psi || !w || !rhoe || nb <= 0 || ld < c->k[ik].Ngw) return fail(c, PW_ERR_ARG, "bad calc_rhoe arguments");
+    CK(c, cudaSetDevice(c->device));
+    const size_t n = (size_t)ld * nb;
+    if ((s = ensure(c, c->st_in, n * sizeof(double2))) || (s = ensure(c, c->st_rho, c->N * sizeof(double)))) return s;
+    CK(c, cudaMemcpyAsync(c->st_in.p, psi, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if (accumulate) CK(c, cudaMemcpyAsync(c->st_rho.p, rhoe, c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (dtype == PW_C128) {
+        if ((s = rhoe_T<double>(c, ik, c->st_in.p, ld, nb, w, (double *)c->st_rho.p, accumulate))) return s;
+    } else {
+        if ((s = ensure(c, c->st_in32, n * sizeof(float2)))) return s;
+        CK(c, convert_c128_to_c64((const double2 *)c->st_in.p, (float2 *)c->st_in32.p, n, c->stream));
+        if ((s = rhoe_T<float>(c, ik, c->st_in32.p, ld, nb, w, (double *)c->st_rho.p, accumulate))) return s;
+    }
+    CK(c, cudaMemcpyAsync(rhoe, c->st_rho.p, c->N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return PW_OK;
+}

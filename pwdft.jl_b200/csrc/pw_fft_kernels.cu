@@ -1,0 +1,359 @@
+// Pruned, band-batched 3-D FFT passes for op_V_loc! and calc_rhoe!.
+//
+// The reference does, per band, a dense scatter into an N-point grid, a full
+// 3-D backward FFT, a pointwise product with V_loc, a full forward FFT and a
+// gather (op_V_loc.jl:137-165).  Here the transform is split along its axes
+// so that only non-zero data is ever transformed or stored:
+//
+//   K-zinv   per (band, column group): gather the sphere entries of each
+//            active (x,y) column (those holding at least one G of the
+//            wavefunction sphere), backward z-FFT, store A[b][z][col].
+//   K-plane  per (band, z-plane): scatter the plane's Ncol column values into
+//            an (active-x) x N2 sub-plane in SMEM, backward y-FFT on the
+//            active-x lines, then for chunks of y lines expand to full x
+//            lines, backward x-FFT, multiply by V(r)/N, forward x-FFT, keep
+//            the active-x outputs; forward y-FFT; store the active columns
+//            back to A.
+//   K-zfwd   per (band, column group): forward z-FFT, gather the sphere
+//            entries and write Hpsi = [Hpsi +] Vpsi [+ 0.5|G+k|^2 psi].
+//   K-rho    per (band group, z-plane): as K-plane up to the backward x-FFT,
+//            then rho_part += w_b |psi(r)|^2 / Omega.
+//
+// HBM traffic per band: psi once in, Hpsi once out, A (Ncol*N3 complex)
+// written/read twice, V once per plane batch (L2-resident across bands).
+#include "pw_fft.cuh"
+
+namespace pwk {
+
+constexpr int FFT_THREADS = 256;
+
+template <typename T> struct MaxV;
+template <> struct MaxV<float> { static constexpr int v = 8; };
+template <> struct MaxV<double> { static constexpr int v = 8; };
+
+// ------------------------------------------------------------------ K-zinv
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+k_zinv(KPlan kp, FftDim dz, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, int64_t ld,
+       Cx<T> *__restrict__ A, int Cg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *Z = tw + kp.N3;
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * Cg;
+    const int cn = min(Cg, kp.Ncol - c0);
+    const int N3 = kp.N3;
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
+    for (int i = threadIdx.x; i < N3 * Cg; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
+    __syncthreads();
+    const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
+    const Cx<T> *ps = psi + (size_t)b * ld;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int cl = kp.ent_col[e] - c0;
+        Z[kp.ent_kz[e] * Cg + cl] = ps[kp.ent_igw[e]];
+    }
+    __syncthreads();
+    fft_lines<T, MaxV<T>::v>(Z, dz, cn, Cg, 1, tw, +1);
+    Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol;
+    for (int p = threadIdx.x; p < N3 * cn; p += blockDim.x) {
+        const int kz = p / cn, cl = p - kz * cn;
+        Ab[(size_t)kz * kp.Ncol + c0 + cl] = Z[kz * Cg + cl];
+    }
+}
+
+// ------------------------------------------------------------------ K-zfwd
+// flags: 1 = add the V_loc part from A, 2 = add 0.5|G+k|^2 psi, 4 = accumulate into Hpsi
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+k_zfwd(KPlan kp, FftDim dz, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, const Cx<T> *__restrict__ psi,
+       Cx<T> *__restrict__ Hpsi, int64_t ld, int Cg, int flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *Z = tw + kp.N3;
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * Cg;
+    const int cn = min(Cg, kp.Ncol - c0);
+    const int N3 = kp.N3;
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
+    const Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol;
+    for (int p = threadIdx.x; p < N3 * cn; p += blockDim.x) {
+        const int kz = p / cn, cl = p - kz * cn;
+        Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + c0 + cl];
+    }
+    __syncthreads();
+    fft_lines<T, MaxV<T>::v>(Z, dz, cn, Cg, 1, tw, -1);
+    const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
+    const Cx<T> *ps = psi + (size_t)b * ld;
+    Cx<T> *hs = Hpsi + (size_t)b * ld;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int cl = kp.ent_col[e] - c0;
+        const int igw = kp.ent_igw[e];
+        Cx<T> out = Z[kp.ent_kz[e] * Cg + cl];
+        if (flags & 2) {
+            const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[igw] : (T)kp.Gk2f[igw];
+            out = cadd(out, cscale(ps[igw], (T)0.5 * g2));
+        }
+        if (flags & 4) out = cadd(out, hs[igw]);
+        hs[igw] = out;
+    }
+}
+
+// Shared-memory layout of the plane kernels.
+struct PlaneSmem {
+    int N1, N2, Nxa, Jc;
+    __host__ __device__ size_t elems() const { return (size_t)N1 + N2 + (size_t)Nxa * N2 + (size_t)Jc * N1; }
+};
+
+// ----------------------------------------------------------------- K-plane
+// Vr: V(r)/N for this spin channel, N1*N2*N3 reals, x fastest.
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+k_plane_vloc(KPlan kp, FftDim dx, FftDim dy, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy,
+             const T *__restrict__ Vr, Cx<T> *__restrict__ A, int Jc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N1 = kp.N1, N2 = kp.N2, N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N1;
+    Cx<T> *S = ty + N2;               // [Nxa][N2]
+    Cx<T> *X = S + (size_t)Nxa * N2;  // [Jc][N1]
+    const int kz = blockIdx.x;
+    const int b = blockIdx.y;
+    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
+    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < Nxa * N2; i += blockDim.x) S[i] = cmake((T)0, (T)0);
+    __syncthreads();
+    Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+    for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+    __syncthreads();
+    fft_lines<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, +1);
+    const T *Vp = Vr + (size_t)kz * N1 * N2;
+    for (int j0 = 0; j0 < N2; j0 += Jc) {
+        const int jc = min(Jc, N2 - j0);
+        for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cmake((T)0, (T)0);
+        __syncthreads();
+        for (int p = threadIdx.x; p < Nxa * jc; p += blockDim.x) {
+            const int ia = p / jc, jl = p - ia * jc;
+            X[jl * N1 + kp.xa[ia]] = S[ia * N2 + j0 + jl];
+        }
+        __syncthreads();
+        fft_lines<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, +1);
+        for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cscale(X[i], Vp[(size_t)j0 * N1 + i]);
+        __syncthreads();
+        fft_lines<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, -1);
+        for (int p = threadIdx.x; p < Nxa * jc; p += blockDim.x) {
+            const int ia = p / jc, jl = p - ia * jc;
+            S[ia * N2 + j0 + jl] = X[jl * N1 + kp.xa[ia]];
+        }
+        __syncthreads();
+    }
+    fft_lines<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, -1);
+    for (int c = threadIdx.x; c < Ncol; c += blockDim.x) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
+}
+
+// ------------------------------------------------------------------- K-rho
+// rho_part[g][ip] (+)= sum over the group's bands of w_b |bfft psi_b(r)|^2
+// (w_b already divided by Omega).  Each CTA owns plane kz of partial g.
+template <typename T>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+k_plane_rho(KPlan kp, FftDim dx, FftDim dy, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy,
+            const Cx<T> *__restrict__ A, int nb, int Bg, const double *__restrict__ w, T *__restrict__ rho_part, int Jc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N1 = kp.N1, N2 = kp.N2, N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N1;
+    Cx<T> *S = ty + N2;
+    Cx<T> *X = S + (size_t)Nxa * N2;
+    const int kz = blockIdx.x;
+    const int g = blockIdx.y;
+    const size_t N12 = (size_t)N1 * N2;
+    T *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
+    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
+    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
+    for (size_t i = threadIdx.x; i < N12; i += blockDim.x) rp[i] = (T)0;
+    const int b0 = g * Bg, b1 = min(nb, b0 + Bg);
+    for (int b = b0; b < b1; ++b) {
+        const T wb = (T)w[b];
+        for (int i = threadIdx.x; i < Nxa * N2; i += blockDim.x) S[i] = cmake((T)0, (T)0);
+        __syncthreads();
+        const Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+        for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+        __syncthreads();
+        fft_lines<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, +1);
+        for (int j0 = 0; j0 < N2; j0 += Jc) {
+            const int jc = min(Jc, N2 - j0);
+            for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cmake((T)0, (T)0);
+            __syncthreads();
+            for (int p = threadIdx.x; p < Nxa * jc; p += blockDim.x) {
+                const int ia = p / jc, jl = p - ia * jc;
+                X[jl * N1 + kp.xa[ia]] = S[ia * N2 + j0 + jl];
+            }
+            __syncthreads();
+            fft_lines<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, +1);
+            for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) {
+                const Cx<T> v = X[i];
+                rp[(size_t)j0 * N1 + i] += wb * (v.x * v.x + v.y * v.y);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// rho[ip] (+)= sum_g rho_part[g][ip]   (FP64 output)
+template <typename T>
+__global__ void k_rho_reduce(const T *__restrict__ part, int G, size_t N, double *__restrict__ rho, int accumulate) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        double s = accumulate ? rho[i] : 0.0;
+        for (int g = 0; g < G; ++g) s += (double)part[(size_t)g * N + i];
+        rho[i] = s;
+    }
+}
+
+// --------------------------------------------------------- elementwise ops
+// Hpsi (+)= 0.5 |G+k|^2 psi   (op_K.jl:67-73)
+template <typename T>
+__global__ void k_opK(int Ngw, int nb, const double *__restrict__ Gk2, const Cx<T> *__restrict__ psi,
+                      Cx<T> *__restrict__ Hpsi, int64_t ld, int accumulate) {
+    const size_t total = (size_t)Ngw * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t / Ngw), g = (int)(t - (size_t)b * Ngw);
+        const size_t o = (size_t)b * ld + g;
+        Cx<T> v = cscale(psi[o], (T)(0.5 * Gk2[g]));
+        if (accumulate) v = cadd(v, Hpsi[o]);
+        Hpsi[o] = v;
+    }
+}
+
+// out = in / (1 + |G+k|^2)   (Kprec.jl:97-111)
+template <typename T>
+__global__ void k_kprec(int Ngw, int nb, const double *__restrict__ Gk2, const Cx<T> *in, Cx<T> *out, int64_t ld) {
+    const size_t total = (size_t)Ngw * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t / Ngw), g = (int)(t - (size_t)b * Ngw);
+        const size_t o = (size_t)b * ld + g;
+        out[o] = cscale(in[o], (T)(1.0 / (1.0 + Gk2[g])));
+    }
+}
+
+template <typename T>
+__global__ void k_zero(Cx<T> *p, int Ngw, int nb, int64_t ld) {
+    const size_t total = (size_t)Ngw * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t / Ngw), g = (int)(t - (size_t)b * Ngw);
+        p[(size_t)b * ld + g] = cmake((T)0, (T)0);
+    }
+}
+
+}  // namespace pwk
+
+// ----------------------------------------------------------- host launchers
+#include "pw_launch.h"
+
+namespace pwk {
+
+static int grid_stride_blocks(size_t total) {
+    size_t b = (total + 255) / 256;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+template <typename T>
+static cudaError_t set_smem(const void *fn, size_t bytes) {
+    if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t launch_zinv(const FftLaunch &L, const void *psi, int64_t ld, int nb, void *A, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    int Cg = L.Cg;
+    size_t smem = (size_t)(kp.N3 + kp.N3 * Cg) * sizeof(Cx<T>);
+    cudaError_t e = set_smem<T>((const void *)k_zinv<T>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
+    k_zinv<T><<<grid, FFT_THREADS, smem, st>>>(kp, L.dz, (const Cx<T> *)L.twz, (const Cx<T> *)psi, ld, (Cx<T> *)A, Cg);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_zfwd(const FftLaunch &L, const void *A, const void *psi, void *Hpsi, int64_t ld, int nb, int flags,
+                        cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    int Cg = L.Cg;
+    size_t smem = (size_t)(kp.N3 + kp.N3 * Cg) * sizeof(Cx<T>);
+    cudaError_t e = set_smem<T>((const void *)k_zfwd<T>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
+    k_zfwd<T><<<grid, FFT_THREADS, smem, st>>>(kp, L.dz, (const Cx<T> *)L.twz, (const Cx<T> *)A, (const Cx<T> *)psi,
+                                               (Cx<T> *)Hpsi, ld, Cg, flags);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_plane_vloc(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
+    size_t smem = ps.elems() * sizeof(Cx<T>);
+    cudaError_t e = set_smem<T>((const void *)k_plane_vloc<T>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(kp.N3, nb);
+    k_plane_vloc<T><<<grid, FFT_THREADS, smem, st>>>(kp, L.dx, L.dy, (const Cx<T> *)L.twx, (const Cx<T> *)L.twy,
+                                                     (const T *)Vr, (Cx<T> *)A, L.Jc);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_plane_rho(const FftLaunch &L, const void *A, int nb, int G, int Bg, const double *w, void *rho_part,
+                             cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
+    size_t smem = ps.elems() * sizeof(Cx<T>);
+    cudaError_t e = set_smem<T>((const void *)k_plane_rho<T>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(kp.N3, G);
+    k_plane_rho<T><<<grid, FFT_THREADS, smem, st>>>(kp, L.dx, L.dy, (const Cx<T> *)L.twx, (const Cx<T> *)L.twy,
+                                                    (const Cx<T> *)A, nb, Bg, w, (T *)rho_part, L.Jc);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_rho_reduce(const void *part, int G, size_t N, double *rho, int accumulate, cudaStream_t st) {
+    k_rho_reduce<T><<<grid_stride_blocks(N), 256, 0, st>>>((const T *)part, G, N, rho, accumulate);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_opK(int Ngw, int nb, const double *Gk2, const void *psi, void *Hpsi, int64_t ld, int accumulate,
+                       cudaStream_t st) {
+    k_opK<T><<<grid_stride_blocks((size_t)Ngw * nb), 256, 0, st>>>(Ngw, nb, Gk2, (const Cx<T> *)psi, (Cx<T> *)Hpsi, ld,
+                                                                   accumulate);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_kprec(int Ngw, int nb, const double *Gk2, const void *in, void *out, int64_t ld, cudaStream_t st) {
+    k_kprec<T><<<grid_stride_blocks((size_t)Ngw * nb), 256, 0, st>>>(Ngw, nb, Gk2, (const Cx<T> *)in, (Cx<T> *)out, ld);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t st) {
+    k_zero<T><<<grid_stride_blocks((size_t)Ngw * nb), 256, 0, st>>>((Cx<T> *)p, Ngw, nb, ld);
+    return cudaGetLastError();
+}
+
+#define PW_INST(T)                                                                                                   \
+    template cudaError_t launch_zinv<T>(const FftLaunch &, const void *, int64_t, int, void *, cudaStream_t);       \
+    template cudaError_t launch_zfwd<T>(const FftLaunch &, const void *, const void *, void *, int64_t, int, int,  \
+                                        cudaStream_t);                                                               \
+    template cudaError_t launch_plane_vloc<T>(const FftLaunch &, const void *, void *, int, cudaStream_t);          \
+    template cudaError_t launch_plane_rho<T>(const FftLaunch &, const void *, int, int, int, const double *, void *, \
+                                             cudaStream_t);                                                          \
+    template cudaError_t launch_rho_reduce<T>(const void *, int, size_t, double *, int, cudaStream_t);              \
+    template cudaError_t launch_opK<T>(int, int, const double *, const void *, void *, int64_t, int, cudaStream_t); \
+    template cudaError_t launch_kprec<T>(int, int, const double *, const void *, void *, int64_t, cudaStream_t);    \
+    template cudaError_t launch_zero<T>(void *, int, int, int64_t, cudaStream_t);
+PW_INST(float)
+PW_INST(double)
+
+}  // namespace pwk

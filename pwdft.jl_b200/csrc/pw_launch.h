@@ -1,0 +1,52 @@
+// Host-side launcher declarations shared by the kernel files and the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "pw_common.cuh"
+
+namespace pwk {
+
+// Everything a pruned-FFT launch needs for one k-point and one precision.
+struct FftLaunch {
+    KPlan kp;
+    FftDim dx, dy, dz;
+    const void *twx, *twy, *twz;  // twiddle tables of the launch precision
+    int Cg;                       // columns per CTA in the z passes
+    int Jc;                       // y lines per x chunk in the plane passes
+};
+
+template <typename T> cudaError_t launch_zinv(const FftLaunch &, const void *psi, int64_t ld, int nb, void *A, cudaStream_t);
+template <typename T>
+cudaError_t launch_zfwd(const FftLaunch &, const void *A, const void *psi, void *Hpsi, int64_t ld, int nb, int flags,
+                        cudaStream_t);
+template <typename T> cudaError_t launch_plane_vloc(const FftLaunch &, const void *Vr, void *A, int nb, cudaStream_t);
+template <typename T>
+cudaError_t launch_plane_rho(const FftLaunch &, const void *A, int nb, int G, int Bg, const double *w, void *rho_part,
+                             cudaStream_t);
+template <typename T> cudaError_t launch_rho_reduce(const void *part, int G, size_t N, double *rho, int acc, cudaStream_t);
+template <typename T>
+cudaError_t launch_opK(int Ngw, int nb, const double *Gk2, const void *psi, void *Hpsi, int64_t ld, int acc, cudaStream_t);
+template <typename T>
+cudaError_t launch_kprec(int Ngw, int nb, const double *Gk2, const void *in, void *out, int64_t ld, cudaStream_t);
+template <typename T> cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t);
+
+// C (m x n, double2, ldc) (+)= A^H B with A (K x m), B (K x n) of element Cx<T>.
+// ws: split-K workspace of at least gemm_tn_ws_bytes() bytes.
+size_t gemm_tn_ws_bytes(int64_t K, int m, int n);
+template <typename T>
+cudaError_t gemm_tn(int64_t K, int m, int n, const void *A, int64_t lda, const void *B, int64_t ldb, double2 *C,
+                    int64_t ldc, int accumulate, void *ws, cudaStream_t);
+// C (M x n, Cx<T>, ldc) (+)= A (M x k, Cx<T>) * B (k x n, double2)
+template <typename T>
+cudaError_t gemm_nn(int64_t M, int n, int k, const void *A, int64_t lda, const double2 *B, int64_t ldb, void *C,
+                    int64_t ldc, int accumulate, cudaStream_t);
+// P2[i][b] = sum_j D[i][j] P[j][b]  (CSR D; P, P2 are nbeta x nb, ld = nbeta)
+cudaError_t apply_dcsr(int nbeta, int nb, const int *rowptr, const int *col, const double *val, const double2 *P,
+                       double2 *P2, cudaStream_t);
+// dtype conversions for the host drop-ins
+cudaError_t convert_c128_to_c64(const double2 *in, float2 *out, size_t n, cudaStream_t);
+cudaError_t convert_c64_to_c128(const float2 *in, double2 *out, size_t n, cudaStream_t);
+cudaError_t convert_d_to_f(const double *in, float *out, size_t n, double scale, cudaStream_t);
+cudaError_t scale_d(const double *in, double *out, size_t n, double scale, cudaStream_t);
+
+}  // namespace pwk

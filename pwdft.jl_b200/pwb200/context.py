@@ -1,0 +1,179 @@
+"""Owning wrapper around a ``pw_ctx`` (one basis, one device, one stream).
+
+Device wavefunction blocks are torch tensors of shape (nb, Ngw), contiguous:
+row b is band b, i.e. the memory of the reference's column-major
+Matrix{ComplexF64}(Ngw, nb) (PWDFT.jl wavefunctions).  Host arrays handed to
+the ``*_host`` methods are NumPy (Ngw, nb) arrays in the reference's layout.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (lib, check, pw_grid_desc, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE)
+
+_dp = C.POINTER(C.c_double)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def dtype_code(t):
+    """Element type code of a torch complex tensor."""
+    import torch
+    if t.dtype == torch.complex128:
+        return PW_C128
+    if t.dtype == torch.complex64:
+        return PW_C64
+    raise TypeError("wavefunctions must be complex128 (FP64 path) or complex64 (mixed precision), got %s" % t.dtype)
+
+
+class Context:
+    """Replaces Ham.pw's FFT plans / index maps plus the operator data
+    (V_loc, betaNL, h_ij) of a PWDFT.jl Hamiltonian on one GPU."""
+
+    def __init__(self, Ns, CellVolume, idx_gw2r, Gk2, Nspin=1, device=0, index_base=0):
+        self._L = lib()
+        self.Ns = tuple(int(n) for n in Ns)
+        self.N = int(np.prod(self.Ns))
+        self.Nkpt = len(idx_gw2r)
+        self.device = device
+        self._idx = [np.ascontiguousarray(np.asarray(i, dtype=np.int64)) for i in idx_gw2r]
+        self._gk2 = [np.ascontiguousarray(np.asarray(g, dtype=np.float64)) for g in Gk2]
+        self.Ngw = [len(i) for i in self._idx]
+        ngw = (C.c_int64 * self.Nkpt)(*self.Ngw)
+        pidx = (C.POINTER(C.c_int64) * self.Nkpt)(*[a.ctypes.data_as(C.POINTER(C.c_int64)) for a in self._idx])
+        pgk2 = (C.POINTER(C.c_double) * self.Nkpt)(*[_dptr(a) for a in self._gk2])
+        d = pw_grid_desc()
+        d.Ns[:] = list(self.Ns)
+        d.Nkpt, d.Nspin, d.index_base, d.CellVolume = self.Nkpt, Nspin, index_base, float(CellVolume)
+        d.Ngw = ngw
+        d.idx_gw2r = pidx
+        d.Gk2 = pgk2
+        h = C.c_void_p()
+        check(self._L.pw_create(device, C.byref(d), C.byref(h)))
+        self.h = h
+        self.CellVolume = float(CellVolume)
+        self.nbeta = 0
+        self._stream = None
+
+    # -------------------------------------------------------------- admin
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.pw_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st):
+        check(st, self.h)
+
+    def use_torch_stream(self):
+        """Order the library's work on torch's current CUDA stream."""
+        import torch
+        s = torch.cuda.current_stream(self.device)
+        if self._stream is not s:
+            self._chk(self._L.pw_set_stream(self.h, C.c_void_p(s.cuda_stream)))
+            self._stream = s
+
+    def synchronize(self):
+        self._chk(self._L.pw_synchronize(self.h))
+
+    # ------------------------------------------------------------ set-up
+    def set_vloc(self, V):
+        V = np.asarray(V, dtype=np.float64)
+        nspin = 1 if V.ndim == 1 else V.shape[1]
+        Vf = np.asfortranarray(V.reshape(self.N, nspin))
+        self._chk(self._L.pw_set_vloc(self.h, _dptr(Vf), nspin))
+
+    def set_vloc_device(self, V):
+        nspin = 1 if V.dim() == 1 else V.shape[0]
+        self.use_torch_stream()
+        self._chk(self._L.pw_set_vloc_device(self.h, C.c_void_p(V.data_ptr()), nspin))
+
+    def set_nonlocal(self, ik, betaNL):
+        b = np.asfortranarray(np.asarray(betaNL, dtype=np.complex128))
+        assert b.shape[0] == self.Ngw[ik]
+        self._chk(self._L.pw_set_nonlocal(self.h, ik, b.ctypes.data_as(_dp), b.shape[1]))
+        self.nbeta = b.shape[1]
+
+    def set_nonlocal_coef(self, triplets):
+        ib = np.array([t[0] for t in triplets], dtype=np.int32)
+        jb = np.array([t[1] for t in triplets], dtype=np.int32)
+        hv = np.array([t[2] for t in triplets], dtype=np.float64)
+        self._chk(self._L.pw_set_nonlocal_coef(self.h, len(triplets), ib.ctypes.data_as(C.POINTER(C.c_int32)),
+                                               jb.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(hv)))
+
+    # ----------------------------------------------------- device entry points
+    def apply(self, ik, ispin, psi, Hpsi, ops=PW_OP_H):
+        """Hpsi (+)= H psi; psi, Hpsi: torch (nb, Ngw) complex, same dtype."""
+        assert psi.dtype == Hpsi.dtype and psi.is_contiguous() and Hpsi.is_contiguous()
+        nb, ld = psi.shape
+        self.use_torch_stream()
+        self._chk(self._L.pw_apply(self.h, ik, ispin, dtype_code(psi), C.c_void_p(psi.data_ptr()),
+                                   C.c_void_p(Hpsi.data_ptr()), ld, nb, ops))
+
+    def kprec(self, ik, x, out):
+        nb, ld = x.shape
+        self.use_torch_stream()
+        self._chk(self._L.pw_kprec(self.h, ik, dtype_code(x), C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()),
+                                   ld, nb))
+
+    def calc_rhoe(self, ik, psi, w, rhoe, accumulate=False):
+        """rhoe (torch float64, N) (+)= sum_b w[b] |(N/sqrt(Omega)) G_to_R(psi_b)|^2."""
+        nb, ld = psi.shape
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        assert len(w) == nb
+        self.use_torch_stream()
+        self._chk(self._L.pw_calc_rhoe(self.h, ik, dtype_code(psi), C.c_void_p(psi.data_ptr()), ld, nb, _dptr(w),
+                                       C.c_void_p(rhoe.data_ptr()), int(accumulate)))
+
+    def gram(self, A, B, out, accumulate=False):
+        """out (torch complex128, (n, m) row-major = m x n column-major) (+)= A^H B,
+        A: (m, K), B: (n, K) band-major blocks."""
+        m, K = A.shape
+        n = B.shape[0]
+        assert out.shape == (n, m) and out.dtype.is_complex and out.element_size() == 16
+        self.use_torch_stream()
+        self._chk(self._L.pw_gram(self.h, dtype_code(A), K, m, n, C.c_void_p(A.data_ptr()), A.stride(0),
+                                  C.c_void_p(B.data_ptr()), B.stride(0), C.c_void_p(out.data_ptr()), m,
+                                  int(accumulate)))
+
+    def rotate(self, A, U, out, accumulate=False):
+        """out (n, M) (+)= A U: A (k, M) band-major, U complex128 (n, k) row-major
+        (= k x n column-major)."""
+        k, M = A.shape
+        n = U.shape[0]
+        assert U.shape[1] == k and out.shape == (n, M)
+        self.use_torch_stream()
+        self._chk(self._L.pw_rotate(self.h, dtype_code(A), M, n, k, C.c_void_p(A.data_ptr()), A.stride(0),
+                                    C.c_void_p(U.data_ptr()), U.stride(0), C.c_void_p(out.data_ptr()), out.stride(0),
+                                    int(accumulate)))
+
+    # ---------------------------------------------------------- host drop-ins
+    def op_H_host(self, ik, ispin, psi, Hpsi=None, ops=PW_OP_H, dtype=PW_C128):
+        """The reference call on host arrays: psi (Ngw, nb) complex128."""
+        psi = np.asfortranarray(np.asarray(psi, dtype=np.complex128))
+        ld, nb = psi.shape
+        if Hpsi is None:
+            Hpsi = np.zeros((ld, nb), dtype=np.complex128, order="F")
+            ops &= ~PW_ACCUMULATE
+        assert Hpsi.flags.f_contiguous and Hpsi.dtype == np.complex128
+        self._chk(self._L.pw_op_H_host(self.h, ik, ispin, psi.ctypes.data_as(_dp), Hpsi.ctypes.data_as(_dp), ld, nb,
+                                       ops, dtype))
+        return Hpsi
+
+    def calc_rhoe_host(self, ik, psi, w, rhoe=None, accumulate=False, dtype=PW_C128):
+        psi = np.asfortranarray(np.asarray(psi, dtype=np.complex128))
+        ld, nb = psi.shape
+        if rhoe is None:
+            rhoe = np.zeros(self.N)
+            accumulate = False
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        self._chk(self._L.pw_calc_rhoe_host(self.h, ik, psi.ctypes.data_as(_dp), ld, nb, _dptr(w), _dptr(rhoe),
+                                            int(accumulate), dtype))
+        return rhoe
