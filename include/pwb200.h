@@ -81,6 +81,10 @@ int         pw_synchronize(pw_ctx *ctx);
 /* Number of kernels this context has launched so far (for launch
  * accounting in benchmarks; no counterpart in the reference). */
 int64_t     pw_launch_count(const pw_ctx *ctx);
+/* Synchronises the context's stream and reports PW_ERR_TIMEOUT if a bounded
+ * device-side wait in one of its kernels gave up (no counterpart in the
+ * reference, whose BLAS calls cannot time out). */
+int         pw_check_device(pw_ctx *ctx);
 
 /* V_loc(r) = Ham.potentials.Total[:, ispin] (Hamiltonian.jl:542), host
  * FP64, N x nspin column-major.  Replaces the potential read by

@@ -14,6 +14,7 @@
 
 #include "../../include/pwb200.h"
 #include "pw_launch.h"
+#include "pw_umma.h"
 
 using namespace pwk;
 
@@ -34,6 +35,8 @@ struct KData {
     float *d_Gk2f = nullptr;
     double2 *d_beta64 = nullptr;
     float2 *d_beta32 = nullptr;
+    UmmaOperand beta_tn;  // split-BF16 betaNL for betaNL' psi   (tensor-core path)
+    UmmaOperand beta_nn;  // split-BF16 betaNL^H for betaNL * P  (tensor-core path)
 };
 
 constexpr int kMaxV64 = 8;  // complex values per thread per round in the FP64 FFT stages
@@ -48,7 +51,7 @@ bool make_plan(int n, FftDim &d) {
         while (m % r == 0) {
             if (d.nstage >= 12) return false;
             const int maxb = std::max(1, kMaxV64 / r);
-            if (n / r > kFftThreads * maxb) return false;
+            if (n / r > 32 * maxb) return false;  // one warp must hold a whole line stage
             d.radix[d.nstage++] = r;
             m /= r;
         }
@@ -81,6 +84,9 @@ struct pw_ctx {
     DevBuf A, P, P2, gemm_ws, rho_part, w, st_in, st_out, st_in32, st_out32, st_rho;
     std::vector<void *> allocs;
     size_t a_chunk_bytes = 48ull << 20;
+    bool use_umma = true;     // mixed-precision contractions on tcgen05 (PW_GEMM=cuda: CUDA cores)
+    int *d_err = nullptr;     // device error word of the bounded waits in the tensor-core kernels
+    DevBuf um_a_hi, um_a_lo, um_b_hi, um_b_lo, um_ws;
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -287,6 +293,53 @@ int band_chunk(const pw_ctx *c, int ik, size_t es, int nb) {
     return (int)std::min<size_t>(ch, (size_t)nb);
 }
 
+// Per-call split-BF16 operands live in grow-only scratch buffers.
+int umma_scratch(pw_ctx *c, DevBuf &hi, DevBuf &lo, int64_t rows, int64_t K, UmmaOperand &op) {
+    const size_t half = umma_operand_bytes(rows, K) / 2;
+    int s;
+    if ((s = ensure(c, hi, half)) || (s = ensure(c, lo, half))) return s;
+    op.hi = (__nv_bfloat16 *)hi.p;
+    op.lo = (__nv_bfloat16 *)lo.p;
+    return PW_OK;
+}
+
+// C (m x n, CT) (+)= Z^H W  on tensor cores; Z, W complex64 (K x m / K x n).
+template <typename CT>
+int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, const void *Wm, int64_t ldw, void *C,
+            int64_t ldc, int acc) {
+    UmmaOperand A, B;
+    int s;
+    if ((s = umma_scratch(c, c->um_a_hi, c->um_a_lo, 2 * (int64_t)m, K, A)) ||
+        (s = umma_scratch(c, c->um_b_hi, c->um_b_lo, n, K, B)))
+        return s;
+    CK(c, umma_prep_tn_a<float2>(Z, ldz, K, m, A, c->stream));
+    CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
+    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp)))) return s;
+    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream));
+    c->launches += 4;
+    return PW_OK;
+}
+
+// C (M x n, complex64) (+)= A (M x k, complex64) U (k x n, complex128) on tensor cores.
+int umma_nn(pw_ctx *c, int64_t M, int n, int k, const void *A, int64_t lda, const UmmaOperand *Aprep, const double2 *U,
+            int64_t ldu, void *C, int64_t ldc, int acc) {
+    UmmaOperand Ao, B;
+    int s;
+    if (Aprep) {
+        Ao = *Aprep;
+    } else {
+        if ((s = umma_scratch(c, c->um_a_hi, c->um_a_lo, 2 * M, k, Ao))) return s;
+        CK(c, umma_prep_nn_a<float2>(A, lda, M, k, Ao, c->stream));
+        c->launches += 2;
+    }
+    if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, n, k, B))) return s;
+    CK(c, umma_prep_tn_b<double2>(U, ldu, k, n, B, c->stream));
+    if ((s = ensure(c, c->um_ws, umma_ws_bytes(Ao.rows, n, Ao.Kp)))) return s;
+    CK(c, umma_gemm<float2>(Ao, B, (int)M, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream));
+    c->launches += 3;
+    return PW_OK;
+}
+
 template <typename T>
 int apply_T(pw_ctx *c, int ik, int ispin, const void *psi, void *Hpsi, int64_t ld, int nb, unsigned ops) {
     const KData &kd = c->k[ik];
@@ -300,12 +353,21 @@ int apply_T(pw_ctx *c, int ik, int ispin, const void *psi, void *Hpsi, int64_t l
             return fail(c, PW_ERR_STATE, "op_V_Ps_nloc requested but the projectors of k-point %d are not set", ik);
         int s;
         const size_t pb = (size_t)c->nbeta * nb * sizeof(double2);
-        if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb)) ||
-            (s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb))))
-            return s;
-        CK(c, (gemm_tn<T>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+        if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb))) return s;
+        if (sizeof(T) == 4 && c->use_umma) {
+            UmmaOperand B;
+            if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B))) return s;
+            CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
+            if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
+            CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, c->P.p, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
+            c->launches += 3;
+        } else {
+            if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb)))) return s;
+            CK(c, (gemm_tn<T>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+            c->launches += 2;
+        }
         CK(c, apply_dcsr(c->nbeta, nb, c->d_Drow, c->d_Dcol, c->d_Dval, (const double2 *)c->P.p, (double2 *)c->P2.p, st));
-        c->launches += 3;
+        c->launches += 1;
     }
     if (o & PW_OP_VLOC) {
         if (c->vloc_nspin <= 0) return fail(c, PW_ERR_STATE, "op_V_loc requested before pw_set_vloc");
@@ -334,8 +396,15 @@ int apply_T(pw_ctx *c, int ik, int ispin, const void *psi, void *Hpsi, int64_t l
         c->launches += 1;
     }
     if (o & PW_OP_VNL) {
-        CK(c, gemm_nn<T>(kd.Ngw, nb, c->nbeta, beta, kd.Ngw, (const double2 *)c->P2.p, c->nbeta, Hpsi, ld, 1, st));
-        c->launches += 1;
+        if (sizeof(T) == 4 && c->use_umma) {
+            int s;
+            if ((s = umma_nn(c, kd.Ngw, nb, c->nbeta, nullptr, 0, &kd.beta_nn, (const double2 *)c->P2.p, c->nbeta, Hpsi,
+                             ld, 1)))
+                return s;
+        } else {
+            CK(c, gemm_nn<T>(kd.Ngw, nb, c->nbeta, beta, kd.Ngw, (const double2 *)c->P2.p, c->nbeta, Hpsi, ld, 1, st));
+            c->launches += 1;
+        }
     }
     return PW_OK;
 }
@@ -409,9 +478,10 @@ extern "C" int pw_create(int device, const pw_grid_desc *d, pw_ctx **out) {
     c->Nspin = d->Nspin;
     c->CellVolume = d->CellVolume;
     if (const char *s = getenv("PW_A_CHUNK_MB")) c->a_chunk_bytes = (size_t)std::max(1, atoi(s)) << 20;
+    if (const char *s = getenv("PW_GEMM")) c->use_umma = strcmp(s, "cuda") != 0;
     int st = PW_OK;
     if (!make_plan(c->N1, c->dx) || !make_plan(c->N2, c->dy) || !make_plan(c->N3, c->dz)) {
-        st = fail(nullptr, PW_ERR_UNSUPPORTED, "grid %dx%dx%d: every dimension must factor into 2,3,5 and be <= 512",
+        st = fail(nullptr, PW_ERR_UNSUPPORTED, "grid %dx%dx%d: every dimension must factor into 2,3,5 and fit one warp per line (<= 160 with a factor 5)",
                   c->N1, c->N2, c->N3);
     }
     if (!st) {
@@ -420,6 +490,10 @@ extern "C" int pw_create(int device, const pw_grid_desc *d, pw_ctx **out) {
         c->own_stream = true;
     }
     for (int s = 0; s < 3 && !st; ++s) st = build_twiddles(c, d->Ns[s], s);
+    if (!st && !(st = dalloc(c, &c->d_err, 1))) {
+        e = cudaMemset(c->d_err, 0, sizeof(int));
+        if (e != cudaSuccess) st = fail(c, PW_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
+    }
     if (!st) {
         c->k.resize(c->Nkpt);
         for (int ik = 0; ik < c->Nkpt && !st; ++ik) {
@@ -460,6 +534,15 @@ extern "C" int pw_set_stream(pw_ctx *c, void *stream) {
 }
 
 extern "C" int64_t pw_launch_count(const pw_ctx *c) { return c ? c->launches : -1; }
+
+extern "C" int pw_check_device(pw_ctx *c) {
+    if (!c) return PW_ERR_ARG;
+    int h = 0;
+    CK(c, cudaStreamSynchronize(c->stream));
+    CK(c, cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return fail(c, PW_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel expired (code %d)", h);
+    return PW_OK;
+}
 
 extern "C" int pw_synchronize(pw_ctx *c) {
     if (!c) return PW_ERR_ARG;
@@ -508,6 +591,20 @@ extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta)
     }
     CK(c, cudaMemcpyAsync(kd.d_beta64, beta, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
     CK(c, convert_c128_to_c64(kd.d_beta64, kd.d_beta32, n, c->stream));
+    if (c->use_umma) {
+        // split-BF16 copies of betaNL for both tensor-core products, built once
+        for (UmmaOperand *op : {&kd.beta_tn, &kd.beta_nn}) {
+            const int64_t rows = (op == &kd.beta_tn) ? 2 * (int64_t)nbeta : 2 * (int64_t)kd.Ngw;
+            const int64_t K = (op == &kd.beta_tn) ? kd.Ngw : nbeta;
+            if (!op->hi) {
+                const size_t half = umma_operand_bytes(rows, K) / 2;
+                if ((s = dalloc(c, (unsigned char **)&op->hi, half)) || (s = dalloc(c, (unsigned char **)&op->lo, half)))
+                    return s;
+            }
+        }
+        CK(c, umma_prep_tn_a<float2>(kd.d_beta32, kd.Ngw, kd.Ngw, nbeta, kd.beta_tn, c->stream));
+        CK(c, umma_prep_nn_a<float2>(kd.d_beta32, kd.Ngw, kd.Ngw, nbeta, kd.beta_nn, c->stream));
+    }
     CK(c, cudaStreamSynchronize(c->stream));
     c->nbeta = nbeta;
     return PW_OK;
@@ -595,11 +692,13 @@ extern "C" int pw_gram(pw_ctx *c, int dtype, int64_t K, int m, int n, const void
     if (!A || !B || !C || K <= 0 || m <= 0 || n <= 0 || lda < K || ldb < K || ldc < m)
         return fail(c, PW_ERR_ARG, "bad gram arguments");
     CK(c, cudaSetDevice(c->device));
+    if (dtype == PW_C64 && c->use_umma) return umma_tn<double2>(c, K, m, n, A, lda, B, ldb, C, ldc, accumulate);
     if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(K, m, n)))) return s;
     if (dtype == PW_C128)
         CK(c, gemm_tn<double>(K, m, n, A, lda, B, ldb, (double2 *)C, ldc, accumulate, c->gemm_ws.p, c->stream));
     else
         CK(c, gemm_tn<float>(K, m, n, A, lda, B, ldb, (double2 *)C, ldc, accumulate, c->gemm_ws.p, c->stream));
+    c->launches += 2;
     return PW_OK;
 }
 
@@ -612,10 +711,13 @@ extern "C" int pw_rotate(pw_ctx *c, int dtype, int64_t M, int n, int k, const vo
         return fail(c, PW_ERR_ARG, "bad rotate arguments");
     if (A == C) return fail(c, PW_ERR_ARG, "A and C must not alias");
     CK(c, cudaSetDevice(c->device));
+    if (dtype == PW_C64 && c->use_umma)
+        return umma_nn(c, M, n, k, A, lda, nullptr, (const double2 *)U, ldu, C, ldc, accumulate);
     if (dtype == PW_C128)
         CK(c, gemm_nn<double>(M, n, k, A, lda, (const double2 *)U, ldu, C, ldc, accumulate, c->stream));
     else
         CK(c, gemm_nn<float>(M, n, k, A, lda, (const double2 *)U, ldu, C, ldc, accumulate, c->stream));
+    c->launches += 1;
     return PW_OK;
 }
 

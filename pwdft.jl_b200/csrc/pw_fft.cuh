@@ -165,3 +165,89 @@ __device__ void fft_lines(Cx<T> *buf, const FftDim &d, int nlines, int es, int l
         Ns *= R;
     }
 }
+
+// ------------------------------------------------------------------------
+// Warp-synchronous variant: each warp owns a group of g whole lines and
+// runs every stage of them with __syncwarp() only, so warps proceed
+// independently (no CTA-wide barrier per stage).  Requires n/R <= 32*MAXB(R)
+// for every stage (checked by fft_warp_ok); ends with a __syncthreads().
+template <typename T, int R, int MAXV>
+__device__ __noinline__ void warp_stage(Cx<T> *buf, int n, int Ns, int l0, int nl, int es, int ls,
+                                           const Cx<T> *tw, int sign, int lane, bool jfast) {
+    constexpr int MAXB = (MAXV / R) > 0 ? (MAXV / R) : 1;
+    const int nbf = n / R;
+    const int total = nl * nbf;
+    const int twstride = n / (Ns * R);
+    const T s = (T)sign;
+    Cx<T> v[MAXB][R];
+#pragma unroll
+    for (int t = 0; t < MAXB; ++t) {
+        const int id = lane + 32 * t;
+        if (id < total) {
+            const int line = jfast ? l0 + id / nbf : l0 + id % nl;
+            const int j = jfast ? id % nbf : id / nl;
+            const int jm = j % Ns;
+            const Cx<T> *p = buf + (size_t)line * ls + (size_t)j * es;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[t][r] = p[(size_t)r * nbf * es];
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                Cx<T> w = tw[r * jm * twstride];
+                if (sign > 0) w.y = -w.y;
+                v[t][r] = cmul(v[t][r], w);
+            }
+            SmallDft<T, R>::run(v[t], s);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < MAXB; ++t) {
+        const int id = lane + 32 * t;
+        if (id < total) {
+            const int line = jfast ? l0 + id / nbf : l0 + id % nl;
+            const int j = jfast ? id % nbf : id / nl;
+            const int jm = j % Ns;
+            const int idxD = (j / Ns) * Ns * R + jm;
+            Cx<T> *q = buf + (size_t)line * ls + (size_t)idxD * es;
+#pragma unroll
+            for (int r = 0; r < R; ++r) q[(size_t)r * Ns * es] = v[t][r];
+        }
+    }
+    __syncwarp();
+}
+
+template <int MAXV>
+__host__ __device__ inline int fft_warp_group(const FftDim &d) {
+    int g = 1 << 20;
+    for (int st = 0; st < d.nstage; ++st) {
+        const int R = d.radix[st];
+        const int maxb = (MAXV / R) > 0 ? (MAXV / R) : 1;
+        const int gg = (32 * maxb) / (d.n / R);
+        g = gg < g ? gg : g;
+    }
+    return g;
+}
+
+template <typename T, int MAXV>
+__device__ void fft_lines_w(Cx<T> *buf, const FftDim &d, int nlines, int es, int ls, const Cx<T> *tw, int sign) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int g = fft_warp_group<MAXV>(d);
+    if (g < 1) g = 1;
+    const bool jfast = (es == 1);
+    for (int l0 = warp * g; l0 < nlines; l0 += nw * g) {
+        const int nl = min(g, nlines - l0);
+        int Ns = 1;
+        for (int st = 0; st < d.nstage; ++st) {
+            const int R = d.radix[st];
+            switch (R) {
+            case 2: warp_stage<T, 2, MAXV>(buf, d.n, Ns, l0, nl, es, ls, tw, sign, lane, jfast); break;
+            case 3: warp_stage<T, 3, MAXV>(buf, d.n, Ns, l0, nl, es, ls, tw, sign, lane, jfast); break;
+            case 4: warp_stage<T, 4, MAXV>(buf, d.n, Ns, l0, nl, es, ls, tw, sign, lane, jfast); break;
+            case 5: warp_stage<T, 5, MAXV>(buf, d.n, Ns, l0, nl, es, ls, tw, sign, lane, jfast); break;
+            default: warp_stage<T, 8, MAXV>(buf, d.n, Ns, l0, nl, es, ls, tw, sign, lane, jfast); break;
+            }
+            Ns *= R;
+        }
+    }
+    __syncthreads();
+}

@@ -53,7 +53,7 @@ k_zinv(KPlan kp, FftDim dz, const Cx<T> *__restrict__ twz, const Cx<T> *__restri
         Z[kp.ent_kz[e] * Cg + cl] = ps[kp.ent_igw[e]];
     }
     __syncthreads();
-    fft_lines<T, MaxV<T>::v>(Z, dz, cn, Cg, 1, tw, +1);
+    fft_lines_w<T, MaxV<T>::v>(Z, dz, cn, Cg, 1, tw, +1);
     Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol;
     for (int p = threadIdx.x; p < N3 * cn; p += blockDim.x) {
         const int kz = p / cn, cl = p - kz * cn;
@@ -81,7 +81,7 @@ k_zfwd(KPlan kp, FftDim dz, const Cx<T> *__restrict__ twz, const Cx<T> *__restri
         Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + c0 + cl];
     }
     __syncthreads();
-    fft_lines<T, MaxV<T>::v>(Z, dz, cn, Cg, 1, tw, -1);
+    fft_lines_w<T, MaxV<T>::v>(Z, dz, cn, Cg, 1, tw, -1);
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
     const Cx<T> *ps = psi + (size_t)b * ld;
     Cx<T> *hs = Hpsi + (size_t)b * ld;
@@ -125,7 +125,7 @@ k_plane_vloc(KPlan kp, FftDim dx, FftDim dy, const Cx<T> *__restrict__ twx, cons
     Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
     for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
     __syncthreads();
-    fft_lines<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, +1);
+    fft_lines_w<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, +1);
     const T *Vp = Vr + (size_t)kz * N1 * N2;
     for (int j0 = 0; j0 < N2; j0 += Jc) {
         const int jc = min(Jc, N2 - j0);
@@ -136,17 +136,17 @@ k_plane_vloc(KPlan kp, FftDim dx, FftDim dy, const Cx<T> *__restrict__ twx, cons
             X[jl * N1 + kp.xa[ia]] = S[ia * N2 + j0 + jl];
         }
         __syncthreads();
-        fft_lines<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, +1);
+        fft_lines_w<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, +1);
         for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cscale(X[i], Vp[(size_t)j0 * N1 + i]);
         __syncthreads();
-        fft_lines<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, -1);
+        fft_lines_w<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, -1);
         for (int p = threadIdx.x; p < Nxa * jc; p += blockDim.x) {
             const int ia = p / jc, jl = p - ia * jc;
             S[ia * N2 + j0 + jl] = X[jl * N1 + kp.xa[ia]];
         }
         __syncthreads();
     }
-    fft_lines<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, -1);
+    fft_lines_w<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, -1);
     for (int c = threadIdx.x; c < Ncol; c += blockDim.x) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
 }
 
@@ -178,7 +178,7 @@ k_plane_rho(KPlan kp, FftDim dx, FftDim dy, const Cx<T> *__restrict__ twx, const
         const Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
         for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
         __syncthreads();
-        fft_lines<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, +1);
+        fft_lines_w<T, MaxV<T>::v>(S, dy, Nxa, 1, N2, ty, +1);
         for (int j0 = 0; j0 < N2; j0 += Jc) {
             const int jc = min(Jc, N2 - j0);
             for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cmake((T)0, (T)0);
@@ -188,7 +188,7 @@ k_plane_rho(KPlan kp, FftDim dx, FftDim dy, const Cx<T> *__restrict__ twx, const
                 X[jl * N1 + kp.xa[ia]] = S[ia * N2 + j0 + jl];
             }
             __syncthreads();
-            fft_lines<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, +1);
+            fft_lines_w<T, MaxV<T>::v>(X, dx, jc, 1, N1, tx, +1);
             for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) {
                 const Cx<T> v = X[i];
                 rp[(size_t)j0 * N1 + i] += wb * (v.x * v.x + v.y * v.y);

@@ -1,0 +1,35 @@
+// Tensor-core (tcgen05) complex GEMM of the mixed-precision path; see pw_umma.cu.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pwk {
+
+// A K-major split-BF16 operand: `rows` rows of Kp BF16 values (hi and lo).
+struct UmmaOperand {
+    __nv_bfloat16 *hi = nullptr;
+    __nv_bfloat16 *lo = nullptr;
+    int64_t rows = 0;
+    int Kp = 0;
+};
+
+int umma_kpad(int64_t K);                          // padded 2K (multiple of 64)
+size_t umma_operand_bytes(int64_t rows, int64_t K);  // hi + lo bytes for `rows` rows
+size_t umma_ws_bytes(int64_t Mp, int Np, int Kp);    // split-K workspace
+
+// Operand builders (CT = float2 or double2 input element).
+//   tn_a: A' (2m rows) from Z (K x m)          for C = Z^H W
+//   tn_b: B' (n rows)  from W (K x n)
+//   nn_a: A' (2M rows) from Z = A^H, A (M x k) for C = A U
+template <typename CT> cudaError_t umma_prep_tn_a(const void *Z, int64_t ld, int64_t K, int m, UmmaOperand &, cudaStream_t);
+template <typename CT> cudaError_t umma_prep_tn_b(const void *W, int64_t ld, int64_t K, int n, UmmaOperand &, cudaStream_t);
+template <typename CT> cudaError_t umma_prep_nn_a(const void *A, int64_t lda, int64_t M, int k, UmmaOperand &, cudaStream_t);
+
+// C (m x n complex of type CT, ldc) (+)= result; A.rows == 2m, B.rows == n.
+// err: device int set non-zero if a bounded wait in the kernel expired.
+template <typename CT>
+cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
+                      float *ws, int *err, cudaStream_t);
+
+}  // namespace pwk

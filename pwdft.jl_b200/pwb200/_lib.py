@@ -49,6 +49,7 @@ SIGNATURES = {
     "pw_set_stream": (_i, [_vp, _vp]),
     "pw_synchronize": (_i, [_vp]),
     "pw_launch_count": (_i64, [_vp]),
+    "pw_check_device": (_i, [_vp]),
     "pw_set_vloc": (_i, [_vp, _dp, _i]),
     "pw_set_vloc_device": (_i, [_vp, _vp, _i]),
     "pw_set_nonlocal": (_i, [_vp, _i, _dp, _i]),

@@ -83,6 +83,13 @@ class Context:
     def synchronize(self):
         self._chk(self._L.pw_synchronize(self.h))
 
+    def check_device(self):
+        """Raise PWError(PW_ERR_TIMEOUT) if a bounded device wait expired."""
+        self._chk(self._L.pw_check_device(self.h))
+
+    def launch_count(self):
+        return int(self._L.pw_launch_count(self.h))
+
     # ------------------------------------------------------------ set-up
     def set_vloc(self, V):
         V = np.asarray(V, dtype=np.float64)

@@ -29,7 +29,7 @@ def system(request):
         H = systems.Ham_Si_fcc(meshk=(3, 3, 3), extra_states=4)
         nb = 8
     else:
-        H = systems.Ham_Si64(Nstates=48)
+        H = systems.Ham_Si64(Nstates=160)
         nb = 48
     rng = np.random.default_rng(11)
     N = H.pw.Npoints
@@ -140,6 +140,7 @@ def test_gram_and_rotate(system, prec):
     out = torch.zeros((5, A.shape[0]), dtype=dt, device="cuda")
     ctx.rotate(to_dev(A, dt), torch.from_numpy(np.ascontiguousarray(U.T)).cuda(), out)
     assert rel_err(to_host(out), A @ U) < TOL[prec]
+    ctx.check_device()   # no bounded device-side wait expired
 
 
 @pytest.mark.parametrize("prec", ["c128", "c64"])
