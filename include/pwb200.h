@@ -131,6 +131,25 @@ int pw_rotate(pw_ctx *ctx, int dtype, int64_t M, int n, int k, const void *A,
               int64_t lda, const double *U, int64_t ldu, void *C, int64_t ldc,
               int accumulate);
 
+/* Allocation-free variant of pw_apply for the local-potential round trip
+ * (ops = PW_OP_VLOC, optionally | PW_OP_K | PW_ACCUMULATE).  It has no
+ * counterpart in the reference.  It is for callers that cannot allocate
+ * device memory on this path: a host that hands the whole GPU to its own
+ * pooling allocator, or a solver loop that must not stall on the implicit
+ * device synchronisation of cudaMalloc/cudaFree.  pw_apply may grow its
+ * intermediate buffer on first use or when nb grows; this call never does.
+ * Its intermediate is one file-scope device array of
+ * pw_noalloc_scratch_bytes() (32 MiB) that every GPU loading the library
+ * holds until exit; bands are processed in batches that fit, and a grid
+ * whose single band needs more returns PW_ERR_UNSUPPORTED.  The first call
+ * on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the array, so calls whose
+ * work overlaps on the GPU (other streams, other contexts) race. */
+int      pw_apply_vloc_noalloc(pw_ctx *ctx, int ik, int ispin, int dtype,
+                               const void *psi, void *Hpsi, int64_t ld,
+                               int nb, unsigned ops);
+uint64_t pw_noalloc_scratch_bytes(void);
+
 /* ---- host drop-ins (the reference's Julia arrays) ------------------- */
 
 /* op_H!(Ham, psi, Hpsi) and friends on host ComplexF64 arrays; compute

@@ -769,3 +769,29 @@ extern "C" int pw_calc_rhoe_host(pw_ctx *c, int ik, const double *psi, int64_t l
     CK(c, cudaStreamSynchronize(c->stream));
     return PW_OK;
 }
+
+// ------------------------------------------------------------------------
+// Internal accessors used by the allocation-free entry point (pw_noalloc.cu).
+int pwk_fail(pw_ctx *c, int code, const char *msg) { return fail(c, code, "%s", msg); }
+
+void pwk_count_launches(pw_ctx *c, int n) { c->launches += n; }
+
+// Validates (ik, ispin, dtype) for an op_V_loc round trip and returns the
+// launch description, the V(r)/N pointer of the precision, the stream, the
+// scratch bytes one band needs, and the context's device.  Allocates nothing.
+int pwk_vloc_view(pw_ctx *c, int ik, int ispin, int dtype, pwk::FftLaunch *L, const void **V, cudaStream_t *st,
+                  size_t *per_band, int *device) {
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (c->vloc_nspin <= 0) return fail(c, PW_ERR_STATE, "op_V_loc requested before pw_set_vloc");
+    if (ispin < 0 || ispin >= c->vloc_nspin) return fail(c, PW_ERR_ARG, "spin index %d outside [0, %d)", ispin, c->vloc_nspin);
+    const bool dbl = dtype == PW_C128;
+    *L = dbl ? make_launch<double>(c, ik) : make_launch<float>(c, ik);
+    *V = dbl ? (const void *)(c->d_V64 + (size_t)ispin * c->N) : (const void *)(c->d_V32 + (size_t)ispin * c->N);
+    *st = c->stream;
+    *per_band = (size_t)c->N3 * c->k[ik].Ncol * (dbl ? sizeof(double2) : sizeof(float2));
+    *device = c->device;
+    return PW_OK;
+}
+
+int pwk_ngw(const pw_ctx *c, int ik) { return c->k[ik].Ngw; }

@@ -55,6 +55,8 @@ SIGNATURES = {
     "pw_set_nonlocal": (_i, [_vp, _i, _dp, _i]),
     "pw_set_nonlocal_coef": (_i, [_vp, _i, _i32p, _i32p, _dp]),
     "pw_apply": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _u]),
+    "pw_apply_vloc_noalloc": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _u]),
+    "pw_noalloc_scratch_bytes": (C.c_uint64, []),
     "pw_kprec": (_i, [_vp, _i, _i, _vp, _vp, _i64, _i]),
     "pw_calc_rhoe": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _vp, _i]),
     "pw_gram": (_i, [_vp, _i, _i64, _i, _i, _vp, _i64, _vp, _i64, _vp, _i64, _i]),

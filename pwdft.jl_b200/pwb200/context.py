@@ -124,6 +124,15 @@ class Context:
         self._chk(self._L.pw_apply(self.h, ik, ispin, dtype_code(psi), C.c_void_p(psi.data_ptr()),
                                    C.c_void_p(Hpsi.data_ptr()), ld, nb, ops))
 
+    def apply_vloc_noalloc(self, ik, ispin, psi, Hpsi, ops):
+        """pw_apply_vloc_noalloc: the V_loc (+K) round trip using the library's
+        fixed device scratch instead of context-allocated buffers."""
+        assert psi.dtype == Hpsi.dtype and psi.is_contiguous() and Hpsi.is_contiguous()
+        nb, ld = psi.shape
+        self.use_torch_stream()
+        self._chk(self._L.pw_apply_vloc_noalloc(self.h, ik, ispin, dtype_code(psi), C.c_void_p(psi.data_ptr()),
+                                                C.c_void_p(Hpsi.data_ptr()), ld, nb, ops))
+
     def kprec(self, ik, x, out):
         nb, ld = x.shape
         self.use_torch_stream()
