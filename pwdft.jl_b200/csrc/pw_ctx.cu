@@ -87,6 +87,7 @@ struct pw_ctx {
     bool use_umma = true;     // mixed-precision contractions on tcgen05 (PW_GEMM=cuda: CUDA cores)
     int *d_err = nullptr;     // device error word of the bounded waits in the tensor-core kernels
     DevBuf um_a_hi, um_a_lo, um_b_hi, um_b_lo, um_ws;
+    DevBuf slots[32];         // grow-only scratch for the eigensolver and LOBPCG
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -795,3 +796,13 @@ int pwk_vloc_view(pw_ctx *c, int ik, int ispin, int dtype, pwk::FftLaunch *L, co
 }
 
 int pwk_ngw(const pw_ctx *c, int ik) { return c->k[ik].Ngw; }
+
+int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out) {
+    if (slot < 0 || slot >= 32) return fail(c, PW_ERR_ARG, "scratch slot %d", slot);
+    int s = ensure(c, c->slots[slot], bytes);
+    if (s) return s;
+    *out = c->slots[slot].p;
+    return PW_OK;
+}
+cudaStream_t pwk_stream(pw_ctx *c) { return c->stream; }
+int pwk_device(const pw_ctx *c) { return c->device; }

@@ -22,6 +22,7 @@
 // HBM traffic per band: psi once in, Hpsi once out, A (Ncol*N3 complex)
 // written/read twice, V once per plane batch (L2-resident across bands).
 #include "pw_fft.cuh"
+#include "pw_fft_tmpl.cuh"
 
 namespace pwk {
 
@@ -243,6 +244,158 @@ __global__ void k_zero(Cx<T> *p, int Ngw, int nb, int64_t ld) {
     }
 }
 
+
+// ======================================================= fixed-size kernels
+// The same passes with the line lengths as template constants (see
+// pw_fft_tmpl.cuh); used for the grid sizes listed in FIXED_SIZES below,
+// the run-time kernels above serve every other {2,3,5}-smooth size.
+template <typename T> struct MinBlocks;
+template <> struct MinBlocks<float> { static constexpr int v = 3; };
+template <> struct MinBlocks<double> { static constexpr int v = 2; };
+
+template <typename T, int N3>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, int64_t ld, Cx<T> *__restrict__ A,
+        int Cg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *Z = tw + N3;
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * Cg;
+    const int cn = min(Cg, kp.Ncol - c0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
+    for (int i = threadIdx.x; i < N3 * Cg; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
+    __syncthreads();
+    const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
+    const Cx<T> *ps = psi + (size_t)b * ld;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0] = ps[kp.ent_igw[e]];
+    __syncthreads();
+    pwt::lines<T, N3, MaxV<T>::v, false>(Z, cn, Cg, 1, tw, +1);
+    Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol + c0;
+    for (int kz = warp; kz < N3; kz += nw)
+        for (int cl = lane; cl < cn; cl += 32) Ab[(size_t)kz * kp.Ncol + cl] = Z[kz * Cg + cl];
+}
+
+template <typename T, int N3>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, const Cx<T> *__restrict__ psi,
+        Cx<T> *__restrict__ Hpsi, int64_t ld, int Cg, int flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *Z = tw + N3;
+    const int b = blockIdx.y;
+    const int c0 = blockIdx.x * Cg;
+    const int cn = min(Cg, kp.Ncol - c0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
+    const Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol + c0;
+    for (int kz = warp; kz < N3; kz += nw)
+        for (int cl = lane; cl < cn; cl += 32) Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + cl];
+    __syncthreads();
+    pwt::lines<T, N3, MaxV<T>::v, false>(Z, cn, Cg, 1, tw, -1);
+    const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
+    const Cx<T> *ps = psi + (size_t)b * ld;
+    Cx<T> *hs = Hpsi + (size_t)b * ld;
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int igw = kp.ent_igw[e];
+        Cx<T> out = Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0];
+        if (flags & 2) {
+            const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[igw] : (T)kp.Gk2f[igw];
+            out = cadd(out, cscale(ps[igw], (T)0.5 * g2));
+        }
+        if (flags & 4) out = cadd(out, hs[igw]);
+        hs[igw] = out;
+    }
+}
+
+template <typename T, int N1, int N2>
+__device__ __forceinline__ void plane_to_real(const KPlan &kp, Cx<T> *S, Cx<T> *X, const Cx<T> *tx, int j0, int jc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cmake((T)0, (T)0);
+    __syncthreads();
+    for (int ia = warp; ia < kp.Nxa; ia += nw) {
+        const int x = kp.xa[ia];
+        for (int jl = lane; jl < jc; jl += 32) X[jl * N1 + x] = S[ia * N2 + j0 + jl];
+    }
+    __syncthreads();
+    pwt::lines<T, N1, MaxV<T>::v, true>(X, jc, 1, N1, tx, +1);
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+kf_plane_vloc(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
+              Cx<T> *__restrict__ A, int Jc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N1;
+    Cx<T> *S = ty + N2;
+    Cx<T> *X = S + Nxa * N2;
+    const int kz = blockIdx.x, b = blockIdx.y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
+    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < Nxa * N2; i += blockDim.x) S[i] = cmake((T)0, (T)0);
+    __syncthreads();
+    Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+    for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+    __syncthreads();
+    pwt::lines<T, N2, MaxV<T>::v, true>(S, Nxa, 1, N2, ty, +1);
+    const T *Vp = Vr + (size_t)kz * N1 * N2;
+    for (int j0 = 0; j0 < N2; j0 += Jc) {
+        const int jc = min(Jc, N2 - j0);
+        plane_to_real<T, N1, N2>(kp, S, X, tx, j0, jc);
+        for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cscale(X[i], Vp[j0 * N1 + i]);
+        __syncthreads();
+        pwt::lines<T, N1, MaxV<T>::v, true>(X, jc, 1, N1, tx, -1);
+        for (int ia = warp; ia < Nxa; ia += nw) {
+            const int x = kp.xa[ia];
+            for (int jl = lane; jl < jc; jl += 32) S[ia * N2 + j0 + jl] = X[jl * N1 + x];
+        }
+        __syncthreads();
+    }
+    pwt::lines<T, N2, MaxV<T>::v, true>(S, Nxa, 1, N2, ty, -1);
+    for (int c = threadIdx.x; c < Ncol; c += blockDim.x) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+kf_plane_rho(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy, const Cx<T> *__restrict__ A,
+             int nb, int Bg, const double *__restrict__ w, T *__restrict__ rho_part, int Jc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N1;
+    Cx<T> *S = ty + N2;
+    Cx<T> *X = S + Nxa * N2;
+    const int kz = blockIdx.x, g = blockIdx.y;
+    constexpr int N12 = N1 * N2;
+    T *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
+    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
+    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < N12; i += blockDim.x) rp[i] = (T)0;
+    const int b0 = g * Bg, b1 = min(nb, b0 + Bg);
+    for (int b = b0; b < b1; ++b) {
+        const T wb = (T)w[b];
+        for (int i = threadIdx.x; i < Nxa * N2; i += blockDim.x) S[i] = cmake((T)0, (T)0);
+        __syncthreads();
+        const Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+        for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+        __syncthreads();
+        pwt::lines<T, N2, MaxV<T>::v, true>(S, Nxa, 1, N2, ty, +1);
+        for (int j0 = 0; j0 < N2; j0 += Jc) {
+            const int jc = min(Jc, N2 - j0);
+            plane_to_real<T, N1, N2>(kp, S, X, tx, j0, jc);
+            for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) {
+                const Cx<T> v = X[i];
+                rp[j0 * N1 + i] += wb * (v.x * v.x + v.y * v.y);
+            }
+            __syncthreads();
+        }
+    }
+}
+
 }  // namespace pwk
 
 // ----------------------------------------------------------- host launchers
@@ -263,11 +416,27 @@ static cudaError_t set_smem(const void *fn, size_t bytes) {
     return cudaSuccess;
 }
 
+// Line lengths with compile-time kernels (every dimension of the grids of
+// the Si2/Al4 (27), Si64 (75) and Si216 (120) systems).
+#define FIXED_SIZES(X) X(27) X(75) X(120)
+
 template <typename T>
 cudaError_t launch_zinv(const FftLaunch &L, const void *psi, int64_t ld, int nb, void *A, cudaStream_t st) {
     const KPlan &kp = L.kp;
     int Cg = L.Cg;
     size_t smem = (size_t)(kp.N3 + kp.N3 * Cg) * sizeof(Cx<T>);
+    {
+        dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
+#define PW_CASE(NN)                                                                                                  \
+    if (kp.N3 == NN) {                                                                                               \
+        cudaError_t e = set_smem<T>((const void *)kf_zinv<T, NN>, smem);                                             \
+        if (e != cudaSuccess) return e;                                                                              \
+        kf_zinv<T, NN><<<grid, FFT_THREADS, smem, st>>>(kp, (const Cx<T> *)L.twz, (const Cx<T> *)psi, ld, (Cx<T> *)A, Cg); \
+        return cudaGetLastError();                                                                                   \
+    }
+        FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+    }
     cudaError_t e = set_smem<T>((const void *)k_zinv<T>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
@@ -281,6 +450,19 @@ cudaError_t launch_zfwd(const FftLaunch &L, const void *A, const void *psi, void
     const KPlan &kp = L.kp;
     int Cg = L.Cg;
     size_t smem = (size_t)(kp.N3 + kp.N3 * Cg) * sizeof(Cx<T>);
+    {
+        dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
+#define PW_CASE(NN)                                                                                                  \
+    if (kp.N3 == NN) {                                                                                               \
+        cudaError_t e = set_smem<T>((const void *)kf_zfwd<T, NN>, smem);                                             \
+        if (e != cudaSuccess) return e;                                                                              \
+        kf_zfwd<T, NN><<<grid, FFT_THREADS, smem, st>>>(kp, (const Cx<T> *)L.twz, (const Cx<T> *)A, (const Cx<T> *)psi, \
+                                                        (Cx<T> *)Hpsi, ld, Cg, flags);                               \
+        return cudaGetLastError();                                                                                   \
+    }
+        FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+    }
     cudaError_t e = set_smem<T>((const void *)k_zfwd<T>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
@@ -294,6 +476,19 @@ cudaError_t launch_plane_vloc(const FftLaunch &L, const void *Vr, void *A, int n
     const KPlan &kp = L.kp;
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
+    if (kp.N1 == kp.N2) {
+        dim3 grid(kp.N3, nb);
+#define PW_CASE(NN)                                                                                                  \
+    if (kp.N1 == NN) {                                                                                               \
+        cudaError_t e = set_smem<T>((const void *)kf_plane_vloc<T, NN, NN>, smem);                                   \
+        if (e != cudaSuccess) return e;                                                                              \
+        kf_plane_vloc<T, NN, NN><<<grid, FFT_THREADS, smem, st>>>(kp, (const Cx<T> *)L.twx, (const Cx<T> *)L.twy,    \
+                                                                  (const T *)Vr, (Cx<T> *)A, L.Jc);                  \
+        return cudaGetLastError();                                                                                   \
+    }
+        FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+    }
     cudaError_t e = set_smem<T>((const void *)k_plane_vloc<T>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid(kp.N3, nb);
@@ -308,6 +503,19 @@ cudaError_t launch_plane_rho(const FftLaunch &L, const void *A, int nb, int G, i
     const KPlan &kp = L.kp;
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
+    if (kp.N1 == kp.N2) {
+        dim3 grid(kp.N3, G);
+#define PW_CASE(NN)                                                                                                  \
+    if (kp.N1 == NN) {                                                                                               \
+        cudaError_t e = set_smem<T>((const void *)kf_plane_rho<T, NN, NN>, smem);                                    \
+        if (e != cudaSuccess) return e;                                                                              \
+        kf_plane_rho<T, NN, NN><<<grid, FFT_THREADS, smem, st>>>(kp, (const Cx<T> *)L.twx, (const Cx<T> *)L.twy,     \
+                                                                 (const Cx<T> *)A, nb, Bg, w, (T *)rho_part, L.Jc);  \
+        return cudaGetLastError();                                                                                   \
+    }
+        FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+    }
     cudaError_t e = set_smem<T>((const void *)k_plane_rho<T>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid(kp.N3, G);
