@@ -150,12 +150,60 @@ int      pw_apply_vloc_noalloc(pw_ctx *ctx, int ik, int ispin, int dtype,
                                int nb, unsigned ops);
 uint64_t pw_noalloc_scratch_bytes(void);
 
+/* Lowest k eigenpairs of the Hermitian-definite pencil (T, G) of order n,
+ * FP64 on the device: T S = G S diag(lam), S^H G S = I (G == NULL: standard
+ * problem T S = S diag(lam)).  T and G are read from their upper triangles
+ * (Julia's Hermitian(A)) and overwritten; lam: device k doubles ascending;
+ * S: device n x k ComplexF64 or NULL for eigenvalues only.  Replaces
+ * eigen(T, G) / eigvals(XHX) / eigen(S) of diag_LOBPCG.jl:86,185,216.
+ * PW_ERR_NOT_POSDEF when G is not positive definite. */
+int pw_eigh(pw_ctx *ctx, int n, int k, double *T, double *G, double *lam,
+            double *S);
+
+/* diag_LOBPCG!(Ham, X; tol, NiterMax, Nstates_conv) for k-point ik
+ * (diag_LOBPCG.jl:51-225): X (device, Ngw x nb, ld) is overwritten with the
+ * Ritz vectors, evals (host, nb) with the Ritz values; converged when
+ * nconv (or nb if nconv <= 0) eigenvalues moved by less than tol between
+ * iterations.  dtype PW_C64 runs the blocks in FP32 with split-BF16x3
+ * tensor-core contractions and FP64 small matrices; PW_C128 is all FP64.
+ * niter (host, may be NULL) receives the iteration count. */
+int pw_lobpcg(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
+              int nb, double tol, int nitermax, int nconv, double *evals,
+              int *niter);
+
+/* ---- update! and energies on the device ----------------------------- */
+
+/* The density G-sphere (PWGrid.gvec: idx_g2r, G2, sorted by G2 so that
+ * G = 0 comes first, PWGrid.jl:199-242), needed by pw_poisson/pw_update. */
+int pw_set_density_sphere(pw_ctx *ctx, int64_t Ng, const int64_t *idx_g2r,
+                          const double *G2, int index_base);
+/* Poisson_solve! (Poisson_solve.jl:22-40): V_H(r) from rho(r), device FP64
+ * arrays of N points. */
+int pw_poisson(pw_ctx *ctx, const double *rho, double *VH);
+/* update! (Hamiltonian.jl:510-545, VWN, Nspin = 1) + the sums of
+ * calc_E_local (calc_energies.jl:245-333): V_tot = V_ps + V_H + V_xc becomes
+ * the context's V_loc; VH / Vxc (device N, may be NULL) receive V_H and
+ * V_xc; E3 (host) = {sum V_H rho, sum V_ps rho, sum eps_xc rho} (multiply by
+ * dVol, and E_Hartree by 1/2). */
+int pw_update(pw_ctx *ctx, const double *rho, const double *Vps, double *VH,
+              double *Vxc, double *E3);
+/* calc_E_kin + calc_E_Ps_nloc (calc_energies.jl:342-375, 7-58) of one
+ * k-point: E2 (host) = {0.5 sum_b w_b sum_g |psi|^2 |G+k|^2,
+ * sum_b w_b sum_ij h_ij conj(B_i) B_j} with w (host, nb) = wk * Focc. */
+int pw_band_energies(pw_ctx *ctx, int ik, int dtype, const void *psi,
+                     int64_t ld, int nb, const double *w, double *E2);
+
 /* ---- host drop-ins (the reference's Julia arrays) ------------------- */
 
 /* op_H!(Ham, psi, Hpsi) and friends on host ComplexF64 arrays; compute
  * precision chosen by dtype (PW_C128 = reference FP64, PW_C64 = mixed). */
 int pw_op_H_host(pw_ctx *ctx, int ik, int ispin, const double *psi,
                  double *Hpsi, int64_t ld, int nb, unsigned ops, int dtype);
+/* diag_LOBPCG!(Ham, X) for k-point ik on the reference's host array X
+ * (Ngw x nb ComplexF64, ld), copied in and out around pw_lobpcg. */
+int pw_lobpcg_host(pw_ctx *ctx, int ik, int ispin, int dtype, double *X,
+                   int64_t ld, int nb, double tol, int nitermax, int nconv,
+                   double *evals, int *niter);
 /* calc_rhoe! inner loop for one k-point on host arrays; rhoe is host FP64
  * (N), accumulated when accumulate != 0. */
 int pw_calc_rhoe_host(pw_ctx *ctx, int ik, const double *psi, int64_t ld,

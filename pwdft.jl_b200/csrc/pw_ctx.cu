@@ -88,6 +88,8 @@ struct pw_ctx {
     int *d_err = nullptr;     // device error word of the bounded waits in the tensor-core kernels
     DevBuf um_a_hi, um_a_lo, um_b_hi, um_b_lo, um_ws;
     DevBuf slots[32];         // grow-only scratch for the eigensolver and LOBPCG
+    KData dens;               // the density G-sphere (for Poisson_solve! on the device)
+    bool have_dens = false;
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -239,8 +241,15 @@ int build_kdata(pw_ctx *c, KData &kd, int64_t Ngw, const int64_t *idx, int base,
 }
 
 template <typename T>
+FftLaunch make_launch_kd(const pw_ctx *c, const KData &kd);
+
+template <typename T>
 FftLaunch make_launch(const pw_ctx *c, int ik) {
-    const KData &kd = c->k[ik];
+    return make_launch_kd<T>(c, c->k[ik]);
+}
+
+template <typename T>
+FftLaunch make_launch_kd(const pw_ctx *c, const KData &kd) {
     FftLaunch L;
     L.kp.N1 = c->N1;
     L.kp.N2 = c->N2;
@@ -806,3 +815,59 @@ int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out) {
 }
 cudaStream_t pwk_stream(pw_ctx *c) { return c->stream; }
 int pwk_device(const pw_ctx *c) { return c->device; }
+int pwk_nkpt(const pw_ctx *c) { return c->Nkpt; }
+
+int pwk_density_launch(pw_ctx *c, pwk::FftLaunch *L, const double **G2, int *Ng, size_t *N) {
+    if (!c->have_dens) return fail(c, PW_ERR_STATE, "call pw_set_density_sphere first");
+    *L = make_launch_kd<double>(c, c->dens);
+    *G2 = c->dens.d_Gk2;
+    *Ng = c->dens.Ngw;
+    *N = c->N;
+    return PW_OK;
+}
+int pwk_set_vloc_device(pw_ctx *c, const double *V, int nspin) { return set_vloc_common(c, V, nspin, true); }
+const double *pwk_gk2(const pw_ctx *c, int ik) { return c->k[ik].d_Gk2; }
+
+// P = betaNL' psi and P2 = D P for k-point ik into the context's buffers
+int pwk_projections(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, int nb, const double2 **P,
+                    const double2 **P2, int *nbeta) {
+    *nbeta = c->nbeta;
+    if (c->nbeta <= 0) return PW_OK;
+    const KData &kd = c->k[ik];
+    const void *beta = dtype == PW_C128 ? (const void *)kd.d_beta64 : (const void *)kd.d_beta32;
+    if (!beta || !c->have_D) return fail(c, PW_ERR_STATE, "projectors of k-point %d are not set", ik);
+    int s;
+    const size_t pb = (size_t)c->nbeta * nb * sizeof(double2);
+    if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb))) return s;
+    cudaStream_t st = c->stream;
+    if (dtype == PW_C64 && c->use_umma) {
+        UmmaOperand B;
+        if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B))) return s;
+        CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
+        if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
+        CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, c->P.p, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
+    } else {
+        if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb)))) return s;
+        if (dtype == PW_C128)
+            CK(c, (gemm_tn<double>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+        else
+            CK(c, (gemm_tn<float>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+    }
+    CK(c, apply_dcsr(c->nbeta, nb, c->d_Drow, c->d_Dcol, c->d_Dval, (const double2 *)c->P.p, (double2 *)c->P2.p, st));
+    c->launches += 3;
+    *P = (const double2 *)c->P.p;
+    *P2 = (const double2 *)c->P2.p;
+    return PW_OK;
+}
+
+extern "C" int pw_set_density_sphere(pw_ctx *c, int64_t Ng, const int64_t *idx_g2r, const double *G2, int index_base) {
+    if (!c) return PW_ERR_ARG;
+    if (!idx_g2r || !G2 || Ng <= 0 || (index_base != 0 && index_base != 1))
+        return fail(c, PW_ERR_ARG, "bad density sphere");
+    CK(c, cudaSetDevice(c->device));
+    if (c->have_dens) return fail(c, PW_ERR_STATE, "density sphere already set");
+    int s = build_kdata(c, c->dens, Ng, idx_g2r, index_base, G2);
+    if (s) return s;
+    c->have_dens = true;
+    return PW_OK;
+}

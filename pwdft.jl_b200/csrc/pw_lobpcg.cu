@@ -1,0 +1,344 @@
+// pw_lobpcg: diag_LOBPCG! for one k-point (diag_LOBPCG.jl:51-225) with every
+// block operation on the device: op_H and Kprec through pw_apply / pw_kprec,
+// the Rayleigh-Ritz contractions through pw_gram / pw_rotate (tcgen05
+// split-BF16x3 for complex64 blocks, FP64 CUDA cores for complex128), and the
+// small FP64 Cholesky / eigen problems through the hand-written solver of
+// pw_eig.cu.  The host only steers: it reads the nb eigenvalues per
+// iteration for the convergence test (|evals - evals_old| < tol, as the
+// reference).  The lock branch of the reference (devals <= 10 eps,
+// :125-163) is not taken: its locking is replaced by the unlocked update.
+// Mixed precision only: the reference's basis Q = [X W P] drifts towards
+// linear dependence (lambda_min(Q'Q) ~ 1e-6 after a few iterations on Si64),
+// which FP64 tolerates but a split-BF16 Gram (~1e-5 absolute error) does
+// not; the mixed path therefore orthogonalises W against X and P, and the
+// new P against the new X (block Gram-Schmidt, then Cholesky-QR as in the
+// reference).  The Rayleigh-Ritz subspace span{X, W, P} of an iteration is
+// unchanged by this; later iterates differ at round-off-amplified level and
+// converge to the same Ritz values.  When the Cholesky of P'P fails the conjugate
+// directions restart (P = W), and when that of W'W fails the iteration stops
+// (residuals at the FP32 noise floor); the count of such events is returned
+// as 1000 x restarts + iterations in *niter.  The FP64 path reports
+// PW_ERR_NOT_POSDEF like the reference's cholesky.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/pwb200.h"
+#include "pw_eig.h"
+#include "pw_launch.h"
+
+int pwk_fail(pw_ctx *c, int code, const char *msg);
+int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out);
+cudaStream_t pwk_stream(pw_ctx *c);
+int pwk_ngw(const pw_ctx *c, int ik);
+int pwk_device(const pw_ctx *c);
+int pwk_nkpt(const pw_ctx *c);
+void pwk_count_launches(pw_ctx *c, int n);
+
+namespace {
+
+enum Slot { S_Q = 16, S_HQ, S_TMP1, S_TMP2, S_SMALL, S_EIGW, S_EIGSTAT };
+
+__global__ void k_scale_c128(const double2 *in, double2 *out, size_t n, double s) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = make_double2(in[i].x * s, in[i].y * s);
+}
+// S := (S + S^H)/2 written to both triangles
+__global__ void k_herm_avg(double2 *S, int n) {
+    const size_t total = (size_t)n * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(t / n), i = (int)(t - (size_t)j * n);
+        if (i < j) {
+            const double2 a = S[t], b = S[(size_t)i * n + j];
+            const double2 m = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+            S[t] = m;
+            S[(size_t)i * n + j] = make_double2(m.x, -m.y);
+        } else if (i == j) {
+            S[t].y = 0.0;
+        }
+    }
+}
+// lower := conj(upper)^T (Julia's Hermitian(A)), diagonal made real
+__global__ void k_herm_from_upper(double2 *A, int n) {
+    const size_t total = (size_t)n * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(t / n), i = (int)(t - (size_t)j * n);
+        if (i > j) {
+            const double2 u = A[(size_t)i * n + j];
+            A[t] = make_double2(u.x, -u.y);
+        } else if (i == j) {
+            A[t].y = 0.0;
+        }
+    }
+}
+int blocks_for(size_t total) {
+    size_t b = (total + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    return b < 1 ? 1 : (int)b;
+}
+
+struct Run {
+    pw_ctx *c;
+    cudaStream_t st;
+    int dtype;
+    size_t es;
+    int ngw, nb;
+    int64_t ldq;
+    char *Q, *HQ, *T1, *T2;     // Q = [X W P], HQ = [HX HW HP], two Ngw x 2nb temporaries
+    double2 *small;             // small FP64 complex matrices
+    void *eigw;
+    size_t eigw_bytes;
+    int *eigstat;
+    int restarts = 0;           // mixed-precision safeguards taken (see pw_lobpcg)
+
+    char *blk(char *base, int j) const { return base + (size_t)j * nb * ldq * es; }
+};
+
+#define RK(x)                     \
+    do {                          \
+        int s_ = (x);             \
+        if (s_ != PW_OK) return s_; \
+    } while (0)
+#define CKR(c, x)                                                           \
+    do {                                                                    \
+        cudaError_t e_ = (x);                                               \
+        if (e_ != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, #x " failed"); \
+    } while (0)
+
+// lowest k eigenpairs of (T, G) (G may be null) of order n; T, G overwritten
+int eig(Run &r, double2 *T, double2 *G, int n, int k, double *lam_dev, double2 *S) {
+    CKR(r.c, pwk::hegv_lowest(T, G, n, k, lam_dev, S, r.eigw, r.eigw_bytes, nullptr, r.eigstat, r.st));
+    int h[2] = {0, 0};
+    CKR(r.c, cudaMemcpyAsync(h, r.eigstat, sizeof(h), cudaMemcpyDeviceToHost, r.st));
+    CKR(r.c, cudaStreamSynchronize(r.st));
+    if (h[0]) return pwk_fail(r.c, PW_ERR_TIMEOUT, "a bounded grid barrier of the eigensolver expired");
+    if (h[1]) return pwk_fail(r.c, PW_ERR_NOT_POSDEF, "overlap matrix not positive definite (Cholesky)");
+    pwk_count_launches(r.c, 10);
+    return PW_OK;
+}
+
+// upper Cholesky factor R of the Hermitian C (C = R^H R) and Rinv = R^-1:
+// via the generalized solver with T = I would cost too much, so use the
+// lower factor of pw_eig's Cholesky: returns Rinv in `Rinv` (n x n).
+int chol_rinv(Run &r, double2 *C, int n, double2 *Rinv);
+
+// X (Ngw x k block, ld ldq) := X * M  (M: k x n device FP64 complex, ld ldm) into out
+int rot(Run &r, const char *A, int k, const double2 *M, int ldm, int n, char *out, int acc) {
+    return pw_rotate(r.c, r.dtype, r.ngw, n, k, A, r.ldq, (const double *)M, ldm, out, r.ldq, acc);
+}
+int gram(Run &r, const char *A, int m, const char *B, int n, double2 *C, int ldc) {
+    return pw_gram(r.c, r.dtype, r.ngw, m, n, A, r.ldq, B, r.ldq, (double *)C, ldc, 0);
+}
+int copy_blk(Run &r, char *dst, const char *src, int ncols) {
+    CKR(r.c, cudaMemcpy2DAsync(dst, r.ldq * r.es, src, r.ldq * r.es, r.ngw * r.es, ncols, cudaMemcpyDeviceToDevice, r.st));
+    return PW_OK;
+}
+
+// B -= A (A'B) and HB -= HA (A'B) for nb-column blocks (A orthonormal):
+// the block Gram-Schmidt step of the mixed-precision LOBPCG.  M: nb x nb scratch.
+__global__ void k_neg_c128(double2 *M, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        M[i] = make_double2(-M[i].x, -M[i].y);
+}
+int project_out(Run &r, const char *A, const char *HA, char *B, char *HB, double2 *M) {
+    const size_t nn = (size_t)r.nb * r.nb;
+    RK(gram(r, A, r.nb, B, r.nb, M, r.nb));
+    k_neg_c128<<<blocks_for(nn), 256, 0, r.st>>>(M, nn);
+    RK(rot(r, A, r.nb, M, r.nb, r.nb, B, 1));
+    RK(rot(r, HA, r.nb, M, r.nb, r.nb, HB, 1));
+    return PW_OK;
+}
+
+}  // namespace
+
+// Rinv = R^-1 with C = R^H R: the lower Cholesky factor L = R^H gives
+// R^-1 = L^-H.  Uses pw_eig's Cholesky through a dedicated small routine.
+namespace pwk {
+cudaError_t chol_inverse_upper(double2 *C, int n, double2 *Rinv, void *work, int *d_status, cudaStream_t st);
+}
+
+namespace {
+int chol_rinv(Run &r, double2 *C, int n, double2 *Rinv) {
+    CKR(r.c, pwk::chol_inverse_upper(C, n, Rinv, r.eigw, r.eigstat, r.st));
+    int h[2] = {0, 0};
+    CKR(r.c, cudaMemcpyAsync(h, r.eigstat, sizeof(h), cudaMemcpyDeviceToHost, r.st));
+    CKR(r.c, cudaStreamSynchronize(r.st));
+    if (h[0]) return pwk_fail(r.c, PW_ERR_TIMEOUT, "a bounded grid barrier of the Cholesky expired");
+    if (h[1]) return pwk_fail(r.c, PW_ERR_NOT_POSDEF, "cholesky(Hermitian(C)) failed: C not positive definite");
+    pwk_count_launches(r.c, 4);
+    return PW_OK;
+}
+}  // namespace
+
+extern "C" int pw_eigh(pw_ctx *c, int n, int k, double *T, double *G, double *lam, double *S) {
+    if (!c) return PW_ERR_ARG;
+    if (n <= 0 || k <= 0 || k > n || !T || !lam) return pwk_fail(c, PW_ERR_ARG, "bad pw_eigh arguments");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    Run r{};
+    r.c = c;
+    r.st = pwk_stream(c);
+    r.eigw_bytes = pwk::eig_work_bytes(n, k);
+    RK(pwk_scratch(c, S_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, S_EIGSTAT, 64, (void **)&r.eigstat));
+    return eig(r, (double2 *)T, (double2 *)G, n, k, lam, (double2 *)S);
+}
+
+extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64_t ld, int nb, double tol, int nitermax,
+                         int nconv_target, double *evals, int *niter_out) {
+    if (!c) return PW_ERR_ARG;
+    if (dtype != PW_C128 && dtype != PW_C64) return pwk_fail(c, PW_ERR_ARG, "unknown dtype");
+    if (!X || !evals || nb <= 0 || nitermax <= 0) return pwk_fail(c, PW_ERR_ARG, "bad pw_lobpcg arguments");
+    if (ik < 0 || ik >= pwk_nkpt(c)) return pwk_fail(c, PW_ERR_ARG, "bad k-point index");
+    const int ngw = pwk_ngw(c, ik);
+    if (ld < ngw || 3 * nb > ngw) return pwk_fail(c, PW_ERR_ARG, "bad pw_lobpcg shape (need ld >= Ngw and 3 nb <= Ngw)");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    if (nconv_target <= 0) nconv_target = nb;
+    Run r{};
+    r.c = c;
+    r.st = pwk_stream(c);
+    r.dtype = dtype;
+    r.es = dtype == PW_C128 ? sizeof(double2) : sizeof(float2);
+    r.ngw = ngw;
+    r.nb = nb;
+    r.ldq = ngw;
+    const size_t blk = (size_t)ngw * nb * r.es;
+    RK(pwk_scratch(c, S_Q, 3 * blk, (void **)&r.Q));
+    RK(pwk_scratch(c, S_HQ, 3 * blk, (void **)&r.HQ));
+    RK(pwk_scratch(c, S_TMP1, 2 * blk, (void **)&r.T1));
+    RK(pwk_scratch(c, S_TMP2, 2 * blk, (void **)&r.T2));
+    const int n3 = 3 * nb;
+    const size_t s_nn = (size_t)nb * nb, s_33 = (size_t)n3 * n3;
+    RK(pwk_scratch(c, S_SMALL, (4 * s_nn + 2 * s_33 + (size_t)n3 * nb + 2 * n3) * sizeof(double2), (void **)&r.small));
+    r.eigw_bytes = pwk::eig_work_bytes(n3, nb) > pwk::eig_work_bytes(nb, nb) ? pwk::eig_work_bytes(n3, nb)
+                                                                             : pwk::eig_work_bytes(nb, nb);
+    RK(pwk_scratch(c, S_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, S_EIGSTAT, 64, (void **)&r.eigstat));
+    double2 *XHX = r.small, *M1 = XHX + s_nn, *Rinv = M1 + s_nn, *Sfin = Rinv + s_nn;
+    double2 *T3 = Sfin + s_nn, *G3 = T3 + s_33, *S3 = G3 + s_33;
+    double *lam = (double *)(S3 + (size_t)n3 * nb);
+
+    char *Xs = r.blk(r.Q, 0), *Ws = r.blk(r.Q, 1), *Ps = r.blk(r.Q, 2);
+    char *HXs = r.blk(r.HQ, 0), *HWs = r.blk(r.HQ, 1), *HPs = r.blk(r.HQ, 2);
+    // X -> Q[:, 0:nb]; HX = op_H(X)
+    CKR(c, cudaMemcpy2DAsync(Xs, r.ldq * r.es, X, ld * r.es, ngw * r.es, nb, cudaMemcpyDeviceToDevice, r.st));
+    RK(pw_apply(c, ik, ispin, dtype, Xs, HXs, r.ldq, nb, PW_OP_H));
+    std::vector<double> ev(nb), ev_old(nb, 0.0);
+    int it = 0;
+    const double SMALL = 10.0 * 2.220446049250313e-16;
+    (void)SMALL;
+    for (it = 1; it <= nitermax; ++it) {
+        // Rayleigh quotient XHX = X' HX and its eigenvalues (:85-86)
+        RK(gram(r, Xs, nb, HXs, nb, XHX, nb));
+        k_herm_from_upper<<<blocks_for(s_nn), 256, 0, r.st>>>(XHX, nb);
+        CKR(c, cudaMemcpyAsync(M1, XHX, s_nn * sizeof(double2), cudaMemcpyDeviceToDevice, r.st));
+        RK(eig(r, M1, nullptr, nb, nb, lam, nullptr));
+        CKR(c, cudaMemcpyAsync(ev.data(), lam, nb * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+        CKR(c, cudaStreamSynchronize(r.st));
+        int nconv = 0;
+        for (int i = 0; i < nb; ++i) {
+            if (!std::isfinite(ev[i])) return pwk_fail(c, PW_ERR_NAN, "non-finite Ritz value in LOBPCG");
+            if (std::fabs(ev[i] - ev_old[i]) < tol) ++nconv;
+            ev_old[i] = ev[i];
+        }
+        if (nconv >= nconv_target) break;
+        // R = HX - X XHX (:92), W = Kprec(R) (:123)
+        RK(copy_blk(r, Ws, HXs, nb));
+        k_scale_c128<<<blocks_for(s_nn), 256, 0, r.st>>>(XHX, M1, s_nn, -1.0);
+        RK(rot(r, Xs, nb, M1, nb, nb, Ws, 1));
+        RK(pw_kprec(c, ik, dtype, Ws, Ws, r.ldq, nb));
+        // HW = op_H(W); C = W'W = R^H R; W = W/R; HW = HW/R (:167-174)
+        RK(pw_apply(c, ik, ispin, dtype, Ws, HWs, r.ldq, nb, PW_OP_H));
+        if (dtype == PW_C64) {
+            // mixed precision: keep Q = [X W P] near-orthonormal so that its
+            // split-BF16 Gram stays positive definite: W -= X (X'W), and
+            // W -= P (P'W); HW follows with the same coefficients (H linear)
+            RK(project_out(r, Xs, HXs, Ws, HWs, M1));
+            if (it > 1) RK(project_out(r, Ps, HPs, Ws, HWs, M1));
+        }
+        RK(gram(r, Ws, nb, Ws, nb, M1, nb));
+        {
+            const int s = chol_rinv(r, M1, nb, Rinv);
+            // mixed precision: a W'W that is not positive definite means the
+            // residuals are at the noise floor of the FP32 blocks; stop here
+            // (the FP64 path keeps the reference's behaviour and reports it)
+            if (s == PW_ERR_NOT_POSDEF && dtype == PW_C64) {
+                ++r.restarts;
+                break;
+            }
+            RK(s);
+        }
+        RK(rot(r, Ws, nb, Rinv, nb, nb, r.T1, 0));
+        RK(rot(r, HWs, nb, Rinv, nb, nb, r.T2, 0));
+        RK(copy_blk(r, Ws, r.T1, nb));
+        RK(copy_blk(r, HWs, r.T2, nb));
+        // Rayleigh-Ritz on Q = [X W (P)] (:176-185)
+        const int nq = (it > 1) ? 3 * nb : 2 * nb;
+        RK(gram(r, r.Q, nq, r.HQ, nq, T3, nq));
+        RK(gram(r, r.Q, nq, r.Q, nq, G3, nq));
+        RK(eig(r, T3, G3, nq, nb, lam, S3));
+        // X = Q U, HX = HQ U  (:187-189) into the temporaries
+        RK(rot(r, r.Q, nq, S3, nq, nb, r.T1, 0));
+        RK(rot(r, r.HQ, nq, S3, nq, nb, r.T2, 0));
+        if (it > 1) {
+            // P = [W P] U[nb:3nb], HP = [HW HP] U[nb:3nb]; P = P/R, HP = HP/R (:190-199)
+            char *Pn = r.T1 + blk, *HPn = r.T2 + blk;
+            RK(rot(r, Ws, 2 * nb, S3 + nb, nq, nb, Pn, 0));
+            RK(rot(r, HWs, 2 * nb, S3 + nb, nq, nb, HPn, 0));
+            if (dtype == PW_C64) RK(project_out(r, r.T1, r.T2, Pn, HPn, M1));   // P -= Xnew (Xnew'P)
+            RK(gram(r, Pn, nb, Pn, nb, M1, nb));
+            const int s = chol_rinv(r, M1, nb, Rinv);
+            if (s == PW_ERR_NOT_POSDEF && dtype == PW_C64) {
+                // mixed precision: restart the conjugate directions, P = W
+                ++r.restarts;
+                RK(copy_blk(r, Ps, Ws, nb));
+                RK(copy_blk(r, HPs, HWs, nb));
+            } else {
+                RK(s);
+                RK(rot(r, Pn, nb, Rinv, nb, nb, Ps, 0));
+                RK(rot(r, HPn, nb, Rinv, nb, nb, HPs, 0));
+            }
+        } else {
+            // P = W, HP = HW (:201-202)
+            RK(copy_blk(r, Ps, Ws, nb));
+            RK(copy_blk(r, HPs, HWs, nb));
+        }
+        RK(copy_blk(r, Xs, r.T1, nb));
+        RK(copy_blk(r, HXs, r.T2, nb));
+    }
+    if (it > nitermax) it = nitermax;
+    // final Rayleigh-Ritz: S = X'HX, S = (S+S')/2, X = X Q (:214-217)
+    RK(gram(r, Xs, nb, HXs, nb, Sfin, nb));
+    k_herm_avg<<<blocks_for(s_nn), 256, 0, r.st>>>(Sfin, nb);
+    RK(eig(r, Sfin, nullptr, nb, nb, lam, M1));
+    RK(rot(r, Xs, nb, M1, nb, nb, r.T1, 0));
+    CKR(c, cudaMemcpy2DAsync(X, ld * r.es, r.T1, r.ldq * r.es, ngw * r.es, nb, cudaMemcpyDeviceToDevice, r.st));
+    CKR(c, cudaMemcpyAsync(evals, lam, nb * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+    CKR(c, cudaStreamSynchronize(r.st));
+    if (niter_out) *niter_out = it + 1000 * r.restarts;
+    return PW_OK;
+}
+
+// Host drop-in: X is the reference's host Matrix{ComplexF64} (Ngw x nb, ld).
+extern "C" int pw_lobpcg_host(pw_ctx *c, int ik, int ispin, int dtype, double *X, int64_t ld, int nb, double tol,
+                              int nitermax, int nconv, double *evals, int *niter) {
+    if (!c) return PW_ERR_ARG;
+    if (!X || nb <= 0 || ld <= 0) return pwk_fail(c, PW_ERR_ARG, "bad pw_lobpcg_host arguments");
+    if (dtype != PW_C128 && dtype != PW_C64) return pwk_fail(c, PW_ERR_ARG, "unknown dtype");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = pwk_stream(c);
+    const size_t n = (size_t)ld * nb;
+    void *d64 = nullptr, *d32 = nullptr;
+    RK(pwk_scratch(c, S_EIGSTAT + 1, n * sizeof(double2), &d64));
+    CKR(c, cudaMemcpyAsync(d64, X, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    void *dev = d64;
+    if (dtype == PW_C64) {
+        RK(pwk_scratch(c, S_EIGSTAT + 2, n * sizeof(float2), &d32));
+        CKR(c, pwk::convert_c128_to_c64((const double2 *)d64, (float2 *)d32, n, st));
+        dev = d32;
+    }
+    RK(pw_lobpcg(c, ik, ispin, dtype, dev, ld, nb, tol, nitermax, nconv, evals, niter));
+    if (dtype == PW_C64) CKR(c, pwk::convert_c64_to_c128((const float2 *)d32, (double2 *)d64, n, st));
+    CKR(c, cudaMemcpyAsync(X, d64, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    CKR(c, cudaStreamSynchronize(st));
+    return PW_OK;
+}

@@ -61,6 +61,13 @@ SIGNATURES = {
     "pw_calc_rhoe": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _vp, _i]),
     "pw_gram": (_i, [_vp, _i, _i64, _i, _i, _vp, _i64, _vp, _i64, _vp, _i64, _i]),
     "pw_rotate": (_i, [_vp, _i, _i64, _i, _i, _vp, _i64, _vp, _i64, _vp, _i64, _i]),
+    "pw_eigh": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "pw_lobpcg": (_i, [_vp, _i, _i, _i, _vp, _i64, _i, _d, _i, _i, _dp, C.POINTER(C.c_int)]),
+    "pw_lobpcg_host": (_i, [_vp, _i, _i, _i, _dp, _i64, _i, _d, _i, _i, _dp, C.POINTER(C.c_int)]),
+    "pw_set_density_sphere": (_i, [_vp, _i64, _i64p, _dp, _i]),
+    "pw_poisson": (_i, [_vp, _vp, _vp]),
+    "pw_update": (_i, [_vp, _vp, _vp, _vp, _vp, _dp]),
+    "pw_band_energies": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _dp]),
     "pw_op_H_host": (_i, [_vp, _i, _i, _dp, _dp, _i64, _i, _u, _i]),
     "pw_calc_rhoe_host": (_i, [_vp, _i, _dp, _i64, _i, _dp, _dp, _i, _i]),
     "pw_good_fft_order": (_i, [_i]),

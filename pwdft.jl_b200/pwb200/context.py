@@ -170,6 +170,62 @@ class Context:
                                     C.c_void_p(U.data_ptr()), U.stride(0), C.c_void_p(out.data_ptr()), out.stride(0),
                                     int(accumulate)))
 
+    def eigh(self, T, G=None, k=None, vectors=True):
+        """Lowest k eigenpairs of (T, G) on the device (FP64): T, G torch
+        complex128 (n, n) device tensors holding the column-major matrices
+        (i.e. the transposes); both are overwritten.  Returns (lam, S) with
+        S a (k, n) tensor (row j = eigenvector j)."""
+        import torch
+        n = T.shape[0]
+        k = n if k is None else k
+        lam = torch.empty(k, dtype=torch.float64, device=T.device)
+        S = torch.empty((k, n), dtype=torch.complex128, device=T.device) if vectors else None
+        self.use_torch_stream()
+        self._chk(self._L.pw_eigh(self.h, n, k, C.c_void_p(T.data_ptr()),
+                                  C.c_void_p(G.data_ptr()) if G is not None else None, C.c_void_p(lam.data_ptr()),
+                                  C.c_void_p(S.data_ptr()) if S is not None else None))
+        return lam, S
+
+    def lobpcg(self, ik, ispin, X, tol=1e-5, nitermax=100, nconv=0):
+        """diag_LOBPCG!: X (nb, Ngw) device block overwritten; returns (evals, niter)."""
+        nb, ld = X.shape
+        ev = np.zeros(nb)
+        nit = C.c_int(0)
+        self.use_torch_stream()
+        self._chk(self._L.pw_lobpcg(self.h, ik, ispin, dtype_code(X), C.c_void_p(X.data_ptr()), ld, nb, float(tol),
+                                    int(nitermax), int(nconv), _dptr(ev), C.byref(nit)))
+        return ev, nit.value
+
+    def set_density_sphere(self, idx_g2r, G2):
+        idx = np.ascontiguousarray(np.asarray(idx_g2r, dtype=np.int64))
+        g2 = np.ascontiguousarray(np.asarray(G2, dtype=np.float64))
+        self._keep_dens = (idx, g2)
+        self._chk(self._L.pw_set_density_sphere(self.h, len(idx), idx.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(g2), 0))
+
+    def poisson(self, rho, VH):
+        self.use_torch_stream()
+        self._chk(self._L.pw_poisson(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(VH.data_ptr())))
+
+    def update(self, rho, Vps, VH=None, Vxc=None):
+        """update!: V_loc := V_ps + V_H[rho] + V_xc[rho] on the device; returns
+        (sum V_H rho, sum V_ps rho, sum eps_xc rho)."""
+        E3 = np.zeros(3)
+        self.use_torch_stream()
+        self._chk(self._L.pw_update(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(Vps.data_ptr()),
+                                    C.c_void_p(VH.data_ptr()) if VH is not None else None,
+                                    C.c_void_p(Vxc.data_ptr()) if Vxc is not None else None, _dptr(E3)))
+        return E3
+
+    def band_energies(self, ik, psi, w):
+        """(E_kin, E_Ps_nloc) contributions of k-point ik with weights w = wk*Focc."""
+        nb, ld = psi.shape
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        E2 = np.zeros(2)
+        self.use_torch_stream()
+        self._chk(self._L.pw_band_energies(self.h, ik, dtype_code(psi), C.c_void_p(psi.data_ptr()), ld, nb, _dptr(w),
+                                           _dptr(E2)))
+        return E2
+
     # ---------------------------------------------------------- host drop-ins
     def op_H_host(self, ik, ispin, psi, Hpsi=None, ops=PW_OP_H, dtype=PW_C128):
         """The reference call on host arrays: psi (Ngw, nb) complex128."""

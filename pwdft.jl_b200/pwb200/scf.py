@@ -1,0 +1,179 @@
+"""KS_solve_SCF! with every step of the SCF iteration on the device.
+
+Mirrors KS_solve_SCF.jl:24-373 (Nspin = 1, LOBPCG, no smearing, Pulay or
+simple density mixing):
+  ethr schedule            KS_solve_SCF.jl:177-185
+  diag_LOBPCG!             pw_lobpcg per k-point          (device)
+  calc_rhoe!               pw_calc_rhoe                   (device)
+  mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
+  rho >= eps clamp         KS_solve_SCF.jl:277-281        (device)
+  update!                  pw_update (Poisson, VWN, V_tot) (device)
+  calc_energies            pw_update sums + pw_band_energies (device, FP64)
+  convergence              |dE| < etot_conv_thr twice      (host scalar)
+The starting density (guess_rhoe.jl) and E_NN (Ewald) are computed once on
+the host, as set-up.
+
+precision = "fp64" runs the reference's FP64 path; "mixed" runs FP32
+blocks with split-BF16x3 tensor-core contractions until |dE| falls below
+`fp64_switch`, then converts psi to complex128 and finishes in FP64
+(iterative refinement).
+"""
+import time
+
+import numpy as np
+
+from .system import kpoint_grid, guess_rhoe, ewald_energy
+
+EPS = np.finfo(np.float64).eps
+
+
+def occupations(Nelectrons, Nstates, Nkpt):
+    """Electrons.jl:120-262 for Nspin = 1 without smearing."""
+    nocc = int(round(Nelectrons / 2))
+    if nocc * 2 < Nelectrons:
+        nocc += 1
+    F = np.zeros((Nstates, Nkpt))
+    F[:nocc - 1, :] = 2.0
+    F[nocc - 1, :] = 1.0 if int(round(Nelectrons)) % 2 == 1 else 2.0
+    return F, nocc
+
+
+def rand_psiks(Ham, Nstates, seed, dtype):
+    """rand_BlochWavefunc (gen_wavefunc.jl:75-92): ortho_sqrt(rand(ComplexF64))."""
+    import torch
+    rng = np.random.default_rng(seed)
+    out = []
+    for ik in range(Ham.basis.Nkpt):
+        ngw = Ham.basis.Ngw[ik]
+        psi = rng.random((ngw, Nstates)) + 1j * rng.random((ngw, Nstates))
+        w, U = np.linalg.eigh(psi.conj().T @ psi)
+        psi = psi @ ((U / np.sqrt(w)) @ U.conj().T)
+        out.append(torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{Ham.ctx.device}").to(dtype).contiguous())
+    return out
+
+
+class PulayMixer:
+    """mix_pulay.jl:1-41 on device vectors."""
+
+    def __init__(self, N, beta, mixdim, device):
+        import torch
+        self.beta, self.mixdim = beta, mixdim
+        self.X = torch.zeros((mixdim, N), dtype=torch.float64, device=device)
+        self.F = torch.zeros((mixdim, N), dtype=torch.float64, device=device)
+        self.x_old = None
+        self.f_old = None
+
+    def __call__(self, x, gx, it):
+        import torch
+        f = gx - x
+        if it == 1:
+            dx, df = x.clone(), f.clone()
+        else:
+            dx, df = x - self.x_old, f - self.f_old
+        if it <= self.mixdim:
+            self.X[it - 1] = dx
+            self.F[it - 1] = df
+        else:
+            self.X = torch.roll(self.X, -1, dims=0)
+            self.F = torch.roll(self.F, -1, dims=0)
+            self.X[-1] = dx
+            self.F[-1] = df
+        self.x_old = x.clone()
+        self.f_old = f.clone()
+        if it > self.mixdim:
+            FtF = (self.F @ self.F.T).cpu().numpy()
+            Ftf = (self.F @ f).cpu().numpy()
+            c = torch.from_numpy(np.linalg.inv(FtF) @ Ftf).to(x.device)
+            addv = (self.X + self.beta * self.F).T @ c
+            return x + self.beta * f - addv
+        return x + self.beta * f
+
+
+def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
+                 ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
+                 verbose=False, lobpcg_maxiter=100):
+    """Runs the SCF loop; returns a dict with energies, eigenvalues, timings
+    and the per-iteration log."""
+    import torch
+    ctx = Ham.ctx
+    b = Ham.basis
+    dev = f"cuda:{ctx.device}"
+    N = b.Npoints
+    dVol = b.CellVolume / N
+    Nel = Ham.Nelectrons
+    if Nstates is None:
+        Nstates = int(round(Nel / 2)) + (1 if int(round(Nel)) % 2 else 0)
+    Focc, Nocc = occupations(Nel, Nstates, b.Nkpt)
+    wk = Ham.wk
+    if not getattr(Ham, "_density_set", False):
+        ctx.set_density_sphere(b.idx_g2r, b.G2)
+        Ham._density_set = True
+    mixed = precision == "mixed"
+    dt = torch.complex64 if mixed else torch.complex128
+    if psiks is None:
+        psiks = rand_psiks(Ham, Nstates, seed, dt)
+    else:
+        psiks = [p.to(dt).contiguous() for p in psiks]
+    Vps = torch.from_numpy(Ham.V_Ps_loc).to(dev)
+    rho = torch.from_numpy(guess_rhoe(Ham.system, b, Ham.pspots, Nel)).to(dev)
+    ctx.update(rho, Vps)
+    E_NN = ewald_energy(Ham.system.LatVecs, Ham.system.positions, Ham.Zvals[Ham.system.atm2species])
+    mixer = PulayMixer(N, betamix, mixdim, dev) if mix_method == "pulay" else None
+    rho_new = torch.zeros(N, dtype=torch.float64, device=dev)
+    Etot_old, Nconv, ethr = 0.0, 0, 0.1
+    log = []
+    evals = np.zeros((Nstates, b.Nkpt))
+    t_start = time.perf_counter()
+    t_diag = t_rho = t_upd = 0.0
+    switched_at = None
+    E = {}
+    for it in range(1, NiterMax + 1):
+        ethr = 0.1 if it == 1 else (0.01 if it == 2 else max(ethr / 5.0, ethr_evals_last))
+        t0 = time.perf_counter()
+        nit = []
+        for ik in range(b.Nkpt):
+            ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
+            evals[:, ik] = ev
+            nit.append(n)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for ik in range(b.Nkpt):
+            ctx.calc_rhoe(ik, psiks[ik], wk[ik] * Focc[:, ik], rho_new, accumulate=(ik > 0))
+        diffRhoe = float(torch.sum(torch.abs(rho_new - rho)).item()) / N
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if mixer is not None:
+            rho = mixer(rho, rho_new, it)
+        else:
+            rho = betamix * rho_new + (1 - betamix) * rho
+        rho = torch.clamp(rho, min=EPS)
+        sums = ctx.update(rho, Vps)
+        Ek = En = 0.0
+        for ik in range(b.Nkpt):
+            e2 = ctx.band_energies(ik, psiks[ik], wk[ik] * Focc[:, ik])
+            Ek += e2[0]
+            En += e2[1]
+        E = {"Kinetic": Ek, "Ps_loc": sums[1] * dVol, "Ps_nloc": En, "Hartree": 0.5 * sums[0] * dVol,
+             "XC": sums[2] * dVol, "NN": E_NN}
+        E["Total"] = sum(E.values())
+        t3 = time.perf_counter()
+        t_diag += t1 - t0
+        t_rho += t2 - t1
+        t_upd += t3 - t2
+        diffE = abs(E["Total"] - Etot_old)
+        log.append((it, E["Total"], diffE, diffRhoe, int(np.max(np.array(nit) % 1000)), "c64" if mixed else "c128"))
+        if verbose:
+            print("SCF: %5d %18.10f %12.5e %12.5e  %s" % (it, E["Total"], diffE, diffRhoe, log[-1][-1]), flush=True)
+        Nconv = Nconv + 1 if diffE < etot_conv_thr else 0
+        if Nconv >= 2:
+            break
+        if mixed and diffE < fp64_switch and it > 2:
+            # iterative refinement: finish in FP64
+            psiks = [p.to(torch.complex128).contiguous() for p in psiks]
+            mixed = False
+            switched_at = it
+        Etot_old = E["Total"]
+    torch.cuda.synchronize()
+    return {"energies": E, "evals": evals, "iterations": len(log), "log": log, "time_s": time.perf_counter() - t_start,
+            "time_diag_s": t_diag, "time_rhoe_s": t_rho, "time_update_s": t_upd, "switched_to_fp64_at": switched_at,
+            "psiks": psiks, "rho": rho}

@@ -230,6 +230,100 @@ def projectors(system, basis, pspots, ik):
     return beta, trip
 
 
+ZATOMS = {"H": 1, "He": 2, "Li": 3, "C": 6, "N": 7, "O": 8, "Na": 11, "Mg": 12, "Al": 13, "Si": 14, "P": 15,
+          "S": 16, "Cl": 17, "Ga": 31, "Ge": 32}
+
+
+def kpoint_grid(LatVecs, mesh, time_reversal=True):
+    """Gamma-centred Monkhorst-Pack grid reduced by k ~ -k only
+    (KPoints.jl:120-262 with the identity as the only rotation).
+    Returns Cartesian k (3, Nk) and weights summing to one."""
+    n1, n2, n3 = mesh
+    frac = np.array([[i / n1, j / n2, k / n3] for i in range(n1) for j in range(n2) for k in range(n3)])
+    frac = frac - np.round(frac)
+    keys = {}
+    order, weight = [], []
+    for f in frac:
+        key = tuple(np.round(f * np.array(mesh)).astype(int) % np.array(mesh))
+        mkey = tuple((-np.array(key)) % np.array(mesh))
+        if key in keys:
+            weight[keys[key]] += 1.0
+        elif time_reversal and mkey in keys:
+            weight[keys[mkey]] += 1.0
+        else:
+            keys[key] = len(order)
+            order.append(f)
+            weight.append(1.0)
+    RecVecs = 2 * np.pi * np.linalg.inv(np.ascontiguousarray(np.asarray(LatVecs).T))
+    k = RecVecs @ np.array(order).T
+    w = np.array(weight)
+    return k, w / w.sum()
+
+
+def atmlength(zion, znucl):
+    """Default decay length of the Gaussian starting density (guess_rhoe.jl:208-308)."""
+    coreel, nval = znucl - zion, int(round(zion))
+    tables = [(0.5, [0.6, 0.4, 0.3, 0.25], 0.2), (2.5, [1.8, 1.4, 1.0, 0.7, 0.6, 0.5, 0.4, 0.35], 0.3),
+              (10.5, [2.0, 1.6, 1.25, 1.1, 1.0, 0.9, 0.8, 0.7, 0.7, 0.7], 0.6),
+              (12.5, [1.9, 1.5, 1.15, 1.0, 0.9, 0.8, 0.7, 0.6, 0.6, 0.6], 0.5),
+              (18.5, [2.0, 1.8, 1.5, 1.2, 1.0, 0.9, 0.85, 0.8, 0.75, 0.7, 0.65, 0.65], 0.6),
+              (28.5, [1.5, 1.25, 1.15, 1.05, 1.00, 0.95, 0.95, 0.9, 0.9, 0.85, 0.85, 0.80, 0.8, 0.75], 0.7),
+              (36.5, [2.0, 2.00, 1.60, 1.40, 1.25, 1.10, 1.00, 0.95, 0.90, 0.85, 0.80, 0.75], 0.7),
+              (1e9, [2.0, 2.00, 1.55, 1.25, 1.15, 1.10, 1.05, 1.0, 0.95, 0.9, 0.85, 0.85], 0.8)]
+    if nval == 0:
+        return 0.0
+    for lim, tab, dflt in tables:
+        if coreel < lim:
+            return tab[nval - 1] if nval <= len(tab) else dflt
+
+
+def guess_rhoe(system, basis, pspots, Nelectrons):
+    """Superposition of atomic Gaussians, normalised to Nelectrons (guess_rhoe.jl:1-38)."""
+    rhoG = np.zeros(basis.Npoints, dtype=np.complex128)
+    for ia in range(system.positions.shape[1]):
+        psp = pspots[system.atm2species[ia]]
+        L = atmlength(float(psp.zval), float(ZATOMS[psp.atsymb]))
+        GX = basis.G @ system.positions[:, ia]
+        rhoG[basis.idx_g2r] += psp.zval * (np.cos(GX) - 1j * np.sin(GX)) * np.exp(-basis.G2 * L * L)
+    N1, N2, N3 = basis.Ns
+    rho = np.fft.ifftn(rhoG.reshape(N3, N2, N1)).real.ravel()
+    return rho * Nelectrons / (rho.sum() * basis.CellVolume / basis.Npoints)
+
+
+def ewald_energy(LatVecs, positions, Z):
+    """Ion-ion (Ewald) energy in Hartree (calc_E_NN.jl:60-172)."""
+    from scipy.special import erfc
+    t = [LatVecs[:, i] for i in range(3)]
+    Omega = abs(np.linalg.det(LatVecs))
+    R = 2 * np.pi * np.linalg.inv(LatVecs.T)
+    g = [R[:, i] for i in range(3)]
+    gcut, ebsl = 2.0, 1e-8
+    gexp = -math.log(ebsl)
+    eta = math.sqrt(gcut * gcut / gexp) / 2
+    e = -2 * eta * float(np.sum(Z ** 2)) / math.sqrt(math.pi) - math.pi * float(np.sum(Z)) ** 2 / (Omega * eta ** 2)
+    tmax = math.sqrt(0.5 * gexp) / eta
+    m = [int(round(tmax / np.linalg.norm(v) + 1.5)) for v in t]
+    ii, jj, kk = [a.ravel() for a in np.meshgrid(*[np.arange(-q, q + 1) for q in m], indexing="ij")]
+    T = np.outer(t[0], ii) + np.outer(t[1], jj) + np.outer(t[2], kk)
+    origin = (np.abs(ii) + np.abs(jj) + np.abs(kk)) == 0
+    nat = positions.shape[1]
+    for a in range(nat):
+        for b in range(nat):
+            r = np.sqrt((((positions[:, a] - positions[:, b])[:, None] - T) ** 2).sum(axis=0))
+            keep = ~origin if a == b else np.ones_like(origin)
+            e += Z[a] * Z[b] * float(np.sum(erfc(eta * r[keep]) / r[keep]))
+    m = [int(round(gcut / np.linalg.norm(v) + 1.5)) for v in g]
+    ii, jj, kk = [a.ravel() for a in np.meshgrid(*[np.arange(-q, q + 1) for q in m], indexing="ij")]
+    keep = (np.abs(ii) + np.abs(jj) + np.abs(kk)) != 0
+    Gv = (np.outer(g[0], ii) + np.outer(g[1], jj) + np.outer(g[2], kk))[:, keep]
+    G2 = (Gv ** 2).sum(axis=0)
+    xg = 4 * np.pi / Omega * np.exp(-0.25 * G2 / eta ** 2) / G2
+    for a in range(nat):
+        for b in range(nat):
+            e += float(np.sum(xg * Z[a] * Z[b] * np.cos((positions[:, a] - positions[:, b]) @ Gv)))
+    return 0.5 * e
+
+
 class Hamiltonian:
     """Device-resident operator data for one geometry (mirror of the parts
     of PWDFT.jl's Hamiltonian that op_H / calc_rhoe read), plus the hidden

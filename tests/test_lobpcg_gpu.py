@@ -1,0 +1,105 @@
+"""The device eigensolvers against SciPy and the FP64 oracle.
+
+  pw_eigh    eigen(T, G) / eigvals(XHX) of diag_LOBPCG.jl:86,185,216
+             (LAPACK zhegv/zheev in the reference) vs scipy.linalg.eigh
+  pw_lobpcg  diag_LOBPCG! (diag_LOBPCG.jl:51-225) vs the exact spectrum of
+             the oracle's dense Hamiltonian and vs the oracle's own LOBPCG
+Tolerances: FP64 eigenvalues 1e-9 Ha (tol 1e-10), mixed 5e-5 Ha (tol 1e-5,
+the SCF's floor ethr_evals_last, KS_solve_SCF.jl:42).
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from conftest import cuda_ok
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx_fcc():
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import pwb200
+    from oracle import systems
+    H = systems.Ham_Si_fcc(meshk=(2, 2, 2), extra_states=4)
+    rng = np.random.default_rng(3)
+    H.V_Total = H.V_Ps_loc + 0.05 * np.cos(np.arange(H.pw.Npoints) * 0.37)
+    pw = H.pw
+    ctx = pwb200.Context(pw.Ns, pw.CellVolume, pw.gvecw.idx_gw2r, [pw.Gk2(k) for k in range(pw.kpoints.Nkpt)])
+    ctx.set_vloc(H.V_Total)
+    for ik in range(pw.kpoints.Nkpt):
+        ctx.set_nonlocal(ik, H.betaNL[ik])
+    ctx.set_nonlocal_coef(H.nl_triplets)
+    yield H, ctx, rng
+    ctx.close()
+
+
+def dev_colmajor(A):
+    """A column-major n x n matrix as a torch (n, n) tensor (its transpose)."""
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+
+
+@pytest.mark.parametrize("n,k", [(40, 40), (150, 50), (333, 111)])
+def test_eigh_generalized(ctx_fcc, n, k):
+    H, ctx, rng = ctx_fcc
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    ev = np.sort(rng.standard_normal(n))
+    ev[3:6] = ev[3]            # a 3-fold and a 2-fold degeneracy
+    ev[10:12] = ev[10]
+    T = (Q * ev) @ Q.conj().T
+    B = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    G = B @ B.conj().T / n + np.eye(n)
+    ref = sla.eigh(T, G, eigvals_only=True)[:k]
+    Tt, Gt = dev_colmajor(np.triu(T)), dev_colmajor(np.triu(G))   # only the upper triangles are read
+    lam, S = ctx.eigh(Tt, Gt, k=k)
+    lam = lam.cpu().numpy()
+    S = S.cpu().numpy().T            # n x k
+    scale = np.abs(ev).max()
+    assert np.abs(lam - ref).max() < 1e-11 * scale
+    assert np.abs(T @ S - G @ S * lam).max() < 1e-10 * scale
+    assert np.abs(S.conj().T @ G @ S - np.eye(k)).max() < 1e-10
+
+
+def test_eigh_standard_and_errors(ctx_fcc):
+    import torch
+    import pwb200
+    H, ctx, rng = ctx_fcc
+    n = 64
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    A = A + A.conj().T
+    lam, _ = ctx.eigh(dev_colmajor(A), None, k=n, vectors=False)
+    assert np.abs(lam.cpu().numpy() - np.linalg.eigvalsh(A)).max() < 1e-11 * np.abs(A).max()
+    Gbad = -np.eye(n, dtype=np.complex128)
+    with pytest.raises(pwb200.PWError) as e:
+        ctx.eigh(dev_colmajor(A), dev_colmajor(Gbad), k=4)
+    assert e.value.status == pwb200._lib.PW_ERR_NOT_POSDEF
+    ctx.check_device()
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_lobpcg_matches_exact_spectrum(ctx_fcc, prec):
+    import torch
+    from oracle import ops, lobpcg
+    H, ctx, rng = ctx_fcc
+    ik = 1
+    ngw = H.pw.gvecw.Ngw[ik]
+    nb = 8
+    Hd = ops.op_H(H, np.eye(ngw, dtype=np.complex128), ik)       # dense H(k)
+    exact = np.linalg.eigvalsh(0.5 * (Hd + Hd.conj().T))[:nb]
+    X0 = lobpcg.ortho_sqrt(rng.standard_normal((ngw, nb)) + 1j * rng.standard_normal((ngw, nb)))
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    X = torch.from_numpy(np.ascontiguousarray(X0.T)).cuda().to(dt).contiguous()
+    tol = 1e-10 if prec == "c128" else 1e-5
+    ev, nit = ctx.lobpcg(ik, 0, X, tol=tol, nitermax=300)
+    bound = 1e-9 if prec == "c128" else 5e-5
+    assert np.abs(ev - exact).max() < bound, (ev - exact, nit)
+    # the oracle's LOBPCG from the same start converges to the same values
+    # (two independently converged runs: each is within its own tolerance)
+    Xo = X0.copy()
+    evo = lobpcg.diag_LOBPCG_k(H, Xo, ik, tol=tol, NiterMax=300)
+    assert np.abs(ev - evo).max() < (1e-9 if prec == "c128" else 2e-4)
+    # returned vectors are orthonormal Ritz vectors
+    Xr = X.cpu().numpy().T.astype(np.complex128)
+    assert np.abs(Xr.conj().T @ Xr - np.eye(nb)).max() < (1e-10 if prec == "c128" else 1e-5)

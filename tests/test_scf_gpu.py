@@ -1,0 +1,46 @@
+"""KS_solve_SCF! on the device (pwb200.scf) against the reference's golden
+total energy and the FP64 oracle's converged SCF.
+
+  Si fcc, GTH-Pade, LDA, ecutwfc 15 Ha, 3x3x3 MP (time reversal: 14 k),
+  Pulay mixing beta = 0.2, etot_conv_thr 1e-8:
+    FP64 path:  |Etot - ABINIT| < 1e-5 (test/validations_old/Si_fcc.jl:15)
+                |Etot - oracle| < 2e-7, components within 2e-6
+    mixed path (FP64 switch at |dE| < 1e-5): |Etot - ABINIT| < 1e-5
+"""
+import numpy as np
+import pytest
+
+from conftest import cuda_ok
+
+pytestmark = pytest.mark.gpu
+ABINIT = -7.9110087934
+
+
+@pytest.fixture(scope="module")
+def si_fcc_gpu():
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import pwb200
+    from pwb200.system import kpoint_grid
+    from oracle import systems
+    Ho = systems.Ham_Si_fcc(meshk=(1, 1, 1))
+    k, w = kpoint_grid(Ho.atoms.LatVecs, (3, 3, 3))
+    sysm = pwb200.System(["Si", "Si"], Ho.atoms.positions, Ho.atoms.LatVecs)
+    H = pwb200.Hamiltonian(sysm, [systems.psp("Si-q4.gth")], 15.0, kpts=k, wk=w)
+    yield H
+    H.ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_scf_si_fcc(si_fcc_gpu, si_fcc_scf, precision):
+    from pwb200 import scf
+    res = scf.KS_solve_SCF(si_fcc_gpu, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-8, precision=precision)
+    E = res["energies"]
+    assert abs(E["Total"] - ABINIT) < 1e-5, res["log"][-3:]
+    if precision == "fp64":
+        _, Eo, _, _ = si_fcc_scf
+        assert abs(E["Total"] - Eo["Total"]) < 2e-7
+        for key in ("Kinetic", "Ps_loc", "Ps_nloc", "Hartree", "XC", "NN"):
+            assert abs(E[key] - Eo[key]) < 2e-6, key
+    else:
+        assert res["switched_to_fp64_at"] is not None
