@@ -193,6 +193,11 @@ int pw_update(pw_ctx *ctx, const double *rho, const double *Vps, double *VH,
 int pw_band_energies(pw_ctx *ctx, int ik, int dtype, const void *psi,
                      int64_t ld, int nb, const double *w, double *E2);
 
+/* ortho_sqrt!(psi) (ortho_sqrt.jl:1-11): psi := psi * inv(sqrt(psi'psi)),
+ * psi device Ngw x nb (ld), in place. */
+int pw_ortho_sqrt(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw,
+                  int nb);
+
 /* ---- host drop-ins (the reference's Julia arrays) ------------------- */
 
 /* op_H!(Ham, psi, Hpsi) and friends on host ComplexF64 arrays; compute

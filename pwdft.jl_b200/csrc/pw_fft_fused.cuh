@@ -1,0 +1,143 @@
+// Line FFTs with composite radices held entirely in registers.
+//
+// Same in-place Stockham stages and warp-group organisation as
+// pw_fft_tmpl.cuh, but a stage may use a composite radix R = R1*R2 whose
+// R-point DFT runs inside one thread (Cooley-Tukey split: R2 DFTs of size R1,
+// twiddles W_R^(n2 k1), R1 DFTs of size R2).  Fewer stages means fewer
+// shared-memory round trips per line: 75 = 15*5 and 120 = 24*5 take two
+// passes instead of three, 27 takes one.
+#pragma once
+#include "pw_fft.cuh"
+
+namespace pwf {
+
+template <typename T, int R> struct Dft;
+
+// radices with direct formulas
+template <typename T> struct Dft<T, 2> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 2>::run(v, s); } };
+template <typename T> struct Dft<T, 3> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 3>::run(v, s); } };
+template <typename T> struct Dft<T, 4> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 4>::run(v, s); } };
+template <typename T> struct Dft<T, 5> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 5>::run(v, s); } };
+template <typename T> struct Dft<T, 8> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 8>::run(v, s); } };
+
+// R = R1*R2 in registers.  tw[m * step] = exp(-2 pi i m / R) for m < R.
+template <typename T, int R1, int R2> struct CompDft {
+    static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
+        constexpr int R = R1 * R2;
+        Cx<T> a[R];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) {
+            Cx<T> t[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
+            Dft<T, R1>::run(t, s, tw, step * R2);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) {
+                if (n2 * k1 != 0) {
+                    Cx<T> w = tw[((n2 * k1) % R) * step];
+                    if (s > 0) w.y = -w.y;
+                    t[k1] = cmul(t[k1], w);
+                }
+                a[n2 * R1 + k1] = t[k1];
+            }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+            Cx<T> t[R2];
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) t[n2] = a[n2 * R1 + k1];
+            Dft<T, R2>::run(t, s, tw, step * R1);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = t[k2];
+        }
+    }
+};
+template <typename T> struct Dft<T, 9> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 3, 3>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 15> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 3, 5>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 24> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 8, 3>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 25> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 5, 5>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 27> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 9, 3>::run(v, s, tw, st); } };
+
+// Fused plans: radices per stage (product = N).
+template <int N> struct FPlan;
+template <> struct FPlan<27> { static constexpr int nst = 1; static __host__ __device__ constexpr int r(int) { return 27; } };
+template <> struct FPlan<75> { static constexpr int nst = 2; static __host__ __device__ constexpr int r(int s) { return s == 0 ? 15 : 5; } };
+template <> struct FPlan<120> { static constexpr int nst = 2; static __host__ __device__ constexpr int r(int s) { return s == 0 ? 24 : 5; } };
+
+template <int N> __host__ __device__ constexpr int fp_ns(int s) {
+    int p = 1;
+    for (int i = 0; i < s; ++i) p *= FPlan<N>::r(i);
+    return p;
+}
+// lines per warp group: the stage with the fewest butterflies per line fills 32 lanes
+template <int N> __host__ __device__ constexpr int fp_group() {
+    int mn = N;
+    for (int s = 0; s < FPlan<N>::nst; ++s) {
+        const int nbf = N / FPlan<N>::r(s);
+        mn = nbf < mn ? nbf : mn;
+    }
+    return 32 / mn > 0 ? 32 / mn : 1;
+}
+
+template <typename T, int N, int S, bool JFAST>
+__device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int ls, const Cx<T> *tw, int sign, int lane) {
+    constexpr int R = FPlan<N>::r(S);
+    constexpr int NS = fp_ns<N>(S);
+    constexpr int NBF = N / R;
+    constexpr int G = fp_group<N>();
+    constexpr int MAXB = (G * NBF + 31) / 32;
+    constexpr int TWS = N / (NS * R);
+    const int total = nl * NBF;
+    const T sg = (T)sign;
+    Cx<T> v[MAXB][R];
+#pragma unroll
+    for (int t = 0; t < MAXB; ++t) {
+        const int id = lane + 32 * t;
+        if (id < total) {
+            const int line = JFAST ? l0 + id / NBF : l0 + id % nl;
+            const int j = JFAST ? id % NBF : id / nl;
+            const int jm = j % NS;
+            const Cx<T> *p = buf + line * ls + j * es;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[t][r] = p[r * NBF * es];
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    Cx<T> w = tw[r * jm * TWS];
+                    if (sign > 0) w.y = -w.y;
+                    v[t][r] = cmul(v[t][r], w);
+                }
+            }
+            Dft<T, R>::run(v[t], sg, tw, N / R);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < MAXB; ++t) {
+        const int id = lane + 32 * t;
+        if (id < total) {
+            const int line = JFAST ? l0 + id / NBF : l0 + id % nl;
+            const int j = JFAST ? id % NBF : id / nl;
+            const int jm = j % NS;
+            Cx<T> *q = buf + line * ls + ((j / NS) * NS * R + jm) * es;
+#pragma unroll
+            for (int r = 0; r < R; ++r) q[r * NS * es] = v[t][r];
+        }
+    }
+    __syncwarp();
+    if constexpr (S + 1 < FPlan<N>::nst) fstage<T, N, S + 1, JFAST>(buf, l0, nl, es, ls, tw, sign, lane);
+}
+
+// All lines [0, nlines) of length N; ends with __syncthreads().
+template <typename T, int N, bool JFAST>
+__device__ __forceinline__ void lines(Cx<T> *buf, int nlines, int es, int ls, const Cx<T> *tw, int sign) {
+    constexpr int G = fp_group<N>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int l0 = warp * G; l0 < nlines; l0 += nw * G) {
+        const int nl = min(G, nlines - l0);
+        fstage<T, N, 0, JFAST>(buf, l0, nl, es, ls, tw, sign, lane);
+    }
+    __syncthreads();
+}
+
+}  // namespace pwf

@@ -23,6 +23,7 @@
 // written/read twice, V once per plane batch (L2-resident across bands).
 #include "pw_fft.cuh"
 #include "pw_fft_tmpl.cuh"
+#include "pw_fft_fused.cuh"
 
 namespace pwk {
 
@@ -249,8 +250,18 @@ __global__ void k_zero(Cx<T> *p, int Ngw, int nb, int64_t ld) {
 // The same passes with the line lengths as template constants (see
 // pw_fft_tmpl.cuh); used for the grid sizes listed in FIXED_SIZES below,
 // the run-time kernels above serve every other {2,3,5}-smooth size.
+// FP32 lines use the register-fused composite radices (fewer shared-memory
+// passes); FP64 lines keep the 2/3/4/5/8 stages (register pressure).
+template <typename T, int N, bool JF>
+__device__ __forceinline__ void line_fft(Cx<T> *buf, int nl, int es, int ls, const Cx<T> *tw, int sign) {
+    if constexpr (sizeof(T) == 4)
+        pwf::lines<T, N, JF>(buf, nl, es, ls, tw, sign);
+    else
+        pwt::lines<T, N, MaxV<T>::v, JF>(buf, nl, es, ls, tw, sign);
+}
+
 template <typename T> struct MinBlocks;
-template <> struct MinBlocks<float> { static constexpr int v = 3; };
+template <> struct MinBlocks<float> { static constexpr int v = 2; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
 
 template <typename T, int N3>
@@ -271,7 +282,7 @@ kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, 
     const Cx<T> *ps = psi + (size_t)b * ld;
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0] = ps[kp.ent_igw[e]];
     __syncthreads();
-    pwt::lines<T, N3, MaxV<T>::v, false>(Z, cn, Cg, 1, tw, +1);
+    line_fft<T, N3, false>(Z, cn, Cg, 1, tw, +1);
     Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol + c0;
     for (int kz = warp; kz < N3; kz += nw)
         for (int cl = lane; cl < cn; cl += 32) Ab[(size_t)kz * kp.Ncol + cl] = Z[kz * Cg + cl];
@@ -293,7 +304,7 @@ kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, co
     for (int kz = warp; kz < N3; kz += nw)
         for (int cl = lane; cl < cn; cl += 32) Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + cl];
     __syncthreads();
-    pwt::lines<T, N3, MaxV<T>::v, false>(Z, cn, Cg, 1, tw, -1);
+    line_fft<T, N3, false>(Z, cn, Cg, 1, tw, -1);
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
     const Cx<T> *ps = psi + (size_t)b * ld;
     Cx<T> *hs = Hpsi + (size_t)b * ld;
@@ -319,7 +330,7 @@ __device__ __forceinline__ void plane_to_real(const KPlan &kp, Cx<T> *S, Cx<T> *
         for (int jl = lane; jl < jc; jl += 32) X[jl * N1 + x] = S[ia * N2 + j0 + jl];
     }
     __syncthreads();
-    pwt::lines<T, N1, MaxV<T>::v, true>(X, jc, 1, N1, tx, +1);
+    line_fft<T, N1, true>(X, jc, 1, N1, tx, +1);
 }
 
 template <typename T, int N1, int N2>
@@ -341,21 +352,21 @@ kf_plane_vloc(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__
     Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
     for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
     __syncthreads();
-    pwt::lines<T, N2, MaxV<T>::v, true>(S, Nxa, 1, N2, ty, +1);
+    line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);
     const T *Vp = Vr + (size_t)kz * N1 * N2;
     for (int j0 = 0; j0 < N2; j0 += Jc) {
         const int jc = min(Jc, N2 - j0);
         plane_to_real<T, N1, N2>(kp, S, X, tx, j0, jc);
         for (int i = threadIdx.x; i < jc * N1; i += blockDim.x) X[i] = cscale(X[i], Vp[j0 * N1 + i]);
         __syncthreads();
-        pwt::lines<T, N1, MaxV<T>::v, true>(X, jc, 1, N1, tx, -1);
+        line_fft<T, N1, true>(X, jc, 1, N1, tx, -1);
         for (int ia = warp; ia < Nxa; ia += nw) {
             const int x = kp.xa[ia];
             for (int jl = lane; jl < jc; jl += 32) S[ia * N2 + j0 + jl] = X[jl * N1 + x];
         }
         __syncthreads();
     }
-    pwt::lines<T, N2, MaxV<T>::v, true>(S, Nxa, 1, N2, ty, -1);
+    line_fft<T, N2, true>(S, Nxa, 1, N2, ty, -1);
     for (int c = threadIdx.x; c < Ncol; c += blockDim.x) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
 }
 
@@ -383,7 +394,7 @@ kf_plane_rho(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ 
         const Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
         for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
         __syncthreads();
-        pwt::lines<T, N2, MaxV<T>::v, true>(S, Nxa, 1, N2, ty, +1);
+        line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);
         for (int j0 = 0; j0 < N2; j0 += Jc) {
             const int jc = min(Jc, N2 - j0);
             plane_to_real<T, N1, N2>(kp, S, X, tx, j0, jc);

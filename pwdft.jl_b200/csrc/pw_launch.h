@@ -6,6 +6,22 @@
 
 namespace pwk {
 
+// Grow-only scratch slots of a context (pwk_scratch).  One list for every
+// file so no two callers share a slot by accident; a slot is only reused by
+// calls that never run at the same time as its other owner.
+enum ScratchSlot {
+    // update!: Poisson, XC, V_tot, reductions
+    SL_UPD_A = 8, SL_UPD_RHOG, SL_UPD_VH, SL_UPD_VXC, SL_UPD_EPS, SL_UPD_VTOT, SL_UPD_RED,
+    // band energies
+    SL_BAND_W, SL_BAND_RED,
+    // LOBPCG / generalized eigenproblem / ortho_sqrt
+    SL_LOB_Q, SL_LOB_HQ, SL_LOB_TMP1, SL_LOB_TMP2, SL_LOB_SMALL, SL_LOB_EIGW, SL_LOB_EIGSTAT,
+    // host drop-in staging of pw_lobpcg_host
+    SL_HOST_C128, SL_HOST_C64,
+    SL_COUNT
+};
+static_assert(SL_COUNT <= 32, "pw_ctx holds 32 scratch slots");
+
 // Everything a pruned-FFT launch needs for one k-point and one precision.
 struct FftLaunch {
     KPlan kp;

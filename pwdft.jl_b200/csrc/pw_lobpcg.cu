@@ -37,7 +37,6 @@ void pwk_count_launches(pw_ctx *c, int n);
 
 namespace {
 
-enum Slot { S_Q = 16, S_HQ, S_TMP1, S_TMP2, S_SMALL, S_EIGW, S_EIGSTAT };
 
 __global__ void k_scale_c128(const double2 *in, double2 *out, size_t n, double s) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -140,12 +139,13 @@ __global__ void k_neg_c128(double2 *M, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         M[i] = make_double2(-M[i].x, -M[i].y);
 }
+// HA/HB null: B only.
 int project_out(Run &r, const char *A, const char *HA, char *B, char *HB, double2 *M) {
     const size_t nn = (size_t)r.nb * r.nb;
     RK(gram(r, A, r.nb, B, r.nb, M, r.nb));
     k_neg_c128<<<blocks_for(nn), 256, 0, r.st>>>(M, nn);
     RK(rot(r, A, r.nb, M, r.nb, r.nb, B, 1));
-    RK(rot(r, HA, r.nb, M, r.nb, r.nb, HB, 1));
+    if (HB) RK(rot(r, HA, r.nb, M, r.nb, r.nb, HB, 1));
     return PW_OK;
 }
 
@@ -178,8 +178,8 @@ extern "C" int pw_eigh(pw_ctx *c, int n, int k, double *T, double *G, double *la
     r.c = c;
     r.st = pwk_stream(c);
     r.eigw_bytes = pwk::eig_work_bytes(n, k);
-    RK(pwk_scratch(c, S_EIGW, r.eigw_bytes, &r.eigw));
-    RK(pwk_scratch(c, S_EIGSTAT, 64, (void **)&r.eigstat));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGSTAT, 64, (void **)&r.eigstat));
     return eig(r, (double2 *)T, (double2 *)G, n, k, lam, (double2 *)S);
 }
 
@@ -202,20 +202,22 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
     r.nb = nb;
     r.ldq = ngw;
     const size_t blk = (size_t)ngw * nb * r.es;
-    RK(pwk_scratch(c, S_Q, 3 * blk, (void **)&r.Q));
-    RK(pwk_scratch(c, S_HQ, 3 * blk, (void **)&r.HQ));
-    RK(pwk_scratch(c, S_TMP1, 2 * blk, (void **)&r.T1));
-    RK(pwk_scratch(c, S_TMP2, 2 * blk, (void **)&r.T2));
+    RK(pwk_scratch(c, pwk::SL_LOB_Q, 3 * blk, (void **)&r.Q));
+    RK(pwk_scratch(c, pwk::SL_LOB_HQ, 3 * blk, (void **)&r.HQ));
+    RK(pwk_scratch(c, pwk::SL_LOB_TMP1, 2 * blk, (void **)&r.T1));
+    RK(pwk_scratch(c, pwk::SL_LOB_TMP2, 2 * blk, (void **)&r.T2));
     const int n3 = 3 * nb;
     const size_t s_nn = (size_t)nb * nb, s_33 = (size_t)n3 * n3;
-    RK(pwk_scratch(c, S_SMALL, (4 * s_nn + 2 * s_33 + (size_t)n3 * nb + 2 * n3) * sizeof(double2), (void **)&r.small));
+    RK(pwk_scratch(c, pwk::SL_LOB_SMALL, (4 * s_nn + 2 * s_33 + (size_t)n3 * nb + 2 * n3 + 8 * s_nn) * sizeof(double2),
+                   (void **)&r.small));
     r.eigw_bytes = pwk::eig_work_bytes(n3, nb) > pwk::eig_work_bytes(nb, nb) ? pwk::eig_work_bytes(n3, nb)
                                                                              : pwk::eig_work_bytes(nb, nb);
-    RK(pwk_scratch(c, S_EIGW, r.eigw_bytes, &r.eigw));
-    RK(pwk_scratch(c, S_EIGSTAT, 64, (void **)&r.eigstat));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGSTAT, 64, (void **)&r.eigstat));
     double2 *XHX = r.small, *M1 = XHX + s_nn, *Rinv = M1 + s_nn, *Sfin = Rinv + s_nn;
     double2 *T3 = Sfin + s_nn, *G3 = T3 + s_33, *S3 = G3 + s_33;
     double *lam = (double *)(S3 + (size_t)n3 * nb);
+    double2 *T2b = (double2 *)(lam + 2 * (size_t)n3), *G2b = T2b + 4 * s_nn;   // [X W] blocks kept for a retry
 
     char *Xs = r.blk(r.Q, 0), *Ws = r.blk(r.Q, 1), *Ps = r.blk(r.Q, 2);
     char *HXs = r.blk(r.HQ, 0), *HWs = r.blk(r.HQ, 1), *HPs = r.blk(r.HQ, 2);
@@ -224,6 +226,7 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
     RK(pw_apply(c, ik, ispin, dtype, Xs, HXs, r.ldq, nb, PW_OP_H));
     std::vector<double> ev(nb), ev_old(nb, 0.0);
     int it = 0;
+    bool dropP = false;
     const double SMALL = 10.0 * 2.220446049250313e-16;
     (void)SMALL;
     for (it = 1; it <= nitermax; ++it) {
@@ -246,14 +249,22 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
         k_scale_c128<<<blocks_for(s_nn), 256, 0, r.st>>>(XHX, M1, s_nn, -1.0);
         RK(rot(r, Xs, nb, M1, nb, nb, Ws, 1));
         RK(pw_kprec(c, ik, dtype, Ws, Ws, r.ldq, nb));
-        // HW = op_H(W); C = W'W = R^H R; W = W/R; HW = HW/R (:167-174)
-        RK(pw_apply(c, ik, ispin, dtype, Ws, HWs, r.ldq, nb, PW_OP_H));
-        if (dtype == PW_C64) {
-            // mixed precision: keep Q = [X W P] near-orthonormal so that its
-            // split-BF16 Gram stays positive definite: W -= X (X'W), and
-            // W -= P (P'W); HW follows with the same coefficients (H linear)
-            RK(project_out(r, Xs, HXs, Ws, HWs, M1));
-            if (it > 1) RK(project_out(r, Ps, HPs, Ws, HWs, M1));
+        // FP64 (reference order): HW = op_H(W); C = W'W = R^H R; W = W/R;
+        // HW = HW/R (:167-174).
+        // Mixed precision: keep Q = [X W P] near-orthonormal so that its
+        // split-BF16 Gram stays positive definite (W -= X (X'W), W -= P (P'W),
+        // twice is enough), normalise, and only then HW = op_H(W).  Carrying
+        // HW through the projections and 1/R instead lets its FP32 rounding,
+        // amplified by 1/R, drift away from H W; that drift reaches HX through
+        // HQ U and grows every iteration.
+        const bool mixed = dtype == PW_C64;
+        if (!mixed) RK(pw_apply(c, ik, ispin, dtype, Ws, HWs, r.ldq, nb, PW_OP_H));
+        if (mixed) {
+            RK(project_out(r, Xs, nullptr, Ws, nullptr, M1));
+            if (it > 1 && !dropP) {
+                RK(project_out(r, Ps, nullptr, Ws, nullptr, M1));
+                RK(project_out(r, Xs, nullptr, Ws, nullptr, M1));
+            }
         }
         RK(gram(r, Ws, nb, Ws, nb, M1, nb));
         {
@@ -268,18 +279,44 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
             RK(s);
         }
         RK(rot(r, Ws, nb, Rinv, nb, nb, r.T1, 0));
-        RK(rot(r, HWs, nb, Rinv, nb, nb, r.T2, 0));
         RK(copy_blk(r, Ws, r.T1, nb));
-        RK(copy_blk(r, HWs, r.T2, nb));
+        if (mixed) {
+            RK(pw_apply(c, ik, ispin, dtype, Ws, HWs, r.ldq, nb, PW_OP_H));
+        } else {
+            RK(rot(r, HWs, nb, Rinv, nb, nb, r.T2, 0));
+            RK(copy_blk(r, HWs, r.T2, nb));
+        }
         // Rayleigh-Ritz on Q = [X W (P)] (:176-185)
-        const int nq = (it > 1) ? 3 * nb : 2 * nb;
+        int nq = (it > 1 && !dropP) ? 3 * nb : 2 * nb;
         RK(gram(r, r.Q, nq, r.HQ, nq, T3, nq));
         RK(gram(r, r.Q, nq, r.Q, nq, G3, nq));
-        RK(eig(r, T3, G3, nq, nb, lam, S3));
+        if (dtype == PW_C64 && nq == 3 * nb) {
+            const size_t w2 = 2 * (size_t)nb * sizeof(double2);
+            CKR(c, cudaMemcpy2DAsync(T2b, w2, T3, nq * sizeof(double2), w2, 2 * nb, cudaMemcpyDeviceToDevice, r.st));
+            CKR(c, cudaMemcpy2DAsync(G2b, w2, G3, nq * sizeof(double2), w2, 2 * nb, cudaMemcpyDeviceToDevice, r.st));
+        }
+        {
+            int s = eig(r, T3, G3, nq, nb, lam, S3);
+            if (s == PW_ERR_NOT_POSDEF && dtype == PW_C64 && nq == 3 * nb) {
+                // mixed precision: Q'Q lost definiteness through P; redo the
+                // Rayleigh-Ritz on [X W] and restart P = W (as iteration 1)
+                ++r.restarts;
+                nq = 2 * nb;
+                s = eig(r, T2b, G2b, nq, nb, lam, S3);
+            }
+            if (s == PW_ERR_NOT_POSDEF && dtype == PW_C64) {
+                // [X W] itself is not definite: W is at the FP32 noise floor,
+                // the block has converged as far as this precision allows
+                ++r.restarts;
+                break;
+            }
+            RK(s);
+        }
+        const bool usedP = (nq == 3 * nb);
         // X = Q U, HX = HQ U  (:187-189) into the temporaries
         RK(rot(r, r.Q, nq, S3, nq, nb, r.T1, 0));
         RK(rot(r, r.HQ, nq, S3, nq, nb, r.T2, 0));
-        if (it > 1) {
+        if (usedP) {
             // P = [W P] U[nb:3nb], HP = [HW HP] U[nb:3nb]; P = P/R, HP = HP/R (:190-199)
             char *Pn = r.T1 + blk, *HPn = r.T2 + blk;
             RK(rot(r, Ws, 2 * nb, S3 + nb, nq, nb, Pn, 0));
@@ -304,6 +341,7 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
         }
         RK(copy_blk(r, Xs, r.T1, nb));
         RK(copy_blk(r, HXs, r.T2, nb));
+        dropP = false;
     }
     if (it > nitermax) it = nitermax;
     // final Rayleigh-Ritz: S = X'HX, S = (S+S')/2, X = X Q (:214-217)
@@ -328,11 +366,11 @@ extern "C" int pw_lobpcg_host(pw_ctx *c, int ik, int ispin, int dtype, double *X
     cudaStream_t st = pwk_stream(c);
     const size_t n = (size_t)ld * nb;
     void *d64 = nullptr, *d32 = nullptr;
-    RK(pwk_scratch(c, S_EIGSTAT + 1, n * sizeof(double2), &d64));
+    RK(pwk_scratch(c, pwk::SL_HOST_C128, n * sizeof(double2), &d64));
     CKR(c, cudaMemcpyAsync(d64, X, n * sizeof(double2), cudaMemcpyHostToDevice, st));
     void *dev = d64;
     if (dtype == PW_C64) {
-        RK(pwk_scratch(c, S_EIGSTAT + 2, n * sizeof(float2), &d32));
+        RK(pwk_scratch(c, pwk::SL_HOST_C64, n * sizeof(float2), &d32));
         CKR(c, pwk::convert_c128_to_c64((const double2 *)d64, (float2 *)d32, n, st));
         dev = d32;
     }
@@ -340,5 +378,64 @@ extern "C" int pw_lobpcg_host(pw_ctx *c, int ik, int ispin, int dtype, double *X
     if (dtype == PW_C64) CKR(c, pwk::convert_c64_to_c128((const float2 *)d32, (double2 *)d64, n, st));
     CKR(c, cudaMemcpyAsync(X, d64, n * sizeof(double2), cudaMemcpyDeviceToHost, st));
     CKR(c, cudaStreamSynchronize(st));
+    return PW_OK;
+}
+
+// ortho_sqrt! (ortho_sqrt.jl:1-11): psi := psi * inv(sqrt(psi'psi)), with
+// psi'psi = U diag(lam) U^H from the FP64 eigensolver and
+// inv(sqrt(.)) = U diag(lam^-1/2) U^H.
+namespace {
+__global__ void k_scale_cols(const double2 *U, const double *lam, double2 *V, int n) {
+    const size_t total = (size_t)n * n;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(t / n);
+        const double s = 1.0 / sqrt(lam[j]);
+        V[t] = make_double2(U[t].x * s, U[t].y * s);
+    }
+}
+}  // namespace
+
+extern "C" int pw_ortho_sqrt(pw_ctx *c, int dtype, void *psi, int64_t ld, int64_t ngw, int nb) {
+    if (!c) return PW_ERR_ARG;
+    if (dtype != PW_C128 && dtype != PW_C64) return pwk_fail(c, PW_ERR_ARG, "unknown dtype");
+    if (!psi || nb <= 0 || ngw <= 0 || ld < ngw) return pwk_fail(c, PW_ERR_ARG, "bad pw_ortho_sqrt arguments");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    Run r{};
+    r.c = c;
+    r.st = pwk_stream(c);
+    const size_t es = dtype == PW_C128 ? sizeof(double2) : sizeof(float2);
+    const size_t nn = (size_t)nb * nb;
+    double2 *S = nullptr, *U = nullptr, *M = nullptr, *V = nullptr;
+    double *lam = nullptr;
+    char *tmp = nullptr;
+    RK(pwk_scratch(c, pwk::SL_LOB_SMALL, 4 * nn * sizeof(double2) + nb * sizeof(double) + 256, (void **)&S));
+    U = S + nn;
+    V = U + nn;
+    M = V + nn;
+    lam = (double *)(M + nn);
+    RK(pwk_scratch(c, pwk::SL_LOB_TMP1, (size_t)ld * nb * es, (void **)&tmp));
+    r.eigw_bytes = pwk::eig_work_bytes(nb, nb);
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGSTAT, 64, (void **)&r.eigstat));
+    RK(pw_gram(c, dtype, ngw, nb, nb, psi, ld, psi, ld, (double *)S, nb, 0));
+    RK(eig(r, S, nullptr, nb, nb, lam, U));
+    std::vector<double> hl(nb);
+    CKR(c, cudaMemcpyAsync(hl.data(), lam, nb * sizeof(double), cudaMemcpyDeviceToHost, r.st));
+    CKR(c, cudaStreamSynchronize(r.st));
+    for (double x : hl)
+        if (!(x > 0.0)) return pwk_fail(c, PW_ERR_NOT_POSDEF, "psi'psi is not positive definite");
+    k_scale_cols<<<blocks_for(nn), 256, 0, r.st>>>(U, lam, V, nb);
+    // M = (U diag(lam^-1/2)) U^H : the C128 rotate computes A * W with A = V (n x n)
+    // and W = U^H (conj-transposed on the host side of this call)
+    std::vector<double2> hu(nn), huh(nn);
+    CKR(c, cudaMemcpyAsync(hu.data(), U, nn * sizeof(double2), cudaMemcpyDeviceToHost, r.st));
+    CKR(c, cudaStreamSynchronize(r.st));
+    for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) huh[(size_t)j * nb + i] = make_double2(hu[(size_t)i * nb + j].x, -hu[(size_t)i * nb + j].y);
+    CKR(c, cudaMemcpyAsync(S, huh.data(), nn * sizeof(double2), cudaMemcpyHostToDevice, r.st));
+    RK(pw_rotate(c, PW_C128, nb, nb, nb, V, nb, (const double *)S, nb, M, nb, 0));
+    RK(pw_rotate(c, dtype, ngw, nb, nb, psi, ld, (const double *)M, nb, tmp, ld, 0));
+    CKR(c, cudaMemcpy2DAsync(psi, ld * es, tmp, ld * es, ngw * es, nb, cudaMemcpyDeviceToDevice, r.st));
+    CKR(c, cudaStreamSynchronize(r.st));
     return PW_OK;
 }

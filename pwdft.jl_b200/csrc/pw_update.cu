@@ -34,7 +34,6 @@ namespace pwk {
 namespace upd {
 
 constexpr int RED_BLOCKS = 296;
-enum { S_A = 8, S_RHOG, S_VH, S_VXC, S_EPS, S_VTOT, S_RED };
 
 // ------------------------------------------------------------ plane kernels
 // real rho plane -> forward x-FFT -> active-x sub-plane -> forward y-FFT -> A
@@ -242,8 +241,8 @@ static int poisson(pw_ctx *c, const double *rho, double *VH) {
     RK(pwk_density_launch(c, &L, &G2, &Ng, &N));
     cudaStream_t st = pwk_stream(c);
     double2 *A = nullptr, *g = nullptr;
-    RK(pwk_scratch(c, S_A, (size_t)L.kp.N3 * L.kp.Ncol * sizeof(double2), (void **)&A));
-    RK(pwk_scratch(c, S_RHOG, (size_t)Ng * sizeof(double2), (void **)&g));
+    RK(pwk_scratch(c, SL_UPD_A, (size_t)L.kp.N3 * L.kp.Ncol * sizeof(double2), (void **)&A));
+    RK(pwk_scratch(c, SL_UPD_RHOG, (size_t)Ng * sizeof(double2), (void **)&g));
     const size_t smem = plane_smem(L);
     if (smem > 48 * 1024) {
         CKU(c, cudaFuncSetAttribute((const void *)k_plane_r2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -279,11 +278,11 @@ extern "C" int pw_update(pw_ctx *c, const double *rho, const double *Vps, double
     RK(pwk_density_launch(c, &L, &G2, &Ng, &N));
     cudaStream_t st = pwk_stream(c);
     double *vh = VH, *vxc = Vxc, *eps = nullptr, *vt = nullptr, *part = nullptr;
-    if (!vh) RK(pwk_scratch(c, S_VH, N * sizeof(double), (void **)&vh));
-    if (!vxc) RK(pwk_scratch(c, S_VXC, N * sizeof(double), (void **)&vxc));
-    RK(pwk_scratch(c, S_EPS, N * sizeof(double), (void **)&eps));
-    RK(pwk_scratch(c, S_VTOT, N * sizeof(double), (void **)&vt));
-    RK(pwk_scratch(c, S_RED, RED_BLOCKS * 3 * sizeof(double), (void **)&part));
+    if (!vh) RK(pwk_scratch(c, SL_UPD_VH, N * sizeof(double), (void **)&vh));
+    if (!vxc) RK(pwk_scratch(c, SL_UPD_VXC, N * sizeof(double), (void **)&vxc));
+    RK(pwk_scratch(c, SL_UPD_EPS, N * sizeof(double), (void **)&eps));
+    RK(pwk_scratch(c, SL_UPD_VTOT, N * sizeof(double), (void **)&vt));
+    RK(pwk_scratch(c, SL_UPD_RED, RED_BLOCKS * 3 * sizeof(double), (void **)&part));
     RK(poisson(c, rho, vh));
     k_vwn_vtot<<<RED_BLOCKS, 256, 0, st>>>(rho, Vps, vh, vxc, eps, vt, N);
     CKU(c, cudaGetLastError());
@@ -312,8 +311,8 @@ extern "C" int pw_band_energies(pw_ctx *c, int ik, int dtype, const void *psi, i
     if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
     cudaStream_t st = pwk_stream(c);
     double *dw = nullptr, *part = nullptr;
-    RK(pwk_scratch(c, S_RED + 1, (size_t)nb * sizeof(double), (void **)&dw));
-    RK(pwk_scratch(c, S_RED + 2, 2 * RED_BLOCKS * sizeof(double), (void **)&part));
+    RK(pwk_scratch(c, SL_BAND_W, (size_t)nb * sizeof(double), (void **)&dw));
+    RK(pwk_scratch(c, SL_BAND_RED, 2 * RED_BLOCKS * sizeof(double), (void **)&part));
     CKU(c, cudaMemcpyAsync(dw, w, nb * sizeof(double), cudaMemcpyHostToDevice, st));
     const int Ngw = pwk_ngw(c, ik);
     if (dtype == PW_C128)

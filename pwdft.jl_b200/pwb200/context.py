@@ -186,6 +186,12 @@ class Context:
                                   C.c_void_p(S.data_ptr()) if S is not None else None))
         return lam, S
 
+    def ortho_sqrt(self, X):
+        """ortho_sqrt!: X (nb, Ngw) device block made orthonormal in place."""
+        nb, ld = X.shape
+        self.use_torch_stream()
+        self._chk(self._L.pw_ortho_sqrt(self.h, dtype_code(X), C.c_void_p(X.data_ptr()), ld, ld, nb))
+
     def lobpcg(self, ik, ispin, X, tol=1e-5, nitermax=100, nconv=0):
         """diag_LOBPCG!: X (nb, Ngw) device block overwritten; returns (evals, niter)."""
         nb, ld = X.shape

@@ -100,6 +100,25 @@ def test_lobpcg_matches_exact_spectrum(ctx_fcc, prec):
     Xo = X0.copy()
     evo = lobpcg.diag_LOBPCG_k(H, Xo, ik, tol=tol, NiterMax=300)
     assert np.abs(ev - evo).max() < (1e-9 if prec == "c128" else 2e-4)
-    # returned vectors are orthonormal Ritz vectors
+    # returned vectors are orthonormal Ritz vectors; in the mixed path the
+    # split-BF16x3 products carry ~2^-17 relative error per term, so the
+    # Gram matrices that orthonormalise X are good to a few 1e-5
     Xr = X.cpu().numpy().T.astype(np.complex128)
-    assert np.abs(Xr.conj().T @ Xr - np.eye(nb)).max() < (1e-10 if prec == "c128" else 1e-5)
+    assert np.abs(Xr.conj().T @ Xr - np.eye(nb)).max() < (1e-10 if prec == "c128" else 5e-5)
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_ortho_sqrt(ctx_fcc, prec):
+    """ortho_sqrt (ortho_sqrt.jl:1-4) against the oracle's."""
+    import torch
+    from oracle import lobpcg
+    H, ctx, rng = ctx_fcc
+    ngw = H.pw.gvecw.Ngw[0]
+    psi = rng.random((ngw, 12)) + 1j * rng.random((ngw, 12))
+    ref = lobpcg.ortho_sqrt(psi)
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    X = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda().to(dt).contiguous()
+    ctx.ortho_sqrt(X)
+    got = X.cpu().numpy().T.astype(np.complex128)
+    assert np.abs(got - ref).max() < (1e-10 if prec == "c128" else 5e-4)
+    assert np.abs(got.conj().T @ got - np.eye(12)).max() < (1e-12 if prec == "c128" else 1e-4)
