@@ -141,3 +141,71 @@ __device__ __forceinline__ void lines(Cx<T> *buf, int nlines, int es, int ls, co
 }
 
 }  // namespace pwf
+
+namespace pwf {
+
+// Stage S of the N-point line FFT for lines [0, nl) of one warp group, with
+// element access through functors ld(line, x) -> Cx<T> and st(line, x, v):
+// the first stage of a line can read its input straight from another
+// layout, the last can scale or scatter its output, with no extra pass.
+template <typename T, int N, int S, class LD, class ST>
+__device__ __forceinline__ void fstage_io(int nl, const Cx<T> *tw, int sign, int lane, LD &ld, ST &st) {
+    constexpr int R = FPlan<N>::r(S);
+    constexpr int NS = fp_ns<N>(S);
+    constexpr int NBF = N / R;
+    constexpr int G = fp_group<N>();
+    constexpr int MAXB = (G * NBF + 31) / 32;
+    constexpr int TWS = N / (NS * R);
+    const int total = nl * NBF;
+    const T sg = (T)sign;
+    Cx<T> v[MAXB][R];
+#pragma unroll
+    for (int t = 0; t < MAXB; ++t) {
+        const int id = lane + 32 * t;
+        if (id < total) {
+            const int line = id / NBF, j = id % NBF, jm = j % NS;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[t][r] = ld(line, j + r * NBF);
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    Cx<T> w = tw[r * jm * TWS];
+                    if (sign > 0) w.y = -w.y;
+                    v[t][r] = cmul(v[t][r], w);
+                }
+            }
+            Dft<T, R>::run(v[t], sg, tw, N / R);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < MAXB; ++t) {
+        const int id = lane + 32 * t;
+        if (id < total) {
+            const int line = id / NBF, j = id % NBF, jm = j % NS;
+            const int x0 = (j / NS) * NS * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) st(line, x0 + r * NS, v[t][r]);
+        }
+    }
+    __syncwarp();
+}
+
+// Whole N-point FFT of nl <= fp_group<N>() lines held by one warp in buf
+// (line stride N): the first stage reads through ld0, the last writes
+// through stl, the stages between use buf.
+template <typename T, int N, class LD0, class STL>
+__device__ __forceinline__ void group_fft(Cx<T> *buf, int nl, const Cx<T> *tw, int sign, int lane, LD0 &ld0, STL &stl) {
+    auto bld = [&](int line, int x) { return buf[line * N + x]; };
+    auto bst = [&](int line, int x, Cx<T> v) { buf[line * N + x] = v; };
+    constexpr int NST = FPlan<N>::nst;
+    static_assert(NST == 1 || NST == 2, "fused plans have one or two stages");
+    if constexpr (NST == 1) {
+        fstage_io<T, N, 0>(nl, tw, sign, lane, ld0, stl);
+    } else {
+        fstage_io<T, N, 0>(nl, tw, sign, lane, ld0, bst);
+        fstage_io<T, N, 1>(nl, tw, sign, lane, bld, stl);
+    }
+}
+
+}  // namespace pwf

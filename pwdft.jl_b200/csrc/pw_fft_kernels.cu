@@ -407,6 +407,146 @@ kf_plane_rho(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ 
     }
 }
 
+
+// ---------------------------------------------- FP32 plane kernels, x fused
+// The x-direction work of a z-plane runs warp by warp on whole rows: the
+// first stage of each inverse x-FFT reads the active-x entries of the
+// sub-plane S directly (zeros elsewhere), the last stage multiplies by V(r)
+// (op_V_loc) or accumulates w |psi(r)|^2 (calc_rhoe), and the last stage of
+// the forward x-FFT writes only the active-x outputs back into S.  No block
+// barrier is needed inside the x-pass, and the zero-fill, scatter, V and
+// gather passes over the full plane disappear.
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// shared-memory layout of the x-fused plane kernels (in float2 units)
+struct PlaneXSmem {
+    int N1, N2, Nxa, nwarps, group, plane_f;  // plane_f: floats of a full plane kept in shared memory (0 or N1*N2)
+    __host__ __device__ size_t elems() const {
+        return (size_t)N1 + N2 + (size_t)Nxa * N2 + (size_t)nwarps * group * N1 + (plane_f + 1) / 2 + (N1 + 3) / 4;
+    }
+};
+
+template <int N1, int N2, bool VS>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
+              float2 *__restrict__ A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using T = float;
+    constexpr int G = pwf::fp_group<N1>();
+    const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = FFT_THREADS / 32;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N1;
+    Cx<T> *S = ty + N2;
+    Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * N1;
+    float *Vs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * N1);
+    short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
+    const int kz = blockIdx.x, b = blockIdx.y;
+    const float *Vp = Vr + (size_t)kz * N1 * N2;
+    if constexpr (VS)
+        for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[i], &Vp[i]);
+    for (int i = threadIdx.x; i < N1; i += FFT_THREADS) {
+        tx[i] = twx[i];
+        iax[i] = -1;
+    }
+    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < Nxa * N2; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
+    Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+#pragma unroll 4
+    for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+    __syncthreads();
+    line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);  // ends with __syncthreads
+    if constexpr (VS) {
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    for (int g0 = warp * G; g0 < N2; g0 += NW * G) {
+        const int nl = min(G, N2 - g0);
+        auto ld_s = [&](int line, int x) {
+            const int ia = iax[x];
+            return ia >= 0 ? S[ia * N2 + g0 + line] : cmake((T)0, (T)0);
+        };
+        auto st_v = [&](int line, int x, Cx<T> v) {
+            const float vv = VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]);
+            Xw[line * N1 + x] = cscale(v, vv);
+        };
+        auto ld_x = [&](int line, int x) { return Xw[line * N1 + x]; };
+        auto st_s = [&](int line, int x, Cx<T> v) {
+            const int ia = iax[x];
+            if (ia >= 0) S[ia * N2 + g0 + line] = v;
+        };
+        pwf::group_fft<T, N1>(Xw, nl, tx, +1, lane, ld_s, st_v);
+        pwf::group_fft<T, N1>(Xw, nl, tx, -1, lane, ld_x, st_s);
+    }
+    __syncthreads();
+    line_fft<T, N2, true>(S, Nxa, 1, N2, ty, -1);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
+}
+
+// calc_rhoe: bands [g*Bg, min(nb, (g+1)*Bg)) of plane kz; the weighted
+// |psi(r)|^2 accumulate in shared memory when the plane fits (RS), else in
+// the global partial sums directly.
+template <int N1, int N2, bool RS>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float2 *__restrict__ A,
+             int nb, int Bg, const double *__restrict__ w, float *__restrict__ rho_part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using T = float;
+    constexpr int G = pwf::fp_group<N1>();
+    constexpr int N12 = N1 * N2;
+    const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = FFT_THREADS / 32;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N1;
+    Cx<T> *S = ty + N2;
+    Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * N1;
+    float *Rs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * N1);
+    short *iax = reinterpret_cast<short *>(Rs + (RS ? N12 + (N12 & 1) : 0));
+    const int kz = blockIdx.x, g = blockIdx.y;
+    float *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
+    for (int i = threadIdx.x; i < N1; i += FFT_THREADS) {
+        tx[i] = twx[i];
+        iax[i] = -1;
+    }
+    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[i];
+    float *acc = RS ? Rs : rp;
+    for (int i = threadIdx.x; i < N12; i += FFT_THREADS) acc[i] = 0.0f;
+    __syncthreads();
+    for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
+    const int b0 = g * Bg, b1 = min(nb, b0 + Bg);
+    for (int b = b0; b < b1; ++b) {
+        const T wb = (T)w[b];
+        for (int i = threadIdx.x; i < Nxa * N2; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
+        __syncthreads();
+        const Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+#pragma unroll 4
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+        __syncthreads();
+        line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);
+        for (int g0 = warp * G; g0 < N2; g0 += NW * G) {
+            const int nl = min(G, N2 - g0);
+            auto ld_s = [&](int line, int x) {
+                const int ia = iax[x];
+                return ia >= 0 ? S[ia * N2 + g0 + line] : cmake((T)0, (T)0);
+            };
+            auto st_r = [&](int line, int x, Cx<T> v) { acc[(g0 + line) * N1 + x] += wb * (v.x * v.x + v.y * v.y); };
+            pwf::group_fft<T, N1>(Xw, nl, tx, +1, lane, ld_s, st_r);
+        }
+        __syncthreads();
+    }
+    if constexpr (RS)
+        for (int i = threadIdx.x; i < N12; i += FFT_THREADS) rp[i] = Rs[i];
+}
+
 }  // namespace pwk
 
 // ----------------------------------------------------------- host launchers
@@ -482,9 +622,47 @@ cudaError_t launch_zfwd(const FftLaunch &L, const void *A, const void *psi, void
     return cudaGetLastError();
 }
 
+// FP32 fixed sizes: the x-fused kernel (V(r) kept in shared memory when
+// the plane takes at most 32 KB)
+template <int NN>
+static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    constexpr bool VS = NN * NN * 4 <= 32 * 1024;
+    const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
+    const size_t smem = ps.elems() * sizeof(float2);
+    cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(kp.N3, nb);
+    kx_plane_vloc<NN, NN, VS><<<grid, FFT_THREADS, smem, st>>>(kp, (const float2 *)L.twx, (const float2 *)L.twy,
+                                                              (const float *)Vr, (float2 *)A);
+    return cudaGetLastError();
+}
+template <int NN>
+static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb, int G, int Bg, const double *w,
+                                      void *rho_part, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    constexpr bool RS = NN * NN * 4 <= 32 * 1024;
+    const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), RS ? NN * NN : 0};
+    const size_t smem = ps.elems() * sizeof(float2);
+    cudaError_t e = set_smem<float>((const void *)kx_plane_rho<NN, NN, RS>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(kp.N3, G);
+    kx_plane_rho<NN, NN, RS><<<grid, FFT_THREADS, smem, st>>>(kp, (const float2 *)L.twx, (const float2 *)L.twy,
+                                                             (const float2 *)A, nb, Bg, w, (float *)rho_part);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_plane_vloc(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
     const KPlan &kp = L.kp;
+    if constexpr (sizeof(T) == 4) {
+        if (kp.N1 == kp.N2) {
+#define PW_CASE(NN) \
+    if (kp.N1 == NN) return launch_plane_vloc_x<NN>(L, Vr, A, nb, st);
+            FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+        }
+    }
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
     if (kp.N1 == kp.N2) {
@@ -512,6 +690,14 @@ template <typename T>
 cudaError_t launch_plane_rho(const FftLaunch &L, const void *A, int nb, int G, int Bg, const double *w, void *rho_part,
                              cudaStream_t st) {
     const KPlan &kp = L.kp;
+    if constexpr (sizeof(T) == 4) {
+        if (kp.N1 == kp.N2) {
+#define PW_CASE(NN) \
+    if (kp.N1 == NN) return launch_plane_rho_x<NN>(L, A, nb, G, Bg, w, rho_part, st);
+            FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+        }
+    }
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
     if (kp.N1 == kp.N2) {
