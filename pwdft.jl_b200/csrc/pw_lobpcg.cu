@@ -135,6 +135,28 @@ int copy_blk(Run &r, char *dst, const char *src, int ncols) {
 
 // B -= A (A'B) and HB -= HA (A'B) for nb-column blocks (A orthonormal):
 // the block Gram-Schmidt step of the mixed-precision LOBPCG.  M: nb x nb scratch.
+// Mixed precision: each column of the FP32 block rescaled to unit norm,
+// the norm summed in FP64 (one CTA per column).  The split-BF16 Gram keeps
+// X orthonormal to about 1e-5; this makes the norms, and so the electron
+// count of calc_rhoe, exact to FP32 rounding.
+__global__ void k_normalize_cols_c64(float2 *X, int64_t ld, int ngw) {
+    __shared__ double red[32];
+    float2 *x = X + (size_t)blockIdx.x * ld;
+    double s = 0.0;
+    for (int g = threadIdx.x; g < ngw; g += blockDim.x) s += (double)x[g].x * x[g].x + (double)x[g].y * x[g].y;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        red[0] = t > 0.0 ? 1.0 / sqrt(t) : 1.0;
+    }
+    __syncthreads();
+    const float f = (float)red[0];
+    for (int g = threadIdx.x; g < ngw; g += blockDim.x) x[g] = make_float2(x[g].x * f, x[g].y * f);
+}
+
 __global__ void k_neg_c128(double2 *M, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         M[i] = make_double2(-M[i].x, -M[i].y);
@@ -350,6 +372,10 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
     RK(eig(r, Sfin, nullptr, nb, nb, lam, M1));
     RK(rot(r, Xs, nb, M1, nb, nb, r.T1, 0));
     CKR(c, cudaMemcpy2DAsync(X, ld * r.es, r.T1, r.ldq * r.es, ngw * r.es, nb, cudaMemcpyDeviceToDevice, r.st));
+    if (dtype == PW_C64) {
+        k_normalize_cols_c64<<<nb, 256, 0, r.st>>>((float2 *)X, ld, ngw);
+        CKR(c, cudaGetLastError());
+    }
     CKR(c, cudaMemcpyAsync(evals, lam, nb * sizeof(double), cudaMemcpyDeviceToHost, r.st));
     CKR(c, cudaStreamSynchronize(r.st));
     if (niter_out) *niter_out = it + 1000 * r.restarts;

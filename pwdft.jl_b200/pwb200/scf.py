@@ -16,7 +16,8 @@ the host, as set-up.
 precision = "fp64" runs the reference's FP64 path; "mixed" runs FP32
 blocks with split-BF16x3 tensor-core contractions until |dE| falls below
 `fp64_switch`, then converts psi to complex128 and finishes in FP64
-(iterative refinement).
+(iterative refinement; the Pulay history is kept: restarting it costs
+more FP64 iterations than it saves).
 """
 import time
 
@@ -121,6 +122,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     mixer = PulayMixer(N, betamix, mixdim, dev) if mix_method == "pulay" else None
     rho_new = torch.zeros(N, dtype=torch.float64, device=dev)
     Etot_old, Nconv, ethr = 0.0, 0, 0.1
+    imix = 0
     log = []
     evals = np.zeros((Nstates, b.Nkpt))
     t_start = time.perf_counter()
@@ -142,8 +144,9 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         diffRhoe = float(torch.sum(torch.abs(rho_new - rho)).item()) / N
         torch.cuda.synchronize()
         t2 = time.perf_counter()
+        imix += 1
         if mixer is not None:
-            rho = mixer(rho, rho_new, it)
+            rho = mixer(rho, rho_new, imix)
         else:
             rho = betamix * rho_new + (1 - betamix) * rho
         rho = torch.clamp(rho, min=EPS)
@@ -161,9 +164,12 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         t_rho += t2 - t1
         t_upd += t3 - t2
         diffE = abs(E["Total"] - Etot_old)
-        log.append((it, E["Total"], diffE, diffRhoe, int(np.max(np.array(nit) % 1000)), "c64" if mixed else "c128"))
+        nit = np.array(nit)
+        log.append((it, E["Total"], diffE, diffRhoe, int(np.max(nit % 1000)), "c64" if mixed else "c128",
+                    int(np.sum(nit // 1000))))
         if verbose:
-            print("SCF: %5d %18.10f %12.5e %12.5e  %s" % (it, E["Total"], diffE, diffRhoe, log[-1][-1]), flush=True)
+            print("SCF: %5d %18.10f %12.5e %12.5e  %s  LOBPCG its %d restarts %d  ethr %.1e  %.2fs" % (
+                it, E["Total"], diffE, diffRhoe, log[-1][5], log[-1][4], log[-1][6], ethr, t1 - t0), flush=True)
         Nconv = Nconv + 1 if diffE < etot_conv_thr else 0
         if Nconv >= 2:
             break

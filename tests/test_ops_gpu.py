@@ -143,6 +143,29 @@ def test_gram_and_rotate(system, prec):
     ctx.check_device()   # no bounded device-side wait expired
 
 
+@pytest.mark.parametrize("m", [480, 1440])
+def test_gram_long_k_accuracy(system, m):
+    """Overlap of an orthonormal FP32 block at the Si216 size (K = 80797
+    plane waves): the split-BF16x3 Gram stays at its per-term error, with no
+    drift from long tensor-core accumulation chains (the 480-band Gram was
+    off by 1e-4 when all of K went through one chain)."""
+    import torch
+    H, ctx, psis = system
+    if psis[0].shape[0] < 10000:
+        pytest.skip("one size suffices")
+    K = 80797
+    g = torch.Generator(device="cuda").manual_seed(11)
+    X = torch.randn((K, m), dtype=torch.complex128, device="cuda", generator=g)
+    Q, _ = torch.linalg.qr(X)
+    X32 = Q.T.contiguous().to(torch.complex64)
+    G = torch.zeros((m, m), dtype=torch.complex128, device="cuda")
+    ctx.gram(X32, X32, G)
+    Xd = X32.to(torch.complex128)
+    exact = Xd.conj() @ Xd.T
+    assert (G - exact).abs().max().item() < 2e-5
+    ctx.check_device()
+
+
 @pytest.mark.parametrize("prec", ["c128", "c64"])
 def test_host_dropin(system, prec):
     import pwb200
