@@ -316,7 +316,7 @@ int umma_scratch(pw_ctx *c, DevBuf &hi, DevBuf &lo, int64_t rows, int64_t K, Umm
 // C (m x n, CT) (+)= Z^H W  on tensor cores; Z, W complex64 (K x m / K x n).
 template <typename CT>
 int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, const void *Wm, int64_t ldw, void *C,
-            int64_t ldc, int acc) {
+            int64_t ldc, int acc, int upper = 0) {
     UmmaOperand A, B;
     int s;
     if ((s = umma_scratch(c, c->um_a_hi, c->um_a_lo, 2 * (int64_t)m, K, A)) ||
@@ -325,7 +325,7 @@ int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, cons
     CK(c, umma_prep_tn_a<float2>(Z, ldz, K, m, A, c->stream));
     CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
     if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp)))) return s;
-    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream));
+    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper));
     c->launches += 4;
     return PW_OK;
 }
@@ -708,6 +708,27 @@ extern "C" int pw_gram(pw_ctx *c, int dtype, int64_t K, int m, int n, const void
         CK(c, gemm_tn<double>(K, m, n, A, lda, B, ldb, (double2 *)C, ldc, accumulate, c->gemm_ws.p, c->stream));
     else
         CK(c, gemm_tn<float>(K, m, n, A, lda, B, ldb, (double2 *)C, ldc, accumulate, c->gemm_ws.p, c->stream));
+    c->launches += 2;
+    return PW_OK;
+}
+
+// Hermitian Gram (A^H B with the result known to be Hermitian, e.g. A = B
+// or B = H A): only the upper triangle C[i][j], i <= j, is formed and
+// written, in half the tiles.  Internal to the eigensolver paths, whose
+// consumers read the upper triangle (Julia's Hermitian(.)).
+int pwk_gram_upper(pw_ctx *c, int dtype, int64_t K, int m, const void *A, int64_t lda, const void *B, int64_t ldb,
+                   double *C, int64_t ldc) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_dtype(c, dtype))) return s;
+    if (!A || !B || !C || K <= 0 || m <= 0 || lda < K || ldb < K || ldc < m) return fail(c, PW_ERR_ARG, "bad gram arguments");
+    CK(c, cudaSetDevice(c->device));
+    if (dtype == PW_C64 && c->use_umma) return umma_tn<double2>(c, K, m, m, A, lda, B, ldb, C, ldc, 0, 1);
+    if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(K, m, m)))) return s;
+    if (dtype == PW_C128)
+        CK(c, gemm_tn<double>(K, m, m, A, lda, B, ldb, (double2 *)C, ldc, 0, c->gemm_ws.p, c->stream, 1));
+    else
+        CK(c, gemm_tn<float>(K, m, m, A, lda, B, ldb, (double2 *)C, ldc, 0, c->gemm_ws.p, c->stream, 1));
     c->launches += 2;
     return PW_OK;
 }

@@ -18,10 +18,11 @@ constexpr int TN_BM = 32, TN_BN = 32, TN_BK = 32;
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_gemm_tn(int64_t K, int m, int n, const Cx<T> *__restrict__ A, int64_t lda, const Cx<T> *__restrict__ B, int64_t ldb,
-          double2 *__restrict__ W, int64_t kchunk) {
+          double2 *__restrict__ W, int64_t kchunk, int upper) {
     __shared__ Cx<T> As[TN_BK][TN_BM + 1];
     __shared__ Cx<T> Bs[TN_BK][TN_BN + 1];
     const int m0 = blockIdx.x * TN_BM, n0 = blockIdx.y * TN_BN;
+    if (upper && m0 > n0 + TN_BN - 1) return;  // tile strictly below the diagonal
     const int64_t kbeg = (int64_t)blockIdx.z * kchunk;
     const int64_t kend = min(K, kbeg + kchunk);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -60,10 +61,11 @@ k_gemm_tn(int64_t K, int m, int n, const Cx<T> *__restrict__ A, int64_t lda, con
 }
 
 __global__ void k_splitk_reduce(const double2 *__restrict__ W, int S, int m, int n, double2 *__restrict__ C, int64_t ldc,
-                                int accumulate) {
+                                int accumulate, int upper) {
     const size_t total = (size_t)m * n;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
         const int nn = (int)(t / m), mm = (int)(t - (size_t)nn * m);
+        if (upper && mm > nn) continue;
         double2 s = accumulate ? C[(size_t)nn * ldc + mm] : make_double2(0.0, 0.0);
         for (int z = 0; z < S; ++z) {
             const double2 v = W[(size_t)z * total + t];
@@ -175,16 +177,16 @@ size_t gemm_tn_ws_bytes(int64_t K, int m, int n) {
 
 template <typename T>
 cudaError_t gemm_tn(int64_t K, int m, int n, const void *A, int64_t lda, const void *B, int64_t ldb, double2 *C,
-                    int64_t ldc, int accumulate, void *ws, cudaStream_t st) {
+                    int64_t ldc, int accumulate, void *ws, cudaStream_t st, int upper) {
     if (m <= 0 || n <= 0) return cudaSuccess;
     const int S = splitk_count(K, m, n);
     int64_t kchunk = (K + S - 1) / S;
     kchunk = ((kchunk + TN_BK - 1) / TN_BK) * TN_BK;
     dim3 grid((m + TN_BM - 1) / TN_BM, (n + TN_BN - 1) / TN_BN, S);
-    k_gemm_tn<T><<<grid, 256, 0, st>>>(K, m, n, (const Cx<T> *)A, lda, (const Cx<T> *)B, ldb, (double2 *)ws, kchunk);
+    k_gemm_tn<T><<<grid, 256, 0, st>>>(K, m, n, (const Cx<T> *)A, lda, (const Cx<T> *)B, ldb, (double2 *)ws, kchunk, upper);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_splitk_reduce<<<blocks_for((size_t)m * n), 256, 0, st>>>((const double2 *)ws, S, m, n, C, ldc, accumulate);
+    k_splitk_reduce<<<blocks_for((size_t)m * n), 256, 0, st>>>((const double2 *)ws, S, m, n, C, ldc, accumulate, upper);
     return cudaGetLastError();
 }
 
@@ -198,9 +200,9 @@ cudaError_t gemm_nn(int64_t M, int n, int k, const void *A, int64_t lda, const d
 }
 
 template cudaError_t gemm_tn<float>(int64_t, int, int, const void *, int64_t, const void *, int64_t, double2 *, int64_t,
-                                    int, void *, cudaStream_t);
+                                    int, void *, cudaStream_t, int);
 template cudaError_t gemm_tn<double>(int64_t, int, int, const void *, int64_t, const void *, int64_t, double2 *, int64_t,
-                                     int, void *, cudaStream_t);
+                                     int, void *, cudaStream_t, int);
 template cudaError_t gemm_nn<float>(int64_t, int, int, const void *, int64_t, const double2 *, int64_t, void *, int64_t,
                                     int, cudaStream_t);
 template cudaError_t gemm_nn<double>(int64_t, int, int, const void *, int64_t, const double2 *, int64_t, void *, int64_t,

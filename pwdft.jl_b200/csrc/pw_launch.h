@@ -50,8 +50,11 @@ template <typename T> cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t 
 // ws: split-K workspace of at least gemm_tn_ws_bytes() bytes.
 size_t gemm_tn_ws_bytes(int64_t K, int m, int n);
 template <typename T>
+// upper != 0: only C[i][j] with i <= j is formed and written (Hermitian
+// products whose consumer reads the upper triangle); tiles strictly below
+// the diagonal are skipped.
 cudaError_t gemm_tn(int64_t K, int m, int n, const void *A, int64_t lda, const void *B, int64_t ldb, double2 *C,
-                    int64_t ldc, int accumulate, void *ws, cudaStream_t);
+                    int64_t ldc, int accumulate, void *ws, cudaStream_t, int upper = 0);
 // C (M x n, Cx<T>, ldc) (+)= A (M x k, Cx<T>) * B (k x n, double2)
 template <typename T>
 cudaError_t gemm_nn(int64_t M, int n, int k, const void *A, int64_t lda, const double2 *B, int64_t ldb, void *C,

@@ -29,6 +29,8 @@
 
 int pwk_fail(pw_ctx *c, int code, const char *msg);
 int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out);
+int pwk_gram_upper(pw_ctx *c, int dtype, int64_t K, int m, const void *A, int64_t lda, const void *B, int64_t ldb,
+                   double *C, int64_t ldc);
 cudaStream_t pwk_stream(pw_ctx *c);
 int pwk_ngw(const pw_ctx *c, int ik);
 int pwk_device(const pw_ctx *c);
@@ -127,6 +129,11 @@ int rot(Run &r, const char *A, int k, const double2 *M, int ldm, int n, char *ou
 }
 int gram(Run &r, const char *A, int m, const char *B, int n, double2 *C, int ldc) {
     return pw_gram(r.c, r.dtype, r.ngw, m, n, A, r.ldq, B, r.ldq, (double *)C, ldc, 0);
+}
+// Hermitian products (X'HX, Q'HQ, Q'Q, W'W, P'P): upper triangle only, which
+// is all their consumers read
+int gram_h(Run &r, const char *A, int m, const char *B, double2 *C, int ldc) {
+    return pwk_gram_upper(r.c, r.dtype, r.ngw, m, A, r.ldq, B, r.ldq, (double *)C, ldc);
 }
 int copy_blk(Run &r, char *dst, const char *src, int ncols) {
     CKR(r.c, cudaMemcpy2DAsync(dst, r.ldq * r.es, src, r.ldq * r.es, r.ngw * r.es, ncols, cudaMemcpyDeviceToDevice, r.st));
@@ -253,7 +260,7 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
     (void)SMALL;
     for (it = 1; it <= nitermax; ++it) {
         // Rayleigh quotient XHX = X' HX and its eigenvalues (:85-86)
-        RK(gram(r, Xs, nb, HXs, nb, XHX, nb));
+        RK(gram_h(r, Xs, nb, HXs, XHX, nb));
         k_herm_from_upper<<<blocks_for(s_nn), 256, 0, r.st>>>(XHX, nb);
         CKR(c, cudaMemcpyAsync(M1, XHX, s_nn * sizeof(double2), cudaMemcpyDeviceToDevice, r.st));
         RK(eig(r, M1, nullptr, nb, nb, lam, nullptr));
@@ -288,7 +295,7 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
                 RK(project_out(r, Xs, nullptr, Ws, nullptr, M1));
             }
         }
-        RK(gram(r, Ws, nb, Ws, nb, M1, nb));
+        RK(gram_h(r, Ws, nb, Ws, M1, nb));
         {
             const int s = chol_rinv(r, M1, nb, Rinv);
             // mixed precision: a W'W that is not positive definite means the
@@ -310,8 +317,8 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
         }
         // Rayleigh-Ritz on Q = [X W (P)] (:176-185)
         int nq = (it > 1 && !dropP) ? 3 * nb : 2 * nb;
-        RK(gram(r, r.Q, nq, r.HQ, nq, T3, nq));
-        RK(gram(r, r.Q, nq, r.Q, nq, G3, nq));
+        RK(gram_h(r, r.Q, nq, r.HQ, T3, nq));
+        RK(gram_h(r, r.Q, nq, r.Q, G3, nq));
         if (dtype == PW_C64 && nq == 3 * nb) {
             const size_t w2 = 2 * (size_t)nb * sizeof(double2);
             CKR(c, cudaMemcpy2DAsync(T2b, w2, T3, nq * sizeof(double2), w2, 2 * nb, cudaMemcpyDeviceToDevice, r.st));
@@ -344,7 +351,7 @@ extern "C" int pw_lobpcg(pw_ctx *c, int ik, int ispin, int dtype, void *X, int64
             RK(rot(r, Ws, 2 * nb, S3 + nb, nq, nb, Pn, 0));
             RK(rot(r, HWs, 2 * nb, S3 + nb, nq, nb, HPn, 0));
             if (dtype == PW_C64) RK(project_out(r, r.T1, r.T2, Pn, HPn, M1));   // P -= Xnew (Xnew'P)
-            RK(gram(r, Pn, nb, Pn, nb, M1, nb));
+            RK(gram_h(r, Pn, nb, Pn, M1, nb));
             const int s = chol_rinv(r, M1, nb, Rinv);
             if (s == PW_ERR_NOT_POSDEF && dtype == PW_C64) {
                 // mixed precision: restart the conjugate directions, P = W

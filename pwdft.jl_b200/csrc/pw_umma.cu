@@ -125,7 +125,11 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 __global__ void __launch_bounds__(THREADS, 1)
 k_umma_gemm(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CUtensorMap tAlo,
             const __grid_constant__ CUtensorMap tBhi, const __grid_constant__ CUtensorMap tBlo, int Mp, int Np, int KB,
-            int kb_per, float *__restrict__ W, int *__restrict__ err) {
+            int kb_per, float *__restrict__ W, int *__restrict__ err, int upper) {
+    // upper: C = Z^H W is Hermitian and only its upper triangle is read; a
+    // tile whose complex rows (m0/2 ..) all lie below its columns is skipped
+    // before any barrier or TMEM allocation
+    if (upper && (int)(blockIdx.x * BM) / 2 > (int)(blockIdx.y * BN) + BN - 1) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     Bars *bars = reinterpret_cast<Bars *>(smem + (size_t)STAGES * STAGE_BYTES);
@@ -332,11 +336,13 @@ __global__ void k_zero_pad(__nv_bfloat16 *hi, __nv_bfloat16 *lo, int64_t rows, i
 
 // C (m x n complex, ldc) (+)= sum_z W[z]  with W[z][j][2i + {0,1}] = {Re, Im}
 template <typename CT>
-__global__ void k_finalize(const float *__restrict__ W, int S, int m, int n, CT *__restrict__ C, int64_t ldc, int accumulate) {
+__global__ void k_finalize(const float *__restrict__ W, int S, int m, int n, CT *__restrict__ C, int64_t ldc, int accumulate,
+                           int upper) {
     const size_t total = (size_t)m * n;
     const size_t Mp = 2 * (size_t)m;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
         const size_t j = t / m, i = t - j * m;
+        if (upper && i > j) continue;
         double re = 0.0, im = 0.0;
         for (int z = 0; z < S; ++z) {
             const float *w = W + (size_t)z * Mp * n + j * Mp + 2 * i;
@@ -444,7 +450,7 @@ size_t umma_ws_bytes(int64_t Mp, int Np, int Kp) { return (size_t)umma_splits(Mp
 
 template <typename CT>
 cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
-                      float *ws, int *err, cudaStream_t st) {
+                      float *ws, int *err, cudaStream_t st, int upper) {
     cudaError_t e = get_encoder();
     if (e != cudaSuccess) return e;
     if (A.Kp != B.Kp || A.rows != 2 * (int64_t)m || B.rows != n) return cudaErrorInvalidValue;
@@ -463,9 +469,9 @@ cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, 
     const int S = umma_splits(A.rows, n, A.Kp);
     const int kb_per = (KB + S - 1) / S;
     dim3 grid((unsigned)((A.rows + BM - 1) / BM), (n + BN - 1) / BN, S);
-    k_umma_gemm<<<grid, THREADS, SMEM_BYTES, st>>>(mAhi, mAlo, mBhi, mBlo, (int)A.rows, n, KB, kb_per, ws, err);
+    k_umma_gemm<<<grid, THREADS, SMEM_BYTES, st>>>(mAhi, mAlo, mBhi, mBlo, (int)A.rows, n, KB, kb_per, ws, err, upper);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_finalize<CT><<<blocks_for((size_t)m * n), 256, 0, st>>>(ws, S, m, n, (CT *)C, ldc, accumulate);
+    k_finalize<CT><<<blocks_for((size_t)m * n), 256, 0, st>>>(ws, S, m, n, (CT *)C, ldc, accumulate, upper);
     return cudaGetLastError();
 }
 
@@ -474,8 +480,8 @@ template cudaError_t umma_prep_tn_b<float2>(const void *, int64_t, int64_t, int,
 template cudaError_t umma_prep_tn_b<double2>(const void *, int64_t, int64_t, int, UmmaOperand &, cudaStream_t);
 template cudaError_t umma_prep_nn_a<float2>(const void *, int64_t, int64_t, int, UmmaOperand &, cudaStream_t);
 template cudaError_t umma_gemm<float2>(const UmmaOperand &, const UmmaOperand &, int, int, void *, int64_t, int, float *,
-                                       int *, cudaStream_t);
+                                       int *, cudaStream_t, int);
 template cudaError_t umma_gemm<double2>(const UmmaOperand &, const UmmaOperand &, int, int, void *, int64_t, int, float *,
-                                        int *, cudaStream_t);
+                                        int *, cudaStream_t, int);
 
 }  // namespace pwk

@@ -29,7 +29,8 @@ template <typename CT> cudaError_t umma_prep_nn_a(const void *A, int64_t lda, in
 // C (m x n complex of type CT, ldc) (+)= result; A.rows == 2m, B.rows == n.
 // err: device int set non-zero if a bounded wait in the kernel expired.
 template <typename CT>
+// upper != 0: C is Hermitian and only C[i][j], i <= j, is formed and written.
 cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
-                      float *ws, int *err, cudaStream_t);
+                      float *ws, int *err, cudaStream_t, int upper = 0);
 
 }  // namespace pwk

@@ -14,8 +14,8 @@ The starting density (guess_rhoe.jl) and E_NN (Ewald) are computed once on
 the host, as set-up.
 
 precision = "fp64" runs the reference's FP64 path; "mixed" runs FP32
-blocks with split-BF16x3 tensor-core contractions until |dE| falls below
-`fp64_switch`, then converts psi to complex128 and finishes in FP64
+blocks with split-BF16x3 tensor-core contractions until |dE| stays below
+`fp64_switch` for two iterations, then converts psi to complex128 and finishes in FP64
 (iterative refinement; the Pulay history is kept: restarting it costs
 more FP64 iterations than it saves).
 """
@@ -123,6 +123,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     rho_new = torch.zeros(N, dtype=torch.float64, device=dev)
     Etot_old, Nconv, ethr = 0.0, 0, 0.1
     imix = 0
+    nsw = 0   # consecutive iterations with |dE| below fp64_switch (as the convergence test)
     log = []
     evals = np.zeros((Nstates, b.Nkpt))
     t_start = time.perf_counter()
@@ -173,7 +174,8 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         Nconv = Nconv + 1 if diffE < etot_conv_thr else 0
         if Nconv >= 2:
             break
-        if mixed and diffE < fp64_switch and it > 2:
+        nsw = nsw + 1 if diffE < fp64_switch else 0
+        if mixed and nsw >= 2 and it > 2:
             # iterative refinement: finish in FP64
             psiks = [p.to(torch.complex128).contiguous() for p in psiks]
             mixed = False
