@@ -48,6 +48,12 @@ PSP = os.path.join(ROOT, "tests", "golden", "psp", "Si-q4.gth")
 DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+# DRAM bytes (read + write) of one FP32 pruned-FFT round trip of the Si64
+# op_H (160 bands: kf_zinv + kx_plane_vloc + kf_zfwd over two band chunks),
+# from one capture of this bench:
+#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+#     --clock-control none -k regex:"kf_z|kx_plane" -s 12 -c 6 python bench.py --steps 3 --warmup 3
+FFT_TRAFFIC_BYTES = {"si64": 277.9e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -127,6 +133,14 @@ def byte_model(Ns, idx_gw2r, nb):
     return 8 * (3 * len(idx_gw2r) + 4 * P) + 4 * N1 * N2 * N3 / nb, nxa
 
 
+def bf16_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["bf16_tflops"])
+    except Exception:
+        return 1590.0
+
+
 def peaks():
     try:
         with open(MEASURED_PEAKS) as f:
@@ -186,16 +200,54 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def build_workload(device):
+WORKLOADS = {"si64": 160, "si216": 480}   # bands of the op_H microbenchmark per system
+
+
+def build_workload(device, workload="si64"):
+    """The op_H microbenchmark: Si64 (2x2x2 cells, 160 bands) or Si216 (3x3x3
+    cells with seeded +-0.02 bohr displacements, 480 bands), Gamma,
+    ecutwfc 15 Ha; V_loc = GTH local part + 0.01 Ha seeded smooth field;
+    psi seeded complex Gaussian, orthonormalised."""
     import pwb200
-    LL, pos = si64_geometry()
+    LL, pos = si64_geometry() if workload == "si64" else si216_geometry(SEED)
     sysm = pwb200.System(["Si"] * pos.shape[1], pos, LL)
     H = pwb200.Hamiltonian(sysm, [PSP], 15.0, device=device)
     rng = np.random.default_rng(SEED)
     b = H.basis
     H.update_vloc(H.V_Ps_loc + 0.01 * smooth_field(b.Ns, b.G2, b.idx_g2r, rng))
-    psi = orthonormal_psi(H.basis.Ngw[0], NBANDS, rng)
+    psi = orthonormal_psi(H.basis.Ngw[0], WORKLOADS[workload], rng)
     return H, psi
+
+
+def time_rayleigh_ritz(ctx, psi32, nb, steps, flush):
+    """The LOBPCG contractions at this workload's size on the tensor cores:
+    the Gram Q^H Q (3nb x 3nb over Ngw) and the rotation Q U (Ngw x 3nb ->
+    nb), split-BF16x3; flops counted once per complex multiply-add (8)."""
+    import torch
+    ngw = psi32.shape[1]
+    Q = torch.cat([psi32, psi32.roll(1, 0), psi32.roll(2, 0)]).contiguous()
+    G = torch.zeros((3 * nb, 3 * nb), dtype=torch.complex128, device=psi32.device)
+    g = torch.Generator(device=psi32.device).manual_seed(SEED)
+    U = torch.randn((nb, 3 * nb), dtype=torch.complex128, device=psi32.device, generator=g)
+    out = torch.empty((nb, ngw), dtype=torch.complex64, device=psi32.device)
+    res = {}
+    for name, fn, flops in (("gram", lambda: ctx.gram(Q, Q, G), 8.0 * (3 * nb) ** 2 * ngw),
+                            ("rotate", lambda: ctx.rotate(Q, U, out), 8.0 * 3 * nb * nb * ngw)):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            flush.add_(1)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e))
+        ms = sum(ts) / len(ts)
+        res[name] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+    return res
 
 
 def time_device(ctx, x, y, ops, steps, warmup, flush):
@@ -245,6 +297,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--workload", default="si64", choices=sorted(WORKLOADS),
+                    help="op_H microbenchmark system (si64: the headline configuration)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -284,10 +338,11 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     torch.cuda.set_device(local)
-    H, psi = build_workload(local)
+    H, psi = build_workload(local, args.workload)
     ctx = H.ctx
-    bpb, nxa = byte_model(H.basis.Ns, H.basis.idx_gw2r[0], NBANDS)
-    step_bytes = bpb * NBANDS
+    nbands = WORKLOADS[args.workload]
+    bpb, nxa = byte_model(H.basis.Ns, H.basis.idx_gw2r[0], nbands)
+    step_bytes = bpb * nbands
     x32 = torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{local}").to(torch.complex64).contiguous()
     x64 = torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{local}").contiguous()
     y32, y64 = torch.empty_like(x32), torch.empty_like(x64)
@@ -312,6 +367,8 @@ def main():
         t = torch.tensor([ms, ms_fft, ms64], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_fft, ms64 = [float(v) for v in t.tolist()]
+
+    rr = time_rayleigh_ritz(ctx, x32, nbands, max(5, args.steps // 20), flush)
 
     # SCF time to 1e-6 Ha/atom on Si216 (the large mixed-precision SCF
     # workload): mixed vs FP64 on this GPU, rank 0 of a single-process run
@@ -351,8 +408,9 @@ def main():
         "vs_baseline": None,
         "dtype": "c64",
         "data": "synthetic",
-        "config": {"workload": "Si64 Gamma op_H (K+V_loc+V_Ps_nloc), 160 bands, 75^3 grid, Ngw 23871, "
-                               "NbetaNL 320", "global_batch": NBANDS * world, "seq_len": 0,
+        "config": {"workload": "%s Gamma op_H (K+V_loc+V_Ps_nloc), %d bands, %d^3 grid, Ngw %d, NbetaNL %d" % (
+                               "Si64" if args.workload == "si64" else "Si216", nbands, H.basis.Ns[0],
+                               H.basis.Ngw[0], H.NbetaNL), "global_batch": nbands * world, "seq_len": 0,
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed between steps (256 MB write)", "bytes_per_band": bpb, "nx_active": nxa},
         "fp64_ms_per_step": ms64,
@@ -362,13 +420,16 @@ def main():
                 "h2d_bytes_per_step": int(psi.size * 16), "d2h_bytes_per_step": int(psi.size * 16),
                 "ms_per_step": e2e_s * 1e3},
         "roofline": {"bound": "hbm", "achieved": fft_gbs, "peak": hbm, "unit": "GB/s", "frac": fft_gbs / hbm,
-                     "traffic": None, "peak_kind": peak_kind,
+                     "traffic": FFT_TRAFFIC_BYTES.get(args.workload), "peak_kind": peak_kind,
                      "kernel": "op_V_loc pruned-FFT round trip (K-zinv+K-plane+K-zfwd), %.4f ms" % ms_fft},
         "clocks": clk.summary(),
+        "rayleigh_ritz": {"gram_3nb": rr["gram"], "rotate_3nb_to_nb": rr["rotate"], "unit": "TFLOP/s",
+                          "peak_bf16_tflops": bf16_peak(), "gram_frac_of_bf16_peak": rr["gram"]["tflops"] / bf16_peak(),
+                          "note": "split-BF16x3: three BF16 products per logical product, one counted"},
     }
     if scf_out is not None:
         out["scf"] = scf_out
-    if rank == 0 and world == 1 and os.environ.get("PW_BENCH_NO_CPU") != "1":
+    if rank == 0 and world == 1 and args.workload == "si64" and os.environ.get("PW_BENCH_NO_CPU") != "1":
         dt, nsamp, reps = cpu_reference(psi, 1000, 1, args.cpu_budget)
         v = nsamp * bpb / dt / 1e9
         out["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
