@@ -86,7 +86,7 @@ struct pw_ctx {
     size_t a_chunk_bytes = 48ull << 20;
     bool use_umma = true;     // mixed-precision contractions on tcgen05 (PW_GEMM=cuda: CUDA cores)
     int *d_err = nullptr;     // device error word of the bounded waits in the tensor-core kernels
-    DevBuf um_a_hi, um_a_lo, um_b_hi, um_b_lo, um_ws;
+    DevBuf um_a_hi, um_a_lo, um_b_hi, um_b_lo, um_b_lo2, um_ws;
     DevBuf slots[32];         // grow-only scratch for the eigensolver and LOBPCG
     KData dens;               // the density G-sphere (for Poisson_solve! on the device)
     bool have_dens = false;
@@ -303,13 +303,19 @@ int band_chunk(const pw_ctx *c, int ik, size_t es, int nb) {
     return (int)std::min<size_t>(ch, (size_t)nb);
 }
 
-// Per-call split-BF16 operands live in grow-only scratch buffers.
-int umma_scratch(pw_ctx *c, DevBuf &hi, DevBuf &lo, int64_t rows, int64_t K, UmmaOperand &op) {
+// Per-call split-BF16 operands live in grow-only scratch buffers (lo2: a
+// third BF16 piece, for the products that need ~2^-24).
+int umma_scratch(pw_ctx *c, DevBuf &hi, DevBuf &lo, int64_t rows, int64_t K, UmmaOperand &op, DevBuf *lo2 = nullptr) {
     const size_t half = umma_operand_bytes(rows, K) / 2;
     int s;
     if ((s = ensure(c, hi, half)) || (s = ensure(c, lo, half))) return s;
     op.hi = (__nv_bfloat16 *)hi.p;
     op.lo = (__nv_bfloat16 *)lo.p;
+    op.lo2 = nullptr;
+    if (lo2) {
+        if ((s = ensure(c, *lo2, half))) return s;
+        op.lo2 = (__nv_bfloat16 *)lo2->p;
+    }
     return PW_OK;
 }
 
@@ -325,7 +331,8 @@ int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, cons
     CK(c, umma_prep_tn_a<float2>(Z, ldz, K, m, A, c->stream));
     CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
     if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp)))) return s;
-    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper));
+    const int same = (Z == Wm && ldz == ldw && m == n);   // Z^H Z: add the lo*lo product
+    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper, same));
     c->launches += 4;
     return PW_OK;
 }
@@ -365,8 +372,10 @@ int apply_T(pw_ctx *c, int ik, int ispin, const void *psi, void *Hpsi, int64_t l
         const size_t pb = (size_t)c->nbeta * nb * sizeof(double2);
         if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb))) return s;
         if (sizeof(T) == 4 && c->use_umma) {
+            // betaNL' psi cancels heavily (|beta' psi| << |beta||psi|): three
+            // BF16 pieces keep its error at FP32 level; two bias <psi|V_NL|psi>
             UmmaOperand B;
-            if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B))) return s;
+            if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B, &c->um_b_lo2))) return s;
             CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
             if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
             CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, c->P.p, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
@@ -610,6 +619,8 @@ extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta)
                 const size_t half = umma_operand_bytes(rows, K) / 2;
                 if ((s = dalloc(c, (unsigned char **)&op->hi, half)) || (s = dalloc(c, (unsigned char **)&op->lo, half)))
                     return s;
+                // betaNL' psi runs with three pieces (see apply_T)
+                if (op == &kd.beta_tn && (s = dalloc(c, (unsigned char **)&op->lo2, half))) return s;
             }
         }
         CK(c, umma_prep_tn_a<float2>(kd.d_beta32, kd.Ngw, kd.Ngw, nbeta, kd.beta_tn, c->stream));
@@ -863,7 +874,7 @@ int pwk_projections(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, i
     cudaStream_t st = c->stream;
     if (dtype == PW_C64 && c->use_umma) {
         UmmaOperand B;
-        if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B))) return s;
+        if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B, &c->um_b_lo2))) return s;
         CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
         if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
         CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, c->P.p, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));

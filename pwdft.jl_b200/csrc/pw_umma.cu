@@ -40,21 +40,31 @@
 namespace pwk {
 namespace umma {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3;
+constexpr int BM = 128, BN = 128, BK = 64;
 constexpr int TILE_BYTES = BM * BK * 2;   // 16 KB per operand tile (BM == BN)
-constexpr int STAGE_BYTES = 4 * TILE_BYTES;
 constexpr int THREADS = 192;
-constexpr uint32_t TMEM_COLS = 128;
+constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulator tiles (double buffer)
 constexpr long long WAIT_LIMIT = 1ll << 26;
+constexpr int MAX_STAGES = 3;
+
+// NS = number of BF16 pieces per FP32 value: 2 (hi, lo: 3 products, ~2^-17)
+// or 3 (hi, mid, lo: 6 products, ~2^-24, for products with heavy
+// cancellation such as betaNL' psi).  Three pieces need 6 tiles per stage,
+// so the pipeline keeps 2 stages instead of 3.
+template <int NS> struct Cfg {
+    static constexpr int STAGES = NS == 2 ? 3 : 2;
+    static constexpr int STAGE_BYTES = 2 * NS * TILE_BYTES;
+};
 
 struct __align__(8) Bars {
-    uint64_t full[STAGES];
-    uint64_t empty[STAGES];
-    uint64_t accum;
+    uint64_t full[MAX_STAGES];
+    uint64_t empty[MAX_STAGES];
+    uint64_t tfull[2];    // accumulator tile b holds a finished k-block
+    uint64_t tempty[2];   // the epilogue has drained accumulator tile b
     uint32_t tmem_base;
     int failed;
 };
-constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + sizeof(Bars);
+template <int NS> constexpr size_t smem_bytes() { return 1024 + (size_t)Cfg<NS>::STAGES * Cfg<NS>::STAGE_BYTES + sizeof(Bars); }
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -98,6 +108,9 @@ __device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uin
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
         "l"(a), "l"(b), "r"(IDESC), "r"(accum));
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
                  : "memory");
@@ -120,12 +133,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// D (Mp x Np) = sum over the split's k-blocks of  Ahi Bhi^T + Ahi Blo^T + Alo Bhi^T
+// D (Mp x Np) = sum over the split's k-blocks of the piece products
+//   NS = 2:  A0 B0^T + A0 B1^T + A1 B0^T
+//   NS = 3:  A0 B0^T + A0 B1^T + A1 B0^T + A0 B2^T + A1 B1^T + A2 B0^T
 // written to W[z][n][m] (fp32, column-major, ld = Mp).
+template <int NS>
 __global__ void __launch_bounds__(THREADS, 1)
-k_umma_gemm(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CUtensorMap tAlo,
-            const __grid_constant__ CUtensorMap tBhi, const __grid_constant__ CUtensorMap tBlo, int Mp, int Np, int KB,
-            int kb_per, float *__restrict__ W, int *__restrict__ err, int upper) {
+k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
+            const __grid_constant__ CUtensorMap tA2, const __grid_constant__ CUtensorMap tB0,
+            const __grid_constant__ CUtensorMap tB1, const __grid_constant__ CUtensorMap tB2, int Mp, int Np, int KB,
+            int kb_per, float *__restrict__ W, int *__restrict__ err, int upper, int lolo) {
+    constexpr int STAGES = Cfg<NS>::STAGES;
+    constexpr int STAGE_BYTES = Cfg<NS>::STAGE_BYTES;
     // upper: C = Z^H W is Hermitian and only its upper triangle is read; a
     // tile whose complex rows (m0/2 ..) all lie below its columns is skipped
     // before any barrier or TMEM allocation
@@ -144,7 +163,10 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CU
             mbar_init(&bars->full[s], 1);
             mbar_init(&bars->empty[s], 1);
         }
-        mbar_init(&bars->accum, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&bars->tfull[b], 1);
+            mbar_init(&bars->tempty[b], 4);   // one arrival per epilogue warp
+        }
         bars->failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -170,10 +192,13 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CU
             unsigned char *st = smem + (size_t)s * STAGE_BYTES;
             mbar_expect_tx(&bars->full[s], STAGE_BYTES);
             const int kc = (kb0 + i) * BK;
-            tma_load_2d(st, &tAhi, &bars->full[s], kc, m0);
-            tma_load_2d(st + TILE_BYTES, &tAlo, &bars->full[s], kc, m0);
-            tma_load_2d(st + 2 * TILE_BYTES, &tBhi, &bars->full[s], kc, n0);
-            tma_load_2d(st + 3 * TILE_BYTES, &tBlo, &bars->full[s], kc, n0);
+            // stage layout: A pieces 0..NS-1, then B pieces 0..NS-1
+            tma_load_2d(st, &tA0, &bars->full[s], kc, m0);
+            tma_load_2d(st + TILE_BYTES, &tA1, &bars->full[s], kc, m0);
+            if constexpr (NS == 3) tma_load_2d(st + 2 * TILE_BYTES, &tA2, &bars->full[s], kc, m0);
+            tma_load_2d(st + NS * TILE_BYTES, &tB0, &bars->full[s], kc, n0);
+            tma_load_2d(st + (NS + 1) * TILE_BYTES, &tB1, &bars->full[s], kc, n0);
+            if constexpr (NS == 3) tma_load_2d(st + (NS + 2) * TILE_BYTES, &tB2, &bars->full[s], kc, n0);
         }
         // wait (bounded) for the loads still in flight before leaving
         for (int i = max(0, nkb - STAGES); i < nkb; ++i) {
@@ -181,52 +206,83 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tAhi, const __grid_constant__ CU
             if (!mbar_wait(&bars->full[s], (uint32_t)((i / STAGES) & 1))) bars->failed = 1;
         }
     } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer
+        // ---------------- MMA issuer: every k-block accumulates into a fresh
+        // TMEM tile (b = i & 1), the correction products first while the
+        // tile is still small and the main product last, so that the
+        // tensor core's truncating FP32 accumulation touches each value only
+        // a few times; the epilogue sums the tiles with round-to-nearest adds
         for (int i = 0; i < nkb; ++i) {
             const int s = i % STAGES;
             const uint32_t ph = (uint32_t)((i / STAGES) & 1);
-            if (!mbar_wait(&bars->full[s], ph)) {
+            const int b = i & 1;
+            const uint32_t tu = (uint32_t)((i >> 1) & 1);
+            if (!mbar_wait(&bars->tempty[b], tu ^ 1) || !mbar_wait(&bars->full[s], ph)) {
                 bars->failed = 1;
                 break;
             }
             fence_after();
             const uint32_t base = su32(smem + (size_t)s * STAGE_BYTES);
+            const uint32_t d = tmem + (uint32_t)(b * BN);
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
                 const uint32_t off = kk * 32;
-                const uint64_t ahi = sdesc(base + off), alo = sdesc(base + TILE_BYTES + off);
-                const uint64_t bhi = sdesc(base + 2 * TILE_BYTES + off), blo = sdesc(base + 3 * TILE_BYTES + off);
-                const uint32_t acc0 = (i > 0 || kk > 0) ? 1u : 0u;
-                mma_bf16(tmem, ahi, bhi, acc0);
-                mma_bf16(tmem, ahi, blo, 1u);
-                mma_bf16(tmem, alo, bhi, 1u);
+                const uint64_t a0 = sdesc(base + off), a1 = sdesc(base + TILE_BYTES + off);
+                const uint64_t b0 = sdesc(base + NS * TILE_BYTES + off), b1 = sdesc(base + (NS + 1) * TILE_BYTES + off);
+                // lolo (two pieces, A and B the same block): the lo*lo term
+                // too, whose omission would bias every |z|^2 on the diagonal low
+                if (NS == 2 && lolo) mma_bf16(d, a1, b1, kk > 0 ? 1u : 0u);
+                mma_bf16(d, a0, b1, (kk > 0 || (NS == 2 && lolo)) ? 1u : 0u);
+                mma_bf16(d, a1, b0, 1u);
+                if constexpr (NS == 3) {
+                    const uint64_t a2 = sdesc(base + 2 * TILE_BYTES + off), b2 = sdesc(base + (NS + 2) * TILE_BYTES + off);
+                    mma_bf16(d, a0, b2, 1u);
+                    mma_bf16(d, a1, b1, 1u);
+                    mma_bf16(d, a2, b0, 1u);
+                }
+            }
+#pragma unroll
+            for (int kk = 0; kk < BK / 16; ++kk) {
+                const uint32_t off = kk * 32;
+                mma_bf16(d, sdesc(base + off), sdesc(base + NS * TILE_BYTES + off), 1u);
             }
             mma_commit(&bars->empty[s]);
+            mma_commit(&bars->tfull[b]);
         }
-        mma_commit(&bars->accum);
     } else if (warp >= 2) {
-        // ---------------- epilogue: TMEM lanes [32q, 32q+32) -> rows m0 + 32q + lane
+        // ---------------- epilogue: TMEM lanes [32q, 32q+32) -> rows m0 + 32q + lane,
+        // the k-block tiles summed in registers
         const int q = warp & 3;
-        const bool ok = (nkb == 0) || mbar_wait(&bars->accum, 0);
-        fence_after();
         const int m = m0 + 32 * q + lane;
-        float *Wz = W + (size_t)blockIdx.z * Mp * (size_t)Np;
-        if (!ok) atomicExch(err, 2);
-#pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
-            float v[32];
-            if (nkb > 0 && ok) {
-                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
-            } else {
+        float acc[BN];
 #pragma unroll
-                for (int t = 0; t < 32; ++t) v[t] = 0.f;
+        for (int t = 0; t < BN; ++t) acc[t] = 0.f;
+        bool ok = true;
+        for (int i = 0; i < nkb; ++i) {
+            const int b = i & 1;
+            const uint32_t tu = (uint32_t)((i >> 1) & 1);
+            if (!mbar_wait(&bars->tfull[b], tu)) {
+                ok = false;
+                break;
             }
-            if (m < Mp) {
+            fence_after();
 #pragma unroll
-                for (int t = 0; t < 32; ++t) {
-                    const int n = n0 + 32 * c + t;
-                    if (n < Np) Wz[(size_t)n * Mp + m] = v[t];
-                }
+            for (int c = 0; c < BN / 32; ++c) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(b * BN + 32 * c), v);
+#pragma unroll
+                for (int t = 0; t < 32; ++t) acc[32 * c + t] += v[t];
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars->tempty[b]);
+        }
+        if (!ok) atomicExch(err, 2);
+        float *Wz = W + (size_t)blockIdx.z * Mp * (size_t)Np;
+        if (m < Mp) {
+#pragma unroll
+            for (int t = 0; t < BN; ++t) {
+                const int n = n0 + t;
+                if (n < Np) Wz[(size_t)n * Mp + m] = acc[t];
             }
         }
     }
@@ -244,46 +300,64 @@ __device__ __forceinline__ void split2(float x, __nv_bfloat16 &hi, __nv_bfloat16
     hi = __float2bfloat16_rn(x);
     lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
+// x = p[0] + p[1] (+ p[2]): successive BF16 roundings of the remainder
+template <int NS> __device__ __forceinline__ void splitn(float x, __nv_bfloat16 *p) {
+    p[0] = __float2bfloat16_rn(x);
+    const float r = x - __bfloat162float(p[0]);
+    p[1] = __float2bfloat16_rn(r);
+    if constexpr (NS == 3) p[2] = __float2bfloat16_rn(r - __bfloat162float(p[1]));
+}
 
-// A' from Z (K x m, complex, column-major, ld): rows 2i, 2i+1 of length Kp.
-template <typename CT>
-__global__ void k_prep_tn_a(const CT *__restrict__ Z, int64_t ld, int64_t K, int m, int Kp, __nv_bfloat16 *__restrict__ hi,
-                            __nv_bfloat16 *__restrict__ lo) {
+// A' from Z (K x m, complex, column-major, ld): rows 2i, 2i+1 of length Kp,
+// one array per BF16 piece (pc[0..NS-1]).
+template <typename CT, int NS>
+__global__ void k_prep_tn_a(const CT *__restrict__ Z, int64_t ld, int64_t K, int m, int Kp, __nv_bfloat16 *__restrict__ p0,
+                            __nv_bfloat16 *__restrict__ p1, __nv_bfloat16 *__restrict__ p2) {
     const int i = blockIdx.y;
     const CT *z = Z + (size_t)i * ld;
-    __nv_bfloat16 *h0 = hi + (size_t)(2 * i) * Kp, *h1 = h0 + Kp;
-    __nv_bfloat16 *l0 = lo + (size_t)(2 * i) * Kp, *l1 = l0 + Kp;
+    __nv_bfloat16 *pc[3] = {p0, p1, p2};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < Kp / 2; k += (int64_t)gridDim.x * blockDim.x) {
         float re = 0.f, im = 0.f;
         if (k < K) {
             re = (float)z[k].x;
             im = (float)z[k].y;
         }
-        __nv_bfloat16 a, b, c, d;
-        split2(re, a, b);
-        split2(im, c, d);
-        h0[2 * k] = a; l0[2 * k] = b; h0[2 * k + 1] = c; l0[2 * k + 1] = d;
-        // i z = (-im, re)
-        __nv_bfloat16 na = __hneg(c), nb = __hneg(d);
-        h1[2 * k] = na; l1[2 * k] = nb; h1[2 * k + 1] = a; l1[2 * k + 1] = b;
+        __nv_bfloat16 a[3], c[3];
+        splitn<NS>(re, a);
+        splitn<NS>(im, c);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            __nv_bfloat16 *r0 = pc[q] + (size_t)(2 * i) * Kp, *r1 = r0 + Kp;
+            r0[2 * k] = a[q];
+            r0[2 * k + 1] = c[q];
+            r1[2 * k] = __hneg(c[q]);  // i z = (-im, re)
+            r1[2 * k + 1] = a[q];
+        }
     }
 }
 
 // B' from W (K x n, complex, column-major, ld): row j = [Re w_j, Im w_j].
-template <typename CT>
-__global__ void k_prep_tn_b(const CT *__restrict__ Wm, int64_t ld, int64_t K, int n, int Kp, __nv_bfloat16 *__restrict__ hi,
-                            __nv_bfloat16 *__restrict__ lo) {
+template <typename CT, int NS>
+__global__ void k_prep_tn_b(const CT *__restrict__ Wm, int64_t ld, int64_t K, int n, int Kp, __nv_bfloat16 *__restrict__ p0,
+                            __nv_bfloat16 *__restrict__ p1, __nv_bfloat16 *__restrict__ p2) {
     const int j = blockIdx.y;
     const CT *w = Wm + (size_t)j * ld;
-    __nv_bfloat16 *h = hi + (size_t)j * Kp, *l = lo + (size_t)j * Kp;
+    __nv_bfloat16 *pc[3] = {p0, p1, p2};
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < Kp / 2; k += (int64_t)gridDim.x * blockDim.x) {
         float re = 0.f, im = 0.f;
         if (k < K) {
             re = (float)w[k].x;
             im = (float)w[k].y;
         }
-        split2(re, h[2 * k], l[2 * k]);
-        split2(im, h[2 * k + 1], l[2 * k + 1]);
+        __nv_bfloat16 a[3], c[3];
+        splitn<NS>(re, a);
+        splitn<NS>(im, c);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            __nv_bfloat16 *r = pc[q] + (size_t)j * Kp;
+            r[2 * k] = a[q];
+            r[2 * k + 1] = c[q];
+        }
     }
 }
 
@@ -403,7 +477,10 @@ cudaError_t umma_prep_tn_a(const void *Z, int64_t ld, int64_t K, int m, UmmaOper
     op.rows = 2 * (int64_t)m;
     op.Kp = umma_kpad(K);
     dim3 grid((unsigned)std::min<int64_t>((op.Kp / 2 + 255) / 256, 64), m);
-    k_prep_tn_a<CT><<<grid, 256, 0, st>>>((const CT *)Z, ld, K, m, op.Kp, op.hi, op.lo);
+    if (op.lo2)
+        k_prep_tn_a<CT, 3><<<grid, 256, 0, st>>>((const CT *)Z, ld, K, m, op.Kp, op.hi, op.lo, op.lo2);
+    else
+        k_prep_tn_a<CT, 2><<<grid, 256, 0, st>>>((const CT *)Z, ld, K, m, op.Kp, op.hi, op.lo, nullptr);
     return cudaGetLastError();
 }
 
@@ -412,7 +489,10 @@ cudaError_t umma_prep_tn_b(const void *Wm, int64_t ld, int64_t K, int n, UmmaOpe
     op.rows = n;
     op.Kp = umma_kpad(K);
     dim3 grid((unsigned)std::min<int64_t>((op.Kp / 2 + 255) / 256, 64), n);
-    k_prep_tn_b<CT><<<grid, 256, 0, st>>>((const CT *)Wm, ld, K, n, op.Kp, op.hi, op.lo);
+    if (op.lo2)
+        k_prep_tn_b<CT, 3><<<grid, 256, 0, st>>>((const CT *)Wm, ld, K, n, op.Kp, op.hi, op.lo, op.lo2);
+    else
+        k_prep_tn_b<CT, 2><<<grid, 256, 0, st>>>((const CT *)Wm, ld, K, n, op.Kp, op.hi, op.lo, nullptr);
     return cudaGetLastError();
 }
 
@@ -431,46 +511,53 @@ cudaError_t umma_prep_nn_a(const void *A, int64_t lda, int64_t M, int k, UmmaOpe
     return e;
 }
 
-// Split-K count: enough CTAs to fill the GPU, and at most KB_CAP k-blocks
-// (K = 1024) accumulated in one TMEM tile.  The tensor-core FP32
-// accumulation drifts with the length of the chain (measured on a
-// 480 x 480 Gram over K = 80797: 1e-4 absolute with the whole K in one
-// chain); the split partials are summed in FP64 by k_finalize.
-constexpr int KB_CAP = 16;
+// Split-K count: enough CTAs to fill the GPU.  (Accuracy does not depend
+// on it: each k-block is its own accumulation chain in TMEM.)
 int umma_splits(int64_t Mp, int Np, int Kp) {
     const int tiles = (int)((Mp + BM - 1) / BM) * ((Np + BN - 1) / BN);
     const int KB = Kp / BK;
     int S = (2 * 148 + tiles - 1) / tiles;
-    S = std::max(1, std::min(S, KB / 4 > 0 ? KB / 4 : 1));
-    S = std::max(S, (KB + KB_CAP - 1) / KB_CAP);
-    return std::min(S, std::max(1, KB));
+    return std::max(1, std::min(S, KB / 4 > 0 ? KB / 4 : 1));
 }
 
 size_t umma_ws_bytes(int64_t Mp, int Np, int Kp) { return (size_t)umma_splits(Mp, Np, Kp) * Mp * Np * sizeof(float); }
 
+template <int NS>
+static cudaError_t launch_umma(const CUtensorMap *mA, const CUtensorMap *mB, dim3 grid, int Mp, int n, int KB, int kb_per,
+                               float *ws, int *err, int upper, int lolo, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_umma_gemm<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<NS>());
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    k_umma_gemm<NS><<<grid, THREADS, smem_bytes<NS>(), st>>>(mA[0], mA[1], mA[2], mB[0], mB[1], mB[2], Mp, n, KB, kb_per,
+                                                              ws, err, upper, lolo);
+    return cudaGetLastError();
+}
+
 template <typename CT>
 cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
-                      float *ws, int *err, cudaStream_t st, int upper) {
+                      float *ws, int *err, cudaStream_t st, int upper, int lolo) {
     cudaError_t e = get_encoder();
     if (e != cudaSuccess) return e;
     if (A.Kp != B.Kp || A.rows != 2 * (int64_t)m || B.rows != n) return cudaErrorInvalidValue;
-    CUtensorMap mAhi, mAlo, mBhi, mBlo;
-    if ((e = make_map(&mAhi, A.hi, A.rows, A.Kp, BM)) != cudaSuccess) return e;
-    if ((e = make_map(&mAlo, A.lo, A.rows, A.Kp, BM)) != cudaSuccess) return e;
-    if ((e = make_map(&mBhi, B.hi, B.rows, B.Kp, BN)) != cudaSuccess) return e;
-    if ((e = make_map(&mBlo, B.lo, B.rows, B.Kp, BN)) != cudaSuccess) return e;
-    static bool attr_set = false;
-    if (!attr_set) {
-        e = cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
+    // three BF16 pieces only when both operands carry them
+    const int ns = (A.lo2 && B.lo2) ? 3 : 2;
+    CUtensorMap mA[3], mB[3];
+    const __nv_bfloat16 *pa[3] = {A.hi, A.lo, ns == 3 ? A.lo2 : A.lo};
+    const __nv_bfloat16 *pb[3] = {B.hi, B.lo, ns == 3 ? B.lo2 : B.lo};
+    for (int q = 0; q < 3; ++q) {
+        if ((e = make_map(&mA[q], pa[q], A.rows, A.Kp, BM)) != cudaSuccess) return e;
+        if ((e = make_map(&mB[q], pb[q], B.rows, B.Kp, BN)) != cudaSuccess) return e;
     }
     const int KB = A.Kp / BK;
     const int S = umma_splits(A.rows, n, A.Kp);
     const int kb_per = (KB + S - 1) / S;
     dim3 grid((unsigned)((A.rows + BM - 1) / BM), (n + BN - 1) / BN, S);
-    k_umma_gemm<<<grid, THREADS, SMEM_BYTES, st>>>(mAhi, mAlo, mBhi, mBlo, (int)A.rows, n, KB, kb_per, ws, err, upper);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    e = ns == 3 ? launch_umma<3>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, 0, st)
+                : launch_umma<2>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, lolo, st);
+    if (e != cudaSuccess) return e;
     k_finalize<CT><<<blocks_for((size_t)m * n), 256, 0, st>>>(ws, S, m, n, (CT *)C, ldc, accumulate, upper);
     return cudaGetLastError();
 }
@@ -480,8 +567,8 @@ template cudaError_t umma_prep_tn_b<float2>(const void *, int64_t, int64_t, int,
 template cudaError_t umma_prep_tn_b<double2>(const void *, int64_t, int64_t, int, UmmaOperand &, cudaStream_t);
 template cudaError_t umma_prep_nn_a<float2>(const void *, int64_t, int64_t, int, UmmaOperand &, cudaStream_t);
 template cudaError_t umma_gemm<float2>(const UmmaOperand &, const UmmaOperand &, int, int, void *, int64_t, int, float *,
-                                       int *, cudaStream_t, int);
+                                       int *, cudaStream_t, int, int);
 template cudaError_t umma_gemm<double2>(const UmmaOperand &, const UmmaOperand &, int, int, void *, int64_t, int, float *,
-                                        int *, cudaStream_t, int);
+                                        int *, cudaStream_t, int, int);
 
 }  // namespace pwk

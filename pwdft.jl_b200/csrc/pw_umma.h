@@ -6,16 +6,20 @@
 
 namespace pwk {
 
-// A K-major split-BF16 operand: `rows` rows of Kp BF16 values (hi and lo).
+// A K-major split-BF16 operand: `rows` rows of Kp BF16 values per piece
+// (hi, lo, and optionally a third piece lo2).  A product runs with three
+// pieces (6 MMAs, ~2^-24) when both operands carry lo2, else with two
+// (3 MMAs, ~2^-17).
 struct UmmaOperand {
     __nv_bfloat16 *hi = nullptr;
     __nv_bfloat16 *lo = nullptr;
+    __nv_bfloat16 *lo2 = nullptr;
     int64_t rows = 0;
     int Kp = 0;
 };
 
 int umma_kpad(int64_t K);                          // padded 2K (multiple of 64)
-size_t umma_operand_bytes(int64_t rows, int64_t K);  // hi + lo bytes for `rows` rows
+size_t umma_operand_bytes(int64_t rows, int64_t K);  // hi + lo bytes for `rows` rows (one piece: half)
 size_t umma_ws_bytes(int64_t Mp, int Np, int Kp);    // split-K workspace
 
 // Operand builders (CT = float2 or double2 input element).
@@ -30,7 +34,9 @@ template <typename CT> cudaError_t umma_prep_nn_a(const void *A, int64_t lda, in
 // err: device int set non-zero if a bounded wait in the kernel expired.
 template <typename CT>
 // upper != 0: C is Hermitian and only C[i][j], i <= j, is formed and written.
+// lolo != 0 (two-piece operands from the same block, C = Z^H Z): add the
+// lo*lo product, whose omission biases the diagonal |z|^2 low.
 cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
-                      float *ws, int *err, cudaStream_t, int upper = 0);
+                      float *ws, int *err, cudaStream_t, int upper = 0, int lolo = 0);
 
 }  // namespace pwk
