@@ -193,6 +193,35 @@ int pw_update(pw_ctx *ctx, const double *rho, const double *Vps, double *VH,
 int pw_band_energies(pw_ctx *ctx, int ik, int dtype, const void *psi,
                      int64_t ld, int nb, const double *w, double *E2);
 
+/* ---- ionic forces --------------------------------------------------- */
+
+/* Tables of calc_forces_Ps_loc! (calc_forces_Ps_loc.jl:20-57), once per
+ * cell: G (host, 3 x Ng, the density sphere of pw_set_density_sphere in its
+ * order) and VlocG (host, Ng x nspecies) = eval_Vloc_G of each species on
+ * those G (without the 1/CellVolume factor, which cancels). */
+int pw_set_force_tables(pw_ctx *ctx, int nspecies, const double *VlocG, const double *G);
+
+/* calc_forces_Ps_loc! (calc_forces_Ps_loc.jl:13-71): F (host, 3 x natoms)
+ * from rho (device, N) and the atoms' positions (host, 3 x natoms, bohr)
+ * and species (host, 0-based). */
+int pw_forces_local(pw_ctx *ctx, const double *rho, int natoms, const double *pos,
+                    const int32_t *species, double *F);
+
+/* The (G+k) vectors of k-point ik (host, 3 x Ngw in the idx_gw2r order),
+ * used by calc_dbetaNL (calc_forces_Ps_nloc.jl:347-391). */
+int pw_set_gkvec(pw_ctx *ctx, int ik, const double *gk);
+
+/* Atom of each projector (host, NbetaNL, 0-based, nondecreasing as in
+ * PsPotNL.jl:147-195). */
+int pw_set_nonlocal_atoms(pw_ctx *ctx, int natoms, const int32_t *atom_of_beta);
+
+/* calc_forces_Ps_nloc! for GTH (calc_forces_Ps_nloc.jl:291-411) of one
+ * k-point: F (host, 3 x natoms) = sum_s 2 w_s Re(h_ij conj(B_i) dB_j) over
+ * each atom's (ibeta, jbeta, h_ij), B = betaNL' psi, dB = dbetaNL' psi;
+ * psi device Ngw x nb (ld), w (host, nb) = wk * Focc.  Overwrites F. */
+int pw_forces_nonlocal(pw_ctx *ctx, int ik, int dtype, const void *psi, int64_t ld,
+                       int nb, const double *w, double *F);
+
 /* ortho_sqrt!(psi) (ortho_sqrt.jl:1-11): psi := psi * inv(sqrt(psi'psi)),
  * psi device Ngw x nb (ld), in place. */
 int pw_ortho_sqrt(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw,

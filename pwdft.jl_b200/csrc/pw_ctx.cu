@@ -37,6 +37,7 @@ struct KData {
     float2 *d_beta32 = nullptr;
     UmmaOperand beta_tn;  // split-BF16 betaNL for betaNL' psi   (tensor-core path)
     UmmaOperand beta_nn;  // split-BF16 betaNL^H for betaNL * P  (tensor-core path)
+    double *d_gk = nullptr;  // (G+k) vectors, 3 x Ngw (forces)
 };
 
 constexpr int kMaxV64 = 8;  // complex values per thread per round in the FP64 FFT stages
@@ -90,6 +91,12 @@ struct pw_ctx {
     DevBuf slots[32];         // grow-only scratch for the eigensolver and LOBPCG
     KData dens;               // the density G-sphere (for Poisson_solve! on the device)
     bool have_dens = false;
+    // forces: G vectors of the density sphere (3 x Ng), V_sp(G) per species
+    // (Ng x nspecies), projector rows of each atom (natoms + 1 offsets)
+    double *d_fG = nullptr, *d_fV = nullptr;
+    int f_nsp = 0;
+    int *d_atom_rows = nullptr;
+    int f_natoms = 0;
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -860,33 +867,45 @@ int pwk_density_launch(pw_ctx *c, pwk::FftLaunch *L, const double **G2, int *Ng,
 int pwk_set_vloc_device(pw_ctx *c, const double *V, int nspin) { return set_vloc_common(c, V, nspin, true); }
 const double *pwk_gk2(const pw_ctx *c, int ik) { return c->k[ik].d_Gk2; }
 
-// P = betaNL' psi and P2 = D P for k-point ik into the context's buffers
-int pwk_projections(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, int nb, const double2 **P,
-                    const double2 **P2, int *nbeta) {
-    *nbeta = c->nbeta;
-    if (c->nbeta <= 0) return PW_OK;
+// out (nbeta x nb, FP64 complex) = betaNL' psi for k-point ik (betaNL' psi
+// with three BF16 pieces on the mixed path, as in op_H)
+int pwk_beta_dot(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, int nb, double2 *out) {
     const KData &kd = c->k[ik];
     const void *beta = dtype == PW_C128 ? (const void *)kd.d_beta64 : (const void *)kd.d_beta32;
-    if (!beta || !c->have_D) return fail(c, PW_ERR_STATE, "projectors of k-point %d are not set", ik);
+    if (c->nbeta <= 0 || !beta) return fail(c, PW_ERR_STATE, "projectors of k-point %d are not set", ik);
     int s;
-    const size_t pb = (size_t)c->nbeta * nb * sizeof(double2);
-    if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb))) return s;
     cudaStream_t st = c->stream;
     if (dtype == PW_C64 && c->use_umma) {
         UmmaOperand B;
         if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, nb, kd.Ngw, B, &c->um_b_lo2))) return s;
         CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
         if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
-        CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, c->P.p, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
+        CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, out, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
+        c->launches += 3;
     } else {
         if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb)))) return s;
         if (dtype == PW_C128)
-            CK(c, (gemm_tn<double>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+            CK(c, (gemm_tn<double>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, out, c->nbeta, 0, c->gemm_ws.p, st)));
         else
-            CK(c, (gemm_tn<float>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
+            CK(c, (gemm_tn<float>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, out, c->nbeta, 0, c->gemm_ws.p, st)));
+        c->launches += 2;
     }
+    return PW_OK;
+}
+
+// P = betaNL' psi and P2 = D P for k-point ik into the context's buffers
+int pwk_projections(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, int nb, const double2 **P,
+                    const double2 **P2, int *nbeta) {
+    *nbeta = c->nbeta;
+    if (c->nbeta <= 0) return PW_OK;
+    if (!c->have_D) return fail(c, PW_ERR_STATE, "nonlocal coefficients are not set");
+    int s;
+    const size_t pb = (size_t)c->nbeta * nb * sizeof(double2);
+    if ((s = ensure(c, c->P, pb)) || (s = ensure(c, c->P2, pb))) return s;
+    cudaStream_t st = c->stream;
+    if ((s = pwk_beta_dot(c, ik, dtype, psi, ld, nb, (double2 *)c->P.p))) return s;
     CK(c, apply_dcsr(c->nbeta, nb, c->d_Drow, c->d_Dcol, c->d_Dval, (const double2 *)c->P.p, (double2 *)c->P2.p, st));
-    c->launches += 3;
+    c->launches += 1;
     *P = (const double2 *)c->P.p;
     *P2 = (const double2 *)c->P2.p;
     return PW_OK;
@@ -901,5 +920,86 @@ extern "C" int pw_set_density_sphere(pw_ctx *c, int64_t Ng, const int64_t *idx_g
     int s = build_kdata(c, c->dens, Ng, idx_g2r, index_base, G2);
     if (s) return s;
     c->have_dens = true;
+    return PW_OK;
+}
+
+// ------------------------------------------------------------------ forces
+extern "C" int pw_set_force_tables(pw_ctx *c, int nspecies, const double *VlocG, const double *G) {
+    if (!c) return PW_ERR_ARG;
+    if (!c->have_dens) return fail(c, PW_ERR_STATE, "call pw_set_density_sphere before pw_set_force_tables");
+    if (nspecies <= 0 || !VlocG || !G) return fail(c, PW_ERR_ARG, "bad force tables");
+    CK(c, cudaSetDevice(c->device));
+    const size_t ng = (size_t)c->dens.Ngw;
+    dfree(c, c->d_fG);
+    dfree(c, c->d_fV);
+    c->d_fG = nullptr;
+    c->d_fV = nullptr;
+    int s;
+    if ((s = dalloc(c, &c->d_fG, 3 * ng)) || (s = dalloc(c, &c->d_fV, ng * nspecies))) return s;
+    CK(c, cudaMemcpy(c->d_fG, G, 3 * ng * sizeof(double), cudaMemcpyHostToDevice));
+    CK(c, cudaMemcpy(c->d_fV, VlocG, ng * nspecies * sizeof(double), cudaMemcpyHostToDevice));
+    c->f_nsp = nspecies;
+    return PW_OK;
+}
+
+extern "C" int pw_set_gkvec(pw_ctx *c, int ik, const double *gk) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik))) return s;
+    if (!gk) return fail(c, PW_ERR_ARG, "NULL G+k vectors");
+    CK(c, cudaSetDevice(c->device));
+    KData &kd = c->k[ik];
+    if (!kd.d_gk && (s = dalloc(c, &kd.d_gk, 3 * (size_t)kd.Ngw))) return s;
+    CK(c, cudaMemcpy(kd.d_gk, gk, 3 * (size_t)kd.Ngw * sizeof(double), cudaMemcpyHostToDevice));
+    return PW_OK;
+}
+
+extern "C" int pw_set_nonlocal_atoms(pw_ctx *c, int natoms, const int32_t *atom_of_beta) {
+    if (!c) return PW_ERR_ARG;
+    if (c->nbeta <= 0) return fail(c, PW_ERR_STATE, "call pw_set_nonlocal before pw_set_nonlocal_atoms");
+    if (natoms <= 0 || !atom_of_beta) return fail(c, PW_ERR_ARG, "bad projector atom list");
+    // the projectors of one atom are contiguous (PsPotNL.jl:147-195 order)
+    std::vector<int> rows(natoms + 1, 0);
+    int prev = -1;
+    for (int b = 0; b < c->nbeta; ++b) {
+        const int a = atom_of_beta[b];
+        if (a < 0 || a >= natoms || a < prev) return fail(c, PW_ERR_ARG, "projector %d: atom %d out of order", b, a);
+        for (int q = prev + 1; q <= a; ++q) rows[q] = b;
+        prev = a;
+    }
+    for (int q = prev + 1; q <= natoms; ++q) rows[q] = c->nbeta;
+    CK(c, cudaSetDevice(c->device));
+    dfree(c, c->d_atom_rows);
+    c->d_atom_rows = nullptr;
+    int s;
+    if ((s = upload(c, &c->d_atom_rows, rows))) return s;
+    c->f_natoms = natoms;
+    return PW_OK;
+}
+
+int pwk_force_local_tables(pw_ctx *c, const double **G, const double **V, int *nsp, int *ng) {
+    if (!c->d_fG || !c->have_dens) return fail(c, PW_ERR_STATE, "force tables are not set (pw_set_force_tables)");
+    *G = c->d_fG;
+    *V = c->d_fV;
+    *nsp = c->f_nsp;
+    *ng = c->dens.Ngw;
+    return PW_OK;
+}
+int pwk_force_nonlocal_tables(pw_ctx *c, int ik, const double **gk, const int **atom_rows, int *natoms, const int **rowptr,
+                              const int **col, const double **val, int *nbeta) {
+    if (!c->k[ik].d_gk) return fail(c, PW_ERR_STATE, "G+k vectors of k-point %d are not set (pw_set_gkvec)", ik);
+    if (!c->d_atom_rows) return fail(c, PW_ERR_STATE, "projector atoms are not set (pw_set_nonlocal_atoms)");
+    if (!c->have_D) return fail(c, PW_ERR_STATE, "nonlocal coefficients are not set");
+    *gk = c->k[ik].d_gk;
+    *atom_rows = c->d_atom_rows;
+    *natoms = c->f_natoms;
+    *rowptr = c->d_Drow;
+    *col = c->d_Dcol;
+    *val = c->d_Dval;
+    *nbeta = c->nbeta;
+    return PW_OK;
+}
+int pwk_grid_points(const pw_ctx *c, size_t *N) {
+    *N = c->N;
     return PW_OK;
 }

@@ -18,6 +18,8 @@ enum ScratchSlot {
     SL_LOB_Q, SL_LOB_HQ, SL_LOB_TMP1, SL_LOB_TMP2, SL_LOB_SMALL, SL_LOB_EIGW, SL_LOB_EIGSTAT,
     // host drop-in staging of pw_lobpcg_host
     SL_HOST_C128, SL_HOST_C64,
+    // forces
+    SL_FRC_A, SL_FRC_B, SL_FRC_C,
     SL_COUNT
 };
 static_assert(SL_COUNT <= 32, "pw_ctx holds 32 scratch slots");

@@ -232,9 +232,10 @@ static size_t plane_smem(const FftLaunch &L) {
     return ((size_t)L.kp.N1 + L.kp.N2 + (size_t)L.kp.Nxa * L.kp.N2 + (size_t)L.Jc * L.kp.N1) * sizeof(double2);
 }
 
-// rho(r) (device, N) -> V_H(r) (device, N): Poisson_solve!
-static int poisson(pw_ctx *c, const double *rho, double *VH) {
-    FftLaunch L;
+// rho(r) (device, N) -> R_to_G(rho) on the density sphere (device, Ng),
+// unnormalised (the reference's fft); A: the plane intermediate.
+static int density_to_G(pw_ctx *c, const double *rho, FftLaunch &L, double2 **gout, double2 **Aout, int *Ngout,
+                        size_t *Nout, const double **G2out) {
     const double *G2 = nullptr;
     int Ng = 0;
     size_t N = 0;
@@ -251,12 +252,41 @@ static int poisson(pw_ctx *c, const double *rho, double *VH) {
     k_plane_r2g<<<L.kp.N3, 256, smem, st>>>(L.kp, L.dx, L.dy, (const double2 *)L.twx, (const double2 *)L.twy, rho, A, L.Jc);
     CKU(c, cudaGetLastError());
     CKU(c, launch_zfwd<double>(L, A, g, g, Ng, 1, 0, st));  // sphere coefficients of R_to_G(rho)
+    pwk_count_launches(c, 2);
+    *gout = g;
+    *Aout = A;
+    *Ngout = Ng;
+    *Nout = N;
+    *G2out = G2;
+    return PW_OK;
+}
+
+int pwk_density_to_G(pw_ctx *c, const double *rho, const double2 **rhoG, int *Ng) {
+    FftLaunch L;
+    double2 *g = nullptr, *A = nullptr;
+    size_t N = 0;
+    const double *G2 = nullptr;
+    RK(density_to_G(c, rho, L, &g, &A, Ng, &N, &G2));
+    *rhoG = g;
+    return PW_OK;
+}
+
+// rho(r) (device, N) -> V_H(r) (device, N): Poisson_solve!
+static int poisson(pw_ctx *c, const double *rho, double *VH) {
+    FftLaunch L;
+    const double *G2 = nullptr;
+    int Ng = 0;
+    size_t N = 0;
+    double2 *A = nullptr, *g = nullptr;
+    RK(density_to_G(c, rho, L, &g, &A, &Ng, &N, &G2));
+    cudaStream_t st = pwk_stream(c);
+    const size_t smem = plane_smem(L);
     k_poisson_scale<<<(Ng + 255) / 256, 256, 0, st>>>(g, G2, Ng);
     CKU(c, launch_zinv<double>(L, g, Ng, 1, A, st));
     k_plane_g2r<<<L.kp.N3, 256, smem, st>>>(L.kp, L.dx, L.dy, (const double2 *)L.twx, (const double2 *)L.twy, A, VH,
                                             1.0 / (double)N, L.Jc);
     CKU(c, cudaGetLastError());
-    pwk_count_launches(c, 5);
+    pwk_count_launches(c, 3);
     return PW_OK;
 }
 

@@ -69,6 +69,11 @@ SIGNATURES = {
     "pw_poisson": (_i, [_vp, _vp, _vp]),
     "pw_update": (_i, [_vp, _vp, _vp, _vp, _vp, _dp]),
     "pw_band_energies": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _dp]),
+    "pw_set_force_tables": (_i, [_vp, _i, _dp, _dp]),
+    "pw_forces_local": (_i, [_vp, _vp, _i, _dp, _i32p, _dp]),
+    "pw_set_gkvec": (_i, [_vp, _i, _dp]),
+    "pw_set_nonlocal_atoms": (_i, [_vp, _i, _i32p]),
+    "pw_forces_nonlocal": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _dp]),
     "pw_op_H_host": (_i, [_vp, _i, _i, _dp, _dp, _i64, _i, _u, _i]),
     "pw_calc_rhoe_host": (_i, [_vp, _i, _dp, _i64, _i, _dp, _dp, _i, _i]),
     "pw_good_fft_order": (_i, [_i]),

@@ -222,6 +222,45 @@ class Context:
                                     C.c_void_p(Vxc.data_ptr()) if Vxc is not None else None, _dptr(E3)))
         return E3
 
+    # ---------------------------------------------------------------- forces
+    def set_force_tables(self, VlocG, G):
+        """VlocG (Ng, nspecies): eval_Vloc_G per species on the density sphere
+        (no 1/Omega); G (Ng, 3) of that sphere, in its order."""
+        V = np.ascontiguousarray(np.asarray(VlocG, dtype=np.float64).T)   # column-major Ng x nspecies
+        g = np.ascontiguousarray(np.asarray(G, dtype=np.float64))          # column-major 3 x Ng
+        self._keep_force = (V, g)
+        self._chk(self._L.pw_set_force_tables(self.h, V.shape[0], _dptr(V), _dptr(g)))
+
+    def forces_local(self, rho, positions, species):
+        """calc_forces_Ps_loc: rho device (N,), positions (3, natoms), species (natoms,) -> F (3, natoms)."""
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).T)
+        sp = np.ascontiguousarray(np.asarray(species, dtype=np.int32))
+        F = np.zeros((pos.shape[0], 3))
+        self.use_torch_stream()
+        self._chk(self._L.pw_forces_local(self.h, C.c_void_p(rho.data_ptr()), pos.shape[0], _dptr(pos),
+                                          sp.ctypes.data_as(C.POINTER(C.c_int32)), _dptr(F)))
+        return F.T.copy()
+
+    def set_gkvec(self, ik, gk):
+        """gk (Ngw, 3): the G+k vectors of k-point ik in the idx_gw2r order."""
+        g = np.ascontiguousarray(np.asarray(gk, dtype=np.float64))
+        self._chk(self._L.pw_set_gkvec(self.h, ik, _dptr(g)))
+
+    def set_nonlocal_atoms(self, natoms, atom_of_beta):
+        a = np.ascontiguousarray(np.asarray(atom_of_beta, dtype=np.int32))
+        self._chk(self._L.pw_set_nonlocal_atoms(self.h, int(natoms), a.ctypes.data_as(C.POINTER(C.c_int32))))
+        self._force_natoms = int(natoms)
+
+    def forces_nonlocal(self, ik, psi, w):
+        """calc_forces_Ps_nloc of one k-point: psi device (nb, Ngw), w (nb,) = wk * Focc -> F (3, natoms)."""
+        nb, ld = psi.shape
+        ww = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        F = np.zeros((self._force_natoms, 3))
+        self.use_torch_stream()
+        self._chk(self._L.pw_forces_nonlocal(self.h, ik, dtype_code(psi), C.c_void_p(psi.data_ptr()), ld, nb,
+                                             _dptr(ww), _dptr(F)))
+        return F.T.copy()
+
     def band_energies(self, ik, psi, w):
         """(E_kin, E_Ps_nloc) contributions of k-point ik with weights w = wk*Focc."""
         nb, ld = psi.shape
