@@ -227,6 +227,17 @@ int pw_forces_nonlocal(pw_ctx *ctx, int ik, int dtype, const void *psi, int64_t 
 int pw_ortho_sqrt(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw,
                   int nb);
 
+/* ortho_cholesky!(Ham, psi) (ortho_sqrt.jl:80-89): O = psi'psi = U^H U,
+ * psi := psi / U, psi device Ngw x nb (ld), in place. */
+int pw_ortho_cholesky(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw, int nb);
+
+/* calc_grad(Ham, psi) (calc_grad.jl:1-57) for k-point ik, spin ispin:
+ * grad = wk f_i (H psi_i - sum_j psi_j <psi_j|H psi_i>), plus
+ * psi (Hred F - F Hred)/2 when Focc (host, nb) is not all 2 or all 1.
+ * psi and grad device Ngw x nb (ld), distinct. */
+int pw_calc_grad(pw_ctx *ctx, int ik, int ispin, int dtype, const void *psi, void *grad,
+                 int64_t ld, int nb, const double *Focc, double wk);
+
 /* ---- host drop-ins (the reference's Julia arrays) ------------------- */
 
 /* op_H!(Ham, psi, Hpsi) and friends on host ComplexF64 arrays; compute

@@ -24,6 +24,12 @@ def ortho_sqrt(psi):
     return psi @ ((U / np.sqrt(w)) @ U.conj().T)
 
 
+def ortho_cholesky(psi):
+    """ortho_sqrt.jl:80-89: psi / U with psi'psi = U^H U."""
+    U = np.linalg.cholesky(psi.conj().T @ psi).conj().T
+    return np.linalg.solve(U.T, psi.T).T
+
+
 def _herm_upper(A):
     """Hermitian(A) with the upper triangle (Julia default uplo=:U)."""
     U = np.triu(A)

@@ -94,3 +94,15 @@ def calc_rhoe(Ham, psiks, Focc=None, chunk=32):
             w = pw.kpoints.wk[ik] * Focc[b0:b1, ik]
             rho += (w[:, None] * (ctmp.real ** 2 + ctmp.imag ** 2)).sum(axis=0)
     return rho
+
+
+def calc_grad(Ham, psi, ik, Focc, wk):
+    """calc_grad.jl:1-57: grad_i = wk f_i (H psi_i - sum_j psi_j <psi_j|H psi_i>), plus
+    psi (Hred F - F Hred)/2 unless all f are 2 or all are 1."""
+    Hpsi = op_H(Ham, psi, ik)
+    Hred = psi.conj().T @ Hpsi
+    grad = (Hpsi - psi @ Hred) * (wk * Focc)[None, :]
+    if not (np.all(Focc == 2.0) or np.all(Focc == 1.0)):
+        F = np.diag(Focc)
+        grad = grad + psi @ (0.5 * (Hred @ F - F @ Hred))
+    return grad

@@ -472,3 +472,99 @@ extern "C" int pw_ortho_sqrt(pw_ctx *c, int dtype, void *psi, int64_t ld, int64_
     CKR(c, cudaStreamSynchronize(r.st));
     return PW_OK;
 }
+
+// ortho_cholesky!(psi) (ortho_sqrt.jl:80-89): O = psi'psi = U^H U (Cholesky),
+// psi := psi / U.
+extern "C" int pw_ortho_cholesky(pw_ctx *c, int dtype, void *psi, int64_t ld, int64_t ngw, int nb) {
+    if (!c) return PW_ERR_ARG;
+    if (dtype != PW_C128 && dtype != PW_C64) return pwk_fail(c, PW_ERR_ARG, "unknown dtype");
+    if (!psi || nb <= 0 || ngw <= 0 || ld < ngw) return pwk_fail(c, PW_ERR_ARG, "bad pw_ortho_cholesky arguments");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    Run r{};
+    r.c = c;
+    r.st = pwk_stream(c);
+    r.dtype = dtype;
+    r.ngw = (int)ngw;
+    r.ldq = ld;
+    r.nb = nb;
+    const size_t es = dtype == PW_C128 ? sizeof(double2) : sizeof(float2);
+    const size_t nn = (size_t)nb * nb;
+    double2 *O = nullptr, *Rinv = nullptr;
+    char *tmp = nullptr;
+    RK(pwk_scratch(c, pwk::SL_LOB_SMALL, 2 * nn * sizeof(double2) + 256, (void **)&O));
+    Rinv = O + nn;
+    RK(pwk_scratch(c, pwk::SL_LOB_TMP1, (size_t)ld * nb * es, (void **)&tmp));
+    r.eigw_bytes = pwk::eig_work_bytes(nb, 1);
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGSTAT, 64, (void **)&r.eigstat));
+    RK(gram_h(r, (const char *)psi, nb, (const char *)psi, O, nb));
+    RK(chol_rinv(r, O, nb, Rinv));
+    RK(pw_rotate(c, dtype, ngw, nb, nb, psi, ld, (const double *)Rinv, nb, tmp, ld, 0));
+    CKR(c, cudaMemcpy2DAsync(psi, ld * es, tmp, ld * es, ngw * es, nb, cudaMemcpyDeviceToDevice, r.st));
+    CKR(c, cudaStreamSynchronize(r.st));
+    return PW_OK;
+}
+
+// calc_grad (calc_grad.jl:1-57): grad_i = wk f_i (H psi_i - sum_j psi_j <psi_j|H psi_i>),
+// plus psi Q with Q = (Hred F - F Hred)/2 when the occupations are not all
+// equal to 2 or all equal to 1 (Hred = psi'H psi, F = diag(f)).
+// As matrices: grad = (H psi) D + psi (-Hred D + Q), D = wk F.
+namespace {
+__global__ void k_grad_coef(const double2 *__restrict__ Hm, const double *__restrict__ f, double wk, int nb, int frac,
+                            double2 *__restrict__ U) {
+    const size_t total = (size_t)nb * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int j = (int)(t / nb), i = (int)(t - (size_t)j * nb);
+        const double2 h = Hm[t];
+        double s = -wk * f[j];
+        if (frac) s += 0.5 * (f[j] - f[i]);
+        U[t] = make_double2(h.x * s, h.y * s);
+    }
+}
+template <typename T>
+__global__ void k_scale_cols_w(Cx<T> *__restrict__ X, int64_t ld, int ngw, int nb, const double *__restrict__ f, double wk) {
+    const size_t total = (size_t)ngw * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t / ngw), g = (int)(t - (size_t)b * ngw);
+        const T s = (T)(wk * f[b]);
+        Cx<T> &x = X[(size_t)b * ld + g];
+        x = cmake(x.x * s, x.y * s);
+    }
+}
+}  // namespace
+
+extern "C" int pw_calc_grad(pw_ctx *c, int ik, int ispin, int dtype, const void *psi, void *grad, int64_t ld, int nb,
+                            const double *Focc, double wk) {
+    if (!c) return PW_ERR_ARG;
+    if (dtype != PW_C128 && dtype != PW_C64) return pwk_fail(c, PW_ERR_ARG, "unknown dtype");
+    if (ik < 0 || ik >= pwk_nkpt(c)) return pwk_fail(c, PW_ERR_ARG, "bad k-point index");
+    const int ngw = pwk_ngw(c, ik);
+    if (!psi || !grad || !Focc || nb <= 0 || ld < ngw || psi == grad) return pwk_fail(c, PW_ERR_ARG, "bad pw_calc_grad arguments");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st = pwk_stream(c);
+    bool all2 = true, all1 = true;
+    for (int i = 0; i < nb; ++i) {
+        all2 = all2 && Focc[i] == 2.0;
+        all1 = all1 && Focc[i] == 1.0;
+    }
+    const int frac = (all2 || all1) ? 0 : 1;
+    const size_t nn = (size_t)nb * nb;
+    double2 *Hm = nullptr, *U = nullptr;
+    double *df = nullptr;
+    RK(pwk_scratch(c, pwk::SL_LOB_SMALL, 2 * nn * sizeof(double2) + (size_t)nb * sizeof(double) + 256, (void **)&Hm));
+    U = Hm + nn;
+    df = (double *)(U + nn);
+    CKR(c, cudaMemcpyAsync(df, Focc, (size_t)nb * sizeof(double), cudaMemcpyHostToDevice, st));
+    RK(pw_apply(c, ik, ispin, dtype, psi, grad, ld, nb, PW_OP_H));
+    RK(pw_gram(c, dtype, ngw, nb, nb, psi, ld, grad, ld, (double *)Hm, nb, 0));
+    k_grad_coef<<<blocks_for(nn), 256, 0, st>>>(Hm, df, wk, nb, frac, U);
+    const int nblk = blocks_for((size_t)ngw * nb);
+    if (dtype == PW_C128)
+        k_scale_cols_w<double><<<nblk, 256, 0, st>>>((double2 *)grad, ld, ngw, nb, df, wk);
+    else
+        k_scale_cols_w<float><<<nblk, 256, 0, st>>>((float2 *)grad, ld, ngw, nb, df, wk);
+    CKR(c, cudaGetLastError());
+    RK(pw_rotate(c, dtype, ngw, nb, nb, psi, ld, (const double *)U, nb, grad, ld, 1));
+    pwk_count_launches(c, 2);
+    return PW_OK;
+}

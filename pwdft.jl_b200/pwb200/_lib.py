@@ -69,6 +69,8 @@ SIGNATURES = {
     "pw_poisson": (_i, [_vp, _vp, _vp]),
     "pw_update": (_i, [_vp, _vp, _vp, _vp, _vp, _dp]),
     "pw_band_energies": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _dp]),
+    "pw_ortho_cholesky": (_i, [_vp, _i, _vp, _i64, _i64, _i]),
+    "pw_calc_grad": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _dp, _d]),
     "pw_set_force_tables": (_i, [_vp, _i, _dp, _dp]),
     "pw_forces_local": (_i, [_vp, _vp, _i, _dp, _i32p, _dp]),
     "pw_set_gkvec": (_i, [_vp, _i, _dp]),

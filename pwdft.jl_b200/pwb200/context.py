@@ -222,6 +222,23 @@ class Context:
                                     C.c_void_p(Vxc.data_ptr()) if Vxc is not None else None, _dptr(E3)))
         return E3
 
+    def ortho_cholesky(self, psi):
+        """ortho_cholesky!: psi (nb, Ngw) device block := psi / chol(psi'psi)."""
+        nb, ld = psi.shape
+        self.use_torch_stream()
+        self._chk(self._L.pw_ortho_cholesky(self.h, dtype_code(psi), C.c_void_p(psi.data_ptr()), ld, ld, nb))
+
+    def calc_grad(self, ik, ispin, psi, Focc, wk):
+        """calc_grad: returns grad (same shape and dtype as psi (nb, Ngw))."""
+        import torch
+        nb, ld = psi.shape
+        g = torch.empty_like(psi)
+        f = np.ascontiguousarray(np.asarray(Focc, dtype=np.float64))
+        self.use_torch_stream()
+        self._chk(self._L.pw_calc_grad(self.h, ik, ispin, dtype_code(psi), C.c_void_p(psi.data_ptr()),
+                                       C.c_void_p(g.data_ptr()), ld, nb, _dptr(f), float(wk)))
+        return g
+
     # ---------------------------------------------------------------- forces
     def set_force_tables(self, VlocG, G):
         """VlocG (Ng, nspecies): eval_Vloc_G per species on the density sphere

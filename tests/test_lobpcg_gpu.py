@@ -122,3 +122,46 @@ def test_ortho_sqrt(ctx_fcc, prec):
     got = X.cpu().numpy().T.astype(np.complex128)
     assert np.abs(got - ref).max() < (1e-10 if prec == "c128" else 5e-4)
     assert np.abs(got.conj().T @ got - np.eye(12)).max() < (1e-12 if prec == "c128" else 1e-4)
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_ortho_cholesky(ctx_fcc, prec):
+    """ortho_cholesky! (ortho_sqrt.jl:80-89) against the oracle."""
+    import torch
+    from oracle import lobpcg
+    H, ctx, rng = ctx_fcc
+    ngw = H.pw.gvecw.Ngw[0]
+    psi = rng.standard_normal((ngw, 8)) + 1j * rng.standard_normal((ngw, 8))
+    ref = lobpcg.ortho_cholesky(psi)
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    X = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda().to(dt).contiguous()
+    ctx.ortho_cholesky(X)
+    got = X.cpu().numpy().T.astype(np.complex128)
+    tol = 1e-11 if prec == "c128" else 2e-5
+    assert np.abs(got - ref).max() < tol * np.abs(ref).max()
+    assert np.abs(got.conj().T @ got - np.eye(8)).max() < (1e-11 if prec == "c128" else 5e-5)
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+@pytest.mark.parametrize("frac", [False, True])
+def test_calc_grad(ctx_fcc, prec, frac):
+    """calc_grad (calc_grad.jl:1-57) against the oracle, integer occupations
+    and fractional ones (the psi (Hred F - F Hred)/2 term)."""
+    import torch
+    from oracle import ops, lobpcg
+    H, ctx, rng = ctx_fcc
+    ik = 1
+    ngw = H.pw.gvecw.Ngw[ik]
+    psi = lobpcg.ortho_sqrt(rng.standard_normal((ngw, 8)) + 1j * rng.standard_normal((ngw, 8)))
+    Focc = np.linspace(2.0, 0.3, 8) if frac else np.full(8, 2.0)
+    wk = float(H.pw.kpoints.wk[ik])
+    ref = ops.calc_grad(H, psi, ik, Focc, wk)
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    X = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda().to(dt).contiguous()
+    g = ctx.calc_grad(ik, 0, X, Focc, wk)
+    got = g.cpu().numpy().T.astype(np.complex128)
+    # mixed: the FP32 op_H (2e-5) plus the split-BF16x3 rotation psi Hred,
+    # whose terms (|Hred| ~ 10 Ha for random vectors) cancel against H psi
+    tol = 1e-11 if prec == "c128" else 1e-4
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    assert err < tol, err
