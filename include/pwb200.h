@@ -171,6 +171,18 @@ int pw_lobpcg(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
               int nb, double tol, int nitermax, int nconv, double *evals,
               int *niter);
 
+/* diag_davidson_qe!(Ham, evc; EBANDS_THR = tol, NiterMax = nitermax) for
+ * k-point ik (diag_davidson_qe_v2.jl:38-216): the QE-style block Davidson
+ * with Nvecx = 2 nb and restart, S = identity (norm-conserving).  X (device,
+ * Ngw x nb, ld) is overwritten with the Ritz vectors evc, evals (host, nb)
+ * with the Ritz values; a root is converged when its Ritz value moved by
+ * less than tol in an iteration.  Needs 2 nb <= Ngw.  dtype as pw_lobpcg;
+ * niter (host, may be NULL) receives the iteration count (+1000 when the
+ * mixed-precision reduced overlap lost definiteness and the iteration
+ * stopped on the previous step's Ritz vectors). */
+int pw_davidson(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
+                int nb, double tol, int nitermax, double *evals, int *niter);
+
 /* ---- update! and energies on the device ----------------------------- */
 
 /* The density G-sphere (PWGrid.gvec: idx_g2r, G2, sorted by G2 so that
@@ -249,6 +261,11 @@ int pw_op_H_host(pw_ctx *ctx, int ik, int ispin, const double *psi,
 int pw_lobpcg_host(pw_ctx *ctx, int ik, int ispin, int dtype, double *X,
                    int64_t ld, int nb, double tol, int nitermax, int nconv,
                    double *evals, int *niter);
+/* diag_davidson_qe!(Ham, evc) for k-point ik on the reference's host array
+ * evc (Ngw x nb ComplexF64, ld), copied in and out around pw_davidson. */
+int pw_davidson_host(pw_ctx *ctx, int ik, int ispin, int dtype, double *X,
+                     int64_t ld, int nb, double tol, int nitermax,
+                     double *evals, int *niter);
 /* calc_rhoe! inner loop for one k-point on host arrays; rhoe is host FP64
  * (N), accumulated when accumulate != 0. */
 int pw_calc_rhoe_host(pw_ctx *ctx, int ik, const double *psi, int64_t ld,

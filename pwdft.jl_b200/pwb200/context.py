@@ -202,6 +202,17 @@ class Context:
                                     int(nitermax), int(nconv), _dptr(ev), C.byref(nit)))
         return ev, nit.value
 
+    def davidson(self, ik, ispin, X, tol=1e-8, nitermax=40):
+        """diag_davidson_qe!: X (nb, Ngw) device block overwritten with the
+        Ritz vectors; returns (evals, niter)."""
+        nb, ld = X.shape
+        ev = np.zeros(nb)
+        nit = C.c_int(0)
+        self.use_torch_stream()
+        self._chk(self._L.pw_davidson(self.h, ik, ispin, dtype_code(X), C.c_void_p(X.data_ptr()), ld, nb, float(tol),
+                                      int(nitermax), _dptr(ev), C.byref(nit)))
+        return ev, nit.value
+
     def set_density_sphere(self, idx_g2r, G2):
         idx = np.ascontiguousarray(np.asarray(idx_g2r, dtype=np.int64))
         g2 = np.ascontiguousarray(np.asarray(G2, dtype=np.float64))
@@ -300,6 +311,17 @@ class Context:
         self._chk(self._L.pw_op_H_host(self.h, ik, ispin, psi.ctypes.data_as(_dp), Hpsi.ctypes.data_as(_dp), ld, nb,
                                        ops, dtype))
         return Hpsi
+
+    def davidson_host(self, ik, ispin, evc, tol=1e-8, nitermax=40, dtype=PW_C128):
+        """diag_davidson_qe!(Ham, evc) on the reference's host array evc
+        (Ngw, nb) complex128, overwritten (Fortran order); returns (evals, niter)."""
+        assert evc.flags.f_contiguous and evc.dtype == np.complex128
+        ld, nb = evc.shape
+        ev = np.zeros(nb)
+        nit = C.c_int(0)
+        self._chk(self._L.pw_davidson_host(self.h, ik, ispin, dtype, evc.ctypes.data_as(_dp), ld, nb, float(tol),
+                                           int(nitermax), _dptr(ev), C.byref(nit)))
+        return ev, nit.value
 
     def calc_rhoe_host(self, ik, psi, w, rhoe=None, accumulate=False, dtype=PW_C128):
         psi = np.asfortranarray(np.asarray(psi, dtype=np.complex128))

@@ -1,9 +1,11 @@
 """KS_solve_SCF! with every step of the SCF iteration on the device.
 
-Mirrors KS_solve_SCF.jl:24-373 (Nspin = 1, LOBPCG, no smearing, Pulay or
-simple density mixing):
+Mirrors KS_solve_SCF.jl:24-373 (Nspin = 1, no smearing, Pulay or simple
+density mixing):
   ethr schedule            KS_solve_SCF.jl:177-185
-  diag_LOBPCG!             pw_lobpcg per k-point          (device)
+  diag_LOBPCG!             pw_lobpcg per k-point          (device, update_psi="LOBPCG")
+  diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson";
+                           the call of electrons_scf.jl:150)
   calc_rhoe!               pw_calc_rhoe                   (device)
   mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
   rho >= eps clamp         KS_solve_SCF.jl:277-281        (device)
@@ -92,7 +94,7 @@ class PulayMixer:
 
 def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
-                 verbose=False, lobpcg_maxiter=100):
+                 verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG"):
     """Runs the SCF loop; returns a dict with energies, eigenvalues, timings
     and the per-iteration log."""
     import torch
@@ -109,6 +111,8 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     if not getattr(Ham, "_density_set", False):
         ctx.set_density_sphere(b.idx_g2r, b.G2)
         Ham._density_set = True
+    if update_psi not in ("LOBPCG", "davidson"):
+        raise ValueError("update_psi must be 'LOBPCG' or 'davidson'")
     mixed = precision == "mixed"
     dt = torch.complex64 if mixed else torch.complex128
     if psiks is None:
@@ -135,7 +139,10 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         t0 = time.perf_counter()
         nit = []
         for ik in range(b.Nkpt):
-            ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
+            if update_psi == "LOBPCG":
+                ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
+            else:
+                ev, n = ctx.davidson(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter)
             evals[:, ik] = ev
             nit.append(n)
         torch.cuda.synchronize()
@@ -169,8 +176,9 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         log.append((it, E["Total"], diffE, diffRhoe, int(np.max(nit % 1000)), "c64" if mixed else "c128",
                     int(np.sum(nit // 1000))))
         if verbose:
-            print("SCF: %5d %18.10f %12.5e %12.5e  %s  LOBPCG its %d restarts %d  ethr %.1e  %.2fs" % (
-                it, E["Total"], diffE, diffRhoe, log[-1][5], log[-1][4], log[-1][6], ethr, t1 - t0), flush=True)
+            print("SCF: %5d %18.10f %12.5e %12.5e  %s  %s its %d restarts %d  ethr %.1e  %.2fs" % (
+                it, E["Total"], diffE, diffRhoe, log[-1][5], update_psi, log[-1][4], log[-1][6], ethr, t1 - t0),
+                flush=True)
         Nconv = Nconv + 1 if diffE < etot_conv_thr else 0
         if Nconv >= 2:
             break

@@ -4,6 +4,7 @@
              (LAPACK zhegv/zheev in the reference) vs scipy.linalg.eigh
   pw_lobpcg  diag_LOBPCG! (diag_LOBPCG.jl:51-225) vs the exact spectrum of
              the oracle's dense Hamiltonian and vs the oracle's own LOBPCG
+  pw_davidson diag_davidson_qe! (diag_davidson_qe_v2.jl:38-216) likewise
 Tolerances: FP64 eigenvalues 1e-9 Ha (tol 1e-10), mixed 5e-5 Ha (tol 1e-5,
 the SCF's floor ethr_evals_last, KS_solve_SCF.jl:42).
 """
@@ -165,3 +166,79 @@ def test_calc_grad(ctx_fcc, prec, frac):
     tol = 1e-11 if prec == "c128" else 1e-4
     err = np.abs(got - ref).max() / np.abs(ref).max()
     assert err < tol, err
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_davidson_matches_exact_spectrum(ctx_fcc, prec):
+    """pw_davidson against the exact spectrum and against the oracle's
+    Davidson from the same start: the FP64 path takes the same steps (same
+    iteration count, restarts included), the mixed one converges to within
+    its FP32 floor."""
+    import torch
+    from oracle import ops, lobpcg, davidson
+    H, ctx, rng = ctx_fcc
+    ik = 1
+    ngw = H.pw.gvecw.Ngw[ik]
+    nb = 8
+    Hd = ops.op_H(H, np.eye(ngw, dtype=np.complex128), ik)
+    exact = np.linalg.eigvalsh(0.5 * (Hd + Hd.conj().T))[:nb]
+    X0 = lobpcg.ortho_sqrt(rng.standard_normal((ngw, nb)) + 1j * rng.standard_normal((ngw, nb)))
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    X = torch.from_numpy(np.ascontiguousarray(X0.T)).cuda().to(dt).contiguous()
+    tol = 1e-10 if prec == "c128" else 1e-5
+    ev, nit = ctx.davidson(ik, 0, X, tol=tol, nitermax=100)
+    bound = 1e-9 if prec == "c128" else 5e-5
+    assert np.abs(ev - exact).max() < bound, (ev - exact, nit)
+    Xo = X0.copy()
+    evo, nito = davidson.diag_davidson_qe(H, Xo, ik, EBANDS_THR=tol, NiterMax=100)
+    assert np.abs(ev - evo).max() < (1e-9 if prec == "c128" else 2e-4)
+    Xr = X.cpu().numpy().T.astype(np.complex128)
+    assert np.abs(Xr.conj().T @ Xr - np.eye(nb)).max() < (1e-10 if prec == "c128" else 5e-5)
+    if prec == "c128":
+        assert nit == nito, (nit, nito)
+        # Ritz vectors agree up to a phase per column
+        ph = np.sum(Xo.conj() * Xr, axis=0)
+        assert np.abs(np.abs(ph) - 1).max() < 1e-8
+
+
+def test_davidson_iterates_match_oracle(ctx_fcc):
+    """A fixed number of FP64 Davidson iterations (NiterMax = 3, so the last
+    one returns unconverged) gives the oracle's Ritz values and vectors:
+    the device follows the reference step by step, restart included (nb = 4,
+    Nvecx = 8, so the basis refreshes after the first expansion)."""
+    import torch
+    from oracle import lobpcg, davidson
+    H, ctx, rng = ctx_fcc
+    ik = 0
+    ngw = H.pw.gvecw.Ngw[ik]
+    nb = 4
+    X0 = lobpcg.ortho_sqrt(rng.standard_normal((ngw, nb)) + 1j * rng.standard_normal((ngw, nb)))
+    X = torch.from_numpy(np.ascontiguousarray(X0.T)).cuda().contiguous()
+    ev, nit = ctx.davidson(ik, 0, X, tol=1e-14, nitermax=3)
+    Xo = X0.copy()
+    evo, nito = davidson.diag_davidson_qe(H, Xo, ik, EBANDS_THR=1e-14, NiterMax=3)
+    assert nit == nito == 3
+    assert np.abs(ev - evo).max() < 1e-11
+    Xr = X.cpu().numpy().T
+    ph = np.sum(Xo.conj() * Xr, axis=0)
+    assert np.abs(Xr - Xo * (ph / np.abs(ph))[None, :]).max() < 1e-9
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_davidson_host_dropin(ctx_fcc, prec):
+    """pw_davidson_host on the reference's host array (Ngw x nb, column-major).
+    nb = 7: at this k-point the 6th and 7th levels are 5e-5 Ha apart, which a
+    6-vector Davidson resolves only slowly (the oracle takes > 100 steps)."""
+    import pwb200
+    from oracle import ops, lobpcg
+    H, ctx, _ = ctx_fcc
+    rng = np.random.default_rng(11)
+    ik = 2
+    ngw = H.pw.gvecw.Ngw[ik]
+    Hd = ops.op_H(H, np.eye(ngw, dtype=np.complex128), ik)
+    exact = np.linalg.eigvalsh(0.5 * (Hd + Hd.conj().T))[:7]
+    evc = np.asfortranarray(lobpcg.ortho_sqrt(rng.standard_normal((ngw, 7)) + 1j * rng.standard_normal((ngw, 7))))
+    code = pwb200.PW_C128 if prec == "c128" else pwb200.PW_C64
+    ev, nit = ctx.davidson_host(ik, 0, evc, tol=1e-10 if prec == "c128" else 1e-5, nitermax=100, dtype=code)
+    assert np.abs(ev - exact).max() < (1e-9 if prec == "c128" else 5e-5), (ev - exact, nit)
+    assert np.abs(evc.conj().T @ evc - np.eye(7)).max() < (1e-10 if prec == "c128" else 5e-5)

@@ -2,6 +2,7 @@
 
 Every constant below is quoted from the reference's tests or logs:
   test/validations_old/Si_fcc.jl:15        Etot(Si fcc, LDA) = -7.9110087934 (ABINIT, atol 1e-5)
+  test/validations_old/Si_fcc.jl:94-101    the same Etot with the Davidson eigensolver
   test/LOG_runtest_v.1.1.1:1171-1181       logged energy components of the same run
   test/test_energies.jl:19                 E_NN(Si fcc) = -8.397927400714764
   test/test_xc.jl:3-4                      VWN eps_xc / V_xc at rho = 0.1 .. 0.5 (atol 1e-5)
@@ -11,7 +12,7 @@ Every constant below is quoted from the reference's tests or logs:
 import numpy as np
 import pytest
 
-from oracle import pwgrid, ham, energies, lobpcg, ops, systems
+from oracle import pwgrid, ham, energies, lobpcg, ops, systems, davidson
 
 
 def test_gen_lattice():
@@ -86,3 +87,27 @@ def test_si_fcc_total_energy(si_fcc_scf):
     assert abs(E["NN"] - (-8.3979274007)) < 1e-9
     # charge conservation of calc_rhoe
     assert abs(rho.sum() * H.pw.CellVolume / H.pw.Npoints - 8.0) < 1e-8
+
+
+def test_free_electron_spectrum_davidson():
+    """diag_davidson_qe! on the free-electron Hamiltonian: the sorted
+    0.5 |G+k|^2 (as the LOBPCG known answer above)."""
+    H = systems.Ham_Si_fcc(meshk=(1, 1, 1), extra_states=8)
+    H.V_Total = np.zeros(H.pw.Npoints)
+    H.NbetaNL = 0
+    rng = np.random.default_rng(7)
+    ngw = H.pw.gvecw.Ngw[0]
+    X = lobpcg.ortho_sqrt(rng.standard_normal((ngw, 12)) + 1j * rng.standard_normal((ngw, 12)))
+    ev, _ = davidson.diag_davidson_qe(H, X, 0, EBANDS_THR=1e-10, NiterMax=200)
+    exact = np.sort(0.5 * H.pw.Gk2(0))[:12]
+    assert np.allclose(ev[:8], exact[:8], atol=1e-7)
+
+
+@pytest.mark.slow
+def test_si_fcc_total_energy_davidson():
+    """KS_solve_SCF with the QE-style Davidson (test/validations_old/Si_fcc.jl:94-101)."""
+    from oracle import scf
+    H = systems.Ham_Si_fcc()
+    E, psiks, rho = scf.KS_solve_SCF(H, betamix=0.5, mix_method="pulay", etot_conv_thr=1e-8,
+                                     diag=lambda Ham, ps, tol, nconv: davidson.diag_davidson_qe_all(Ham, ps, tol=tol))
+    assert abs(E["Total"] - (-7.9110087934)) < 1e-5

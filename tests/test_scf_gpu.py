@@ -6,6 +6,9 @@ total energy and the FP64 oracle's converged SCF.
     FP64 path:  |Etot - ABINIT| < 1e-5 (test/validations_old/Si_fcc.jl:15)
                 |Etot - oracle| < 2e-7, components within 2e-6
     mixed path (FP64 switch at |dE| < 1e-5): |Etot - ABINIT| < 1e-5
+  The same with update_psi = "davidson" (diag_davidson_qe!, Pulay beta 0.5 as
+  test/validations_old/Si_fcc.jl:94-101): |Etot - ABINIT| < 1e-5 and the
+  FP64 result within 2e-7 of the LOBPCG-driven oracle SCF.
 """
 import numpy as np
 import pytest
@@ -44,3 +47,15 @@ def test_scf_si_fcc(si_fcc_gpu, si_fcc_scf, precision):
             assert abs(E[key] - Eo[key]) < 2e-6, key
     else:
         assert res["switched_to_fp64_at"] is not None
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_scf_si_fcc_davidson(si_fcc_gpu, si_fcc_scf, precision):
+    from pwb200 import scf
+    res = scf.KS_solve_SCF(si_fcc_gpu, betamix=0.5, mix_method="pulay", etot_conv_thr=1e-8, precision=precision,
+                           update_psi="davidson")
+    E = res["energies"]
+    assert abs(E["Total"] - ABINIT) < 1e-5, res["log"][-3:]
+    if precision == "fp64":
+        _, Eo, _, _ = si_fcc_scf
+        assert abs(E["Total"] - Eo["Total"]) < 2e-7
