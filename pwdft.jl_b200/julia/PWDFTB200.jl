@@ -178,4 +178,28 @@ function PWDFT.diag_LOBPCG!(B::B200Hamiltonian, psiks::BlochWavefunc; tol=1e-5, 
     return evals
 end
 
+# diag_davidson_qe_v2.jl:6-34: every (ispin, ik) block through
+# pw_davidson_host (diag_davidson_qe!, S = identity); EBANDS_THR = tol.
+function PWDFT.diag_davidson_qe!(B::B200Hamiltonian, psiks::BlochWavefunc; tol=1e-5, NiterMax=100,
+                                 verbose=false, verbose_last=false, Nstates_conv=0)
+    Ham = B.Ham
+    Nkpt = Ham.pw.gvecw.kpoints.Nkpt
+    Nspin = Ham.electrons.Nspin_wf
+    Nstates = Ham.electrons.Nstates
+    evals = zeros(Float64, Nstates, Nkpt * Nspin)
+    niter = Ref{Cint}(0)
+    for ispin in 1:Nspin, ik in 1:Nkpt
+        Ham.ik, Ham.ispin = ik, ispin
+        ikspin = ik + (ispin - 1) * Nkpt
+        X = psiks[ikspin]
+        ev = zeros(Float64, Nstates)
+        check(ccall((:pw_davidson_host, libpwb200), Cint,
+                    (Ptr{Cvoid}, Cint, Cint, Cint, Ptr{ComplexF64}, Int64, Cint, Float64, Cint, Ptr{Float64}, Ref{Cint}),
+                    B.ctx, ik - 1, ispin - 1, B.dtype, X, stride(X, 2), size(X, 2), tol, NiterMax, ev, niter),
+              B.ctx)
+        evals[:, ikspin] = ev
+    end
+    return evals
+end
+
 end # module
