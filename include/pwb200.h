@@ -189,10 +189,19 @@ int pw_davidson(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
  * G = 0 comes first, PWGrid.jl:199-242), needed by pw_poisson/pw_update. */
 int pw_set_density_sphere(pw_ctx *ctx, int64_t Ng, const int64_t *idx_g2r,
                           const double *G2, int index_base);
+/* Exchange-correlation of pw_update: the reference's internal functionals
+ * (Hamiltonian.jl:270-277, use_xc_internal = true): PW_XC_VWN (default;
+ * LDA_VWN_internal.jl) or PW_XC_PBE (GGA_PBE_internal.jl:29-145, gradients
+ * by PWGrid.jl:351-398 op_nabla / op_nabla_dot on the density sphere).
+ * G (host, 3 x Ng, the sphere of pw_set_density_sphere in its order) is
+ * required for PBE and ignored for VWN. */
+#define PW_XC_VWN 0
+#define PW_XC_PBE 1
+int pw_set_xc(pw_ctx *ctx, int xc, const double *G);
 /* Poisson_solve! (Poisson_solve.jl:22-40): V_H(r) from rho(r), device FP64
  * arrays of N points. */
 int pw_poisson(pw_ctx *ctx, const double *rho, double *VH);
-/* update! (Hamiltonian.jl:510-545, VWN, Nspin = 1) + the sums of
+/* update! (Hamiltonian.jl:510-545, VWN or PBE per pw_set_xc, Nspin = 1) + the sums of
  * calc_E_local (calc_energies.jl:245-333): V_tot = V_ps + V_H + V_xc becomes
  * the context's V_loc; VH / Vxc (device N, may be NULL) receive V_H and
  * V_xc; E3 (host) = {sum V_H rho, sum V_ps rho, sum eps_xc rho} (multiply by

@@ -36,11 +36,16 @@ def calc_E_Ps_nloc(Ham, psiks):
 
 
 def calc_E_local(Ham, Rhoe):
-    """calc_energies.jl:245-274 (+ calc_E_xc :276-333 for VWN)."""
+    """calc_energies.jl:245-274 (+ calc_E_xc :276-333 for VWN and PBE)."""
     dVol = Ham.pw.CellVolume / Ham.pw.Npoints
     E_Hartree = 0.5 * float(np.dot(Ham.V_Hartree, Rhoe)) * dVol
     E_Ps_loc = float(np.dot(Ham.V_Ps_loc, Rhoe)) * dVol
-    E_xc = float(np.sum(calc_epsxc_VWN(Rhoe) * Rhoe)) * dVol
+    if getattr(Ham, "xcfunc", "VWN") == "PBE":
+        from .pbe import calc_epsxc_PBE
+        epsxc = calc_epsxc_PBE(Ham.pw, Rhoe)
+    else:
+        epsxc = calc_epsxc_VWN(Rhoe)
+    E_xc = float(np.sum(epsxc * Rhoe)) * dVol
     return E_Ps_loc, E_Hartree, E_xc
 
 

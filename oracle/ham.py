@@ -202,10 +202,14 @@ def calc_Vxc_VWN(rho):
 
 class Hamiltonian:
     """Hamiltonian.jl:41-302 / 337-405 for GTH pseudopotentials, dual = 4,
-    Nspin_wf = Nspin_dens = 1, xcfunc = "VWN" (internal formulas)."""
+    Nspin_wf = Nspin_dens = 1, xcfunc = "VWN" or "PBE" (internal formulas,
+    Hamiltonian.jl:270-277)."""
 
     def __init__(self, atoms, pspfiles, ecutwfc, meshk=(1, 1, 1), extra_states=None,
-                 Nstates=None, kpoints=None, Ns=None):
+                 Nstates=None, kpoints=None, Ns=None, xcfunc="VWN"):
+        if xcfunc not in ("VWN", "PBE"):
+            raise ValueError("xcfunc must be 'VWN' or 'PBE'")
+        self.xcfunc = xcfunc
         self.atoms = atoms
         self.pspots = [PsPot_GTH(f) for f in pspfiles]
         for isp, s in enumerate(atoms.SpeciesSymbols):
@@ -260,9 +264,13 @@ class Hamiltonian:
 
     # ------------------------------------------------------------ update!
     def update(self, Rhoe):
-        """Hamiltonian.jl:510-545 (Nspin = 1, VWN)."""
+        """Hamiltonian.jl:510-545 (Nspin = 1)."""
         self.V_Hartree = Poisson_solve(self.pw, Rhoe)
-        self.V_xc = calc_Vxc_VWN(Rhoe)
+        if self.xcfunc == "PBE":
+            from .pbe import calc_Vxc_PBE
+            self.V_xc = calc_Vxc_PBE(self.pw, Rhoe)
+        else:
+            self.V_xc = calc_Vxc_VWN(Rhoe)
         self.V_Total = self.V_Ps_loc + self.V_Hartree + self.V_xc
 
     def guess_rhoe(self):

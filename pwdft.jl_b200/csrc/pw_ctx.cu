@@ -97,6 +97,10 @@ struct pw_ctx {
     int f_nsp = 0;
     int *d_atom_rows = nullptr;
     int f_natoms = 0;
+    // exchange-correlation of update!: PW_XC_VWN or PW_XC_PBE (with the G
+    // vectors of the density sphere, 3 x Ng, for grad rho and div h)
+    int xc = PW_XC_VWN;
+    double *d_xcG = nullptr;
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -921,6 +925,26 @@ extern "C" int pw_set_density_sphere(pw_ctx *c, int64_t Ng, const int64_t *idx_g
     if (s) return s;
     c->have_dens = true;
     return PW_OK;
+}
+
+extern "C" int pw_set_xc(pw_ctx *c, int xc, const double *G) {
+    if (!c) return PW_ERR_ARG;
+    if (xc != PW_XC_VWN && xc != PW_XC_PBE) return fail(c, PW_ERR_ARG, "unknown exchange-correlation %d", xc);
+    CK(c, cudaSetDevice(c->device));
+    if (xc == PW_XC_PBE) {
+        if (!c->have_dens) return fail(c, PW_ERR_STATE, "call pw_set_density_sphere before pw_set_xc(PBE)");
+        if (!G) return fail(c, PW_ERR_ARG, "PBE needs the G vectors of the density sphere");
+        const size_t ng = (size_t)c->dens.Ngw;
+        int s;
+        if (!c->d_xcG && (s = dalloc(c, &c->d_xcG, 3 * ng))) return s;
+        CK(c, cudaMemcpy(c->d_xcG, G, 3 * ng * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    c->xc = xc;
+    return PW_OK;
+}
+int pwk_xc(const pw_ctx *c, const double **G) {
+    *G = c->d_xcG;
+    return c->xc;
 }
 
 // ------------------------------------------------------------------ forces

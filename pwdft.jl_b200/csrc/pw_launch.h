@@ -12,6 +12,8 @@ namespace pwk {
 enum ScratchSlot {
     // update!: Poisson, XC, V_tot, reductions
     SL_UPD_A = 8, SL_UPD_RHOG, SL_UPD_VH, SL_UPD_VXC, SL_UPD_EPS, SL_UPD_VTOT, SL_UPD_RED,
+    // update! with PBE: grad rho / h (3 x N), div h on the density sphere
+    SL_UPD_GRAD, SL_UPD_DIVG,
     // band energies
     SL_BAND_W, SL_BAND_RED,
     // LOBPCG / generalized eigenproblem / ortho_sqrt

@@ -5,6 +5,12 @@
 //                    -> V_H(r) = Re G_to_R
 //   calc_Vxc_VWN!    (LDA_VWN_internal.jl:33-52, XC_funcs/XC_x_slater.jl,
 //                    XC_funcs/XC_c_vwn.jl): eps_xc(r), V_xc(r)
+//   calc_Vxc_PBE! / calc_epsxc_PBE! (GGA_PBE_internal.jl:29-145,
+//                    XC_funcs/XC_x_pbe.jl, XC_c_pw.jl, XC_c_pbe.jl): grad rho
+//                    by op_nabla (PWGrid.jl:351-375: i G rho(G) on the density
+//                    sphere, three sphere-to-grid transforms), the pointwise
+//                    functional, and div h by op_nabla_dot (PWGrid.jl:378-398:
+//                    three grid-to-sphere transforms, i G . h(G), one back)
 //   update!          (Hamiltonian.jl:510-545): V_tot = V_Ps_loc + V_H + V_xc,
 //                    handed to op_V_loc as the context's V_loc
 //   calc_E_local     (calc_energies.jl:245-333): E_Hartree, E_Ps_loc, E_xc
@@ -29,6 +35,7 @@ int pwk_projections(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, i
                     const double2 **P2, int *nbeta);
 int pwk_ngw(const pw_ctx *c, int ik);
 const double *pwk_gk2(const pw_ctx *c, int ik);
+int pwk_xc(const pw_ctx *c, const double **G);
 
 namespace pwk {
 namespace upd {
@@ -136,6 +143,130 @@ __global__ void k_vwn_vtot(const double *__restrict__ rho, const double *__restr
         Vxc[i] = vx + vc;
         eps[i] = ex + ec;
         Vtot[i] = Vps[i] + VH[i] + vx + vc;
+    }
+}
+
+// ------------------------------------------------------------------ PBE
+// XC_x_slater (energy and potential per particle)
+__device__ inline void slater(double r, double &ex, double &vx) {
+    ex = vx = 0.0;
+    if (r > 1e-10) {
+        const double rs = 0.6203504908994 / cbrt(r);
+        const double f = -0.687247939924714, alpha = 2.0 / 3.0;
+        ex = f * alpha / rs;
+        vx = 4.0 / 3.0 * f * alpha / rs;
+    }
+}
+// XC_c_pw: Perdew-Wang 92 correlation per particle
+__device__ inline void c_pw(double r, double &ec, double &vc) {
+    ec = vc = 0.0;
+    if (r <= 1e-10) return;
+    const double a = 0.031091, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+    const double rs = 0.6203504908994 / cbrt(r);
+    const double rs12 = sqrt(rs), rs32 = rs * rs12, rs2 = rs * rs;
+    const double om = 2.0 * a * (b1 * rs12 + b2 * rs + b3 * rs32 + b4 * rs2);
+    const double dom = 2.0 * a * (0.5 * b1 * rs12 + b2 * rs + 1.5 * b3 * rs32 + 2.0 * b4 * rs2);
+    const double olog = log(1.0 + 1.0 / om);
+    ec = -2.0 * a * (1.0 + a1 * rs) * olog;
+    vc = -2.0 * a * (1.0 + 2.0 / 3.0 * a1 * rs) * olog - 2.0 / 3.0 * a * (1.0 + a1 * rs) * dom / (om * (om + 1.0));
+}
+// XC_x_pbe: gradient part of PBE exchange (energy density sx, v1x, v2x)
+__device__ inline void x_pbe(double r, double g2, double &sx, double &v1x, double &v2x) {
+    sx = v1x = v2x = 0.0;
+    if (r <= 1e-6 || g2 <= 1e-10) return;
+    const double third = 1.0 / 3.0, k = 0.804, mu = 0.2195149727645171;
+    const double c1 = 0.75 / M_PI, c2 = 3.093667726280136, c5 = 4.0 * third;
+    const double agrho = sqrt(g2);
+    const double kf = c2 * cbrt(r);
+    const double dsg = 0.5 / kf;
+    const double s1 = agrho * dsg / r;
+    const double s2 = s1 * s1;
+    const double ds = -c5 * s1;
+    const double f2 = 1.0 + s2 * mu / k;
+    const double fx = k - k / f2;
+    const double exunif = -c1 * kf;
+    const double sx_s = exunif * fx;
+    const double dfx = 2.0 * mu * s1 / (f2 * f2);
+    v1x = sx_s + exunif * third * fx + exunif * dfx * ds;
+    v2x = exunif * dfx * dsg / agrho;
+    sx = sx_s * r;
+}
+// XC_c_pbe: gradient correction to PW92 correlation (sc, v1c, v2c)
+__device__ inline void c_pbe(double r, double g2, double &sc, double &v1c, double &v2c) {
+    sc = v1c = v2c = 0.0;
+    if (r <= 1e-6 || g2 <= 1e-10) return;
+    const double ga = 0.0310906908696548950, be = 0.06672455060314922;
+    const double xkf = 1.919158292677513, xks = 1.128379167095513;
+    const double rs = 0.6203504908994 / cbrt(r);
+    double ec, vc;
+    c_pw(r, ec, vc);
+    const double kf = xkf / rs;
+    const double ks = xks * sqrt(kf);
+    const double t = sqrt(g2) / (2.0 * ks * r);
+    const double expe = exp(-ec / ga);
+    const double af = be / ga * (1.0 / (expe - 1.0));
+    const double bf = expe * (vc - ec);
+    const double y = af * t * t;
+    const double d = 1.0 + y + y * y;
+    const double xy = (1.0 + y) / d;
+    const double qy = y * y * (2.0 + y) / (d * d);
+    const double s1 = 1.0 + be / ga * t * t * xy;
+    const double h0 = ga * log(s1);
+    const double dh0 = be * t * t / s1 * (-7.0 / 3.0 * xy - qy * (af * bf / be - 7.0 / 3.0));
+    const double ddh0 = be / (2.0 * ks * ks * r) * (xy - qy) / s1;
+    sc = r * h0;
+    v1c = h0 + dh0;
+    v2c = ddh0;
+}
+
+// out[ig] = i G_d[ig] rhoG[ig]  (one Cartesian component of op_nabla)
+__global__ void k_grad_G(const double2 *__restrict__ rhoG, const double *__restrict__ G, int d, double2 *__restrict__ out,
+                         int Ng) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Ng; i += gridDim.x * blockDim.x) {
+        const double gd = G[3 * i + d];
+        const double2 v = rhoG[i];
+        out[i] = make_double2(-gd * v.y, gd * v.x);
+    }
+}
+// div[ig] (+)= G_d[ig] hG[ig]; last: div := i div (op_nabla_dot)
+__global__ void k_div_acc(double2 *__restrict__ div, const double2 *__restrict__ hG, const double *__restrict__ G, int d,
+                          int Ng, int first, int last) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Ng; i += gridDim.x * blockDim.x) {
+        const double gd = G[3 * i + d];
+        double2 a = first ? make_double2(0.0, 0.0) : div[i];
+        a.x += gd * hG[i].x;
+        a.y += gd * hG[i].y;
+        div[i] = last ? make_double2(-a.y, a.x) : a;
+    }
+}
+// pointwise PBE (GGA_PBE_internal.jl:39-50, 114-130): eps_xc, the local
+// part of V_xc, and h = (v2x + v2c) grad rho written over grad rho
+__global__ void k_pbe_point(const double *__restrict__ rho, double *__restrict__ gx, double *__restrict__ gy,
+                            double *__restrict__ gz, double *__restrict__ Vxc, double *__restrict__ eps, size_t N) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const double r = rho[i];
+        const double a = gx[i], b = gy[i], c = gz[i];
+        const double g2 = a * a + b * b + c * c;
+        double ex, vx, ec, vc, sx, v1x, v2x, sc, v1c, v2c;
+        slater(r, ex, vx);
+        c_pw(r, ec, vc);
+        x_pbe(r, g2, sx, v1x, v2x);
+        c_pbe(r, g2, sc, v1c, v2c);
+        eps[i] = ex + ec + (r != 0.0 ? (sx + sc) / r : 0.0);
+        Vxc[i] = vx + vc + v1x + v1c;
+        const double v2 = v2x + v2c;
+        gx[i] = v2 * a;
+        gy[i] = v2 * b;
+        gz[i] = v2 * c;
+    }
+}
+// V_xc -= div h; V_tot = V_ps + V_H + V_xc
+__global__ void k_pbe_vtot(double *__restrict__ Vxc, const double *__restrict__ dh, const double *__restrict__ Vps,
+                           const double *__restrict__ VH, double *__restrict__ Vtot, size_t N) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = Vxc[i] - dh[i];
+        Vxc[i] = v;
+        Vtot[i] = Vps[i] + VH[i] + v;
     }
 }
 
@@ -290,6 +421,55 @@ static int poisson(pw_ctx *c, const double *rho, double *VH) {
     return PW_OK;
 }
 
+// sphere coefficients g (device, Ng; clobbered by the z pass) -> out(r) =
+// Re G_to_R (the reference's ifft, 1/N)
+static int sphere_to_R(pw_ctx *c, FftLaunch &L, const double2 *g, int Ng, size_t N, double *out) {
+    cudaStream_t st = pwk_stream(c);
+    double2 *A = nullptr;
+    RK(pwk_scratch(c, SL_UPD_A, (size_t)L.kp.N3 * L.kp.Ncol * sizeof(double2), (void **)&A));
+    CKU(c, launch_zinv<double>(L, g, Ng, 1, A, st));
+    k_plane_g2r<<<L.kp.N3, 256, plane_smem(L), st>>>(L.kp, L.dx, L.dy, (const double2 *)L.twx, (const double2 *)L.twy, A,
+                                                     out, 1.0 / (double)N, L.Jc);
+    CKU(c, cudaGetLastError());
+    pwk_count_launches(c, 2);
+    return PW_OK;
+}
+
+// calc_Vxc_PBE! + calc_epsxc_PBE! (Nspin = 1): Vxc (N) and eps (N) from rho
+static int pbe(pw_ctx *c, const double *rho, const double *G, double *Vxc, double *eps) {
+    FftLaunch L;
+    double2 *g = nullptr, *A = nullptr, *div = nullptr, *tmp = nullptr;
+    int Ng = 0;
+    size_t N = 0;
+    const double *G2 = nullptr;
+    RK(density_to_G(c, rho, L, &g, &A, &Ng, &N, &G2));
+    cudaStream_t st = pwk_stream(c);
+    double *grad = nullptr;
+    RK(pwk_scratch(c, SL_UPD_GRAD, 3 * N * sizeof(double), (void **)&grad));
+    RK(pwk_scratch(c, SL_UPD_DIVG, 2 * (size_t)Ng * sizeof(double2), (void **)&div));
+    tmp = div + Ng;
+    const int gb = (Ng + 255) / 256;
+    // grad rho (op_nabla)
+    for (int d = 0; d < 3; ++d) {
+        k_grad_G<<<gb, 256, 0, st>>>(g, G, d, tmp, Ng);
+        CKU(c, cudaGetLastError());
+        pwk_count_launches(c, 1);
+        RK(sphere_to_R(c, L, tmp, Ng, N, grad + d * N));
+    }
+    k_pbe_point<<<RED_BLOCKS, 256, 0, st>>>(rho, grad, grad + N, grad + 2 * N, Vxc, eps, N);
+    CKU(c, cudaGetLastError());
+    pwk_count_launches(c, 1);
+    // div h (op_nabla_dot)
+    for (int d = 0; d < 3; ++d) {
+        RK(density_to_G(c, grad + d * N, L, &g, &A, &Ng, &N, &G2));
+        k_div_acc<<<gb, 256, 0, st>>>(div, g, G, d, Ng, d == 0, d == 2);
+        CKU(c, cudaGetLastError());
+        pwk_count_launches(c, 1);
+    }
+    RK(sphere_to_R(c, L, div, Ng, N, grad));   // div h(r) over h_x, no longer needed
+    return PW_OK;
+}
+
 extern "C" int pw_poisson(pw_ctx *c, const double *rho, double *VH) {
     if (!c) return PW_ERR_ARG;
     if (!rho || !VH) return pwk_fail(c, PW_ERR_ARG, "NULL density or potential");
@@ -314,7 +494,15 @@ extern "C" int pw_update(pw_ctx *c, const double *rho, const double *Vps, double
     RK(pwk_scratch(c, SL_UPD_VTOT, N * sizeof(double), (void **)&vt));
     RK(pwk_scratch(c, SL_UPD_RED, RED_BLOCKS * 3 * sizeof(double), (void **)&part));
     RK(poisson(c, rho, vh));
-    k_vwn_vtot<<<RED_BLOCKS, 256, 0, st>>>(rho, Vps, vh, vxc, eps, vt, N);
+    const double *xcG = nullptr;
+    if (pwk_xc(c, &xcG) == PW_XC_PBE) {
+        RK(pbe(c, rho, xcG, vxc, eps));
+        double *dh = nullptr;
+        RK(pwk_scratch(c, SL_UPD_GRAD, 3 * N * sizeof(double), (void **)&dh));
+        k_pbe_vtot<<<RED_BLOCKS, 256, 0, st>>>(vxc, dh, Vps, vh, vt, N);
+    } else {
+        k_vwn_vtot<<<RED_BLOCKS, 256, 0, st>>>(rho, Vps, vh, vxc, eps, vt, N);
+    }
     CKU(c, cudaGetLastError());
     RK(pwk_set_vloc_device(c, vt, 1));
     k_dot3<<<RED_BLOCKS, 256, 0, st>>>(vh, rho, Vps, rho, eps, rho, N, part);

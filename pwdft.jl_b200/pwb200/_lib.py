@@ -15,6 +15,7 @@ PW_OK, PW_ERR_ARG, PW_ERR_CUDA, PW_ERR_NOMEM, PW_ERR_NOT_POSDEF, PW_ERR_NAN, PW_
 PW_C128, PW_C64 = 0, 1
 PW_OP_K, PW_OP_VLOC, PW_OP_VNL, PW_OP_H = 1, 2, 4, 7
 PW_ACCUMULATE = 0x100
+PW_XC_VWN, PW_XC_PBE = 0, 1
 
 STATUS_NAMES = {0: "PW_OK", 1: "PW_ERR_ARG", 2: "PW_ERR_CUDA", 3: "PW_ERR_NOMEM", 4: "PW_ERR_NOT_POSDEF",
                 5: "PW_ERR_NAN", 6: "PW_ERR_STATE", 7: "PW_ERR_UNSUPPORTED", 8: "PW_ERR_TIMEOUT"}
@@ -74,6 +75,7 @@ SIGNATURES = {
     "pw_ortho_cholesky": (_i, [_vp, _i, _vp, _i64, _i64, _i]),
     "pw_calc_grad": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _dp, _d]),
     "pw_set_force_tables": (_i, [_vp, _i, _dp, _dp]),
+    "pw_set_xc": (_i, [_vp, _i, _dp]),
     "pw_forces_local": (_i, [_vp, _vp, _i, _dp, _i32p, _dp]),
     "pw_set_gkvec": (_i, [_vp, _i, _dp]),
     "pw_set_nonlocal_atoms": (_i, [_vp, _i, _i32p]),

@@ -251,6 +251,13 @@ class Context:
         return g
 
     # ---------------------------------------------------------------- forces
+    def set_xc(self, xc, G=None):
+        """Exchange-correlation of update(): PW_XC_VWN or PW_XC_PBE; G (Ng, 3)
+        of the density sphere, in its order (PBE only)."""
+        g = None if G is None else np.ascontiguousarray(np.asarray(G, dtype=np.float64))
+        self._keep_xc = g
+        self._chk(self._L.pw_set_xc(self.h, int(xc), None if g is None else _dptr(g)))
+
     def set_force_tables(self, VlocG, G):
         """VlocG (Ng, nspecies): eval_Vloc_G per species on the density sphere
         (no 1/Omega); G (Ng, 3) of that sphere, in its order."""

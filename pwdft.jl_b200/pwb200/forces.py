@@ -16,9 +16,7 @@ def setup_forces(Ham):
     vectors of every k-point and the atom of every projector."""
     b = Ham.basis
     ctx = Ham.ctx
-    if not getattr(Ham, "_density_set", False):
-        ctx.set_density_sphere(b.idx_g2r, b.G2)
-        Ham._density_set = True
+    Ham.setup_density()
     VlocG = np.stack([psp.vloc_G(b.G2) for psp in Ham.pspots], axis=1)     # (Ng, nspecies)
     ctx.set_force_tables(VlocG, b.G)
     for ik in range(b.Nkpt):

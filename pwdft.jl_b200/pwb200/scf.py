@@ -108,9 +108,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         Nstates = int(round(Nel / 2)) + (1 if int(round(Nel)) % 2 else 0)
     Focc, Nocc = occupations(Nel, Nstates, b.Nkpt)
     wk = Ham.wk
-    if not getattr(Ham, "_density_set", False):
-        ctx.set_density_sphere(b.idx_g2r, b.G2)
-        Ham._density_set = True
+    Ham.setup_density()
     if update_psi not in ("LOBPCG", "davidson"):
         raise ValueError("update_psi must be 'LOBPCG' or 'davidson'")
     mixed = precision == "mixed"

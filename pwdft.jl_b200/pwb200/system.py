@@ -329,7 +329,11 @@ class Hamiltonian:
     of PWDFT.jl's Hamiltonian that op_H / calc_rhoe read), plus the hidden
     (ik, ispin) state of the reference (Hamiltonian.jl: Ham.ik, Ham.ispin)."""
 
-    def __init__(self, system, pspfiles, ecutwfc, kpts=None, wk=None, device=0, Ns=None, V_loc=None):
+    def __init__(self, system, pspfiles, ecutwfc, kpts=None, wk=None, device=0, Ns=None, V_loc=None,
+                 xcfunc="VWN"):
+        if xcfunc not in ("VWN", "PBE"):
+            raise ValueError("xcfunc must be 'VWN' or 'PBE'")
+        self.xcfunc = xcfunc
         self.system = system
         self.pspots = [GTH(f) for f in pspfiles]
         self.basis = b = Basis(system.LatVecs, ecutwfc, kpts=kpts, Ns=Ns)
@@ -351,6 +355,19 @@ class Hamiltonian:
         self.Nelectrons = float(sum(self.Zvals[system.atm2species]))
         self.ik = 0
         self.ispin = 0
+
+    def setup_density(self):
+        """Uploads, once, the density G-sphere that update!, the energies and
+        the forces run on, and the exchange-correlation choice
+        (Hamiltonian.jl:270-277: the internal VWN or PBE)."""
+        if getattr(self, "_density_set", False):
+            return
+        b = self.basis
+        self.ctx.set_density_sphere(b.idx_g2r, b.G2)
+        if self.xcfunc == "PBE":
+            from ._lib import PW_XC_PBE
+            self.ctx.set_xc(PW_XC_PBE, b.G)
+        self._density_set = True
 
     def update_vloc(self, V):
         """New V_loc(r) after update! (Hamiltonian.jl:510-545)."""
