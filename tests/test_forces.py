@@ -4,7 +4,7 @@ The reference has no force golden numbers, so the oracle's forces are
 pinned against central finite differences of its own SCF total energy,
 and the device forces against the oracle on the same wavefunctions and
 density (FP64 1e-10 Ha/bohr, mixed 1e-6), and against finite differences
-of the device SCF energy on a displaced Si64 cell (config C4, LDA).
+of the device SCF energy on a displaced Si64 cell with PBE (config C4).
 """
 import numpy as np
 import pytest
@@ -95,11 +95,11 @@ def _psp():
 
 @pytest.mark.gpu
 def test_device_forces_match_finite_differences_si64():
-    """Config C4 geometry (Si64, every atom moved by seeded uniform noise in
-    [-0.05, 0.05] bohr), LDA: forces from the device SCF (FP64) against
-    central finite differences (h = 1e-3 bohr) of the device SCF energy for
-    one Cartesian component, and the mixed-precision SCF's forces against
-    the FP64 ones."""
+    """Config C4: Si64, every atom moved by seeded uniform noise in
+    [-0.05, 0.05] bohr, GTH-PBE Si-q4, PBE: forces from the device SCF (FP64)
+    against central finite differences (h = 1e-4 bohr) of the device SCF
+    energy for one Cartesian component, and the mixed-precision SCF's
+    forces against the FP64 ones."""
     if not cuda_ok():
         pytest.skip("no CUDA device")
     import pwb200
@@ -110,8 +110,9 @@ def test_device_forces_match_finite_differences_si64():
     nat = at.positions.shape[1]
 
     def run(pos, precision="fp64"):
-        H = pwb200.Hamiltonian(pwb200.System(["Si"] * nat, pos, at.LatVecs), [_psp()], 15.0)
-        res = scf.KS_solve_SCF(H, Nstates=136, etot_conv_thr=1e-10, ethr_evals_last=1e-10, precision=precision,
+        H = pwb200.Hamiltonian(pwb200.System(["Si"] * nat, pos, at.LatVecs), [systems.psp("Si-q4-pbe.gth")], 15.0,
+                               xcfunc="PBE")
+        res = scf.KS_solve_SCF(H, Nstates=136, etot_conv_thr=1e-11, ethr_evals_last=1e-11, precision=precision,
                                fp64_switch=1e-5 * nat)
         return H, res
 
@@ -120,7 +121,7 @@ def test_device_forces_match_finite_differences_si64():
     Focc, _ = scf.occupations(H.Nelectrons, 136, 1)
     F = pf.calc_forces(H, res["psiks"], res["rho"], Focc)
     assert np.abs(F.sum(axis=1)).max() < 1e-4
-    h = 1e-3
+    h = 1e-4
     Es = []
     for s in (+1, -1):
         p = pos.copy()
