@@ -96,7 +96,8 @@ def calc_E_NN(LatVecs, positions, atm2species, Zvals):
 
 def calc_energies(Ham, psiks, Rhoe):
     """calc_energies.jl:457-492.  Returns a dict of components; 'Total'
-    follows Energies.jl:30-34 (mTS = 0 without smearing)."""
+    follows Energies.jl:30-34 (the free energy: mTS, Ham.mTS, is added when
+    smearing set it, and is 0 otherwise)."""
     E = {}
     E["Kinetic"] = calc_E_kin(Ham, psiks)
     E["Ps_loc"], E["Hartree"], E["XC"] = calc_E_local(Ham, Rhoe)
@@ -104,5 +105,6 @@ def calc_energies(Ham, psiks, Rhoe):
     if Ham.E_NN is None:
         Ham.E_NN = calc_E_NN(Ham.atoms.LatVecs, Ham.atoms.positions, Ham.atoms.atm2species, Ham.Zvals)
     E["NN"] = Ham.E_NN
-    E["Total"] = E["Kinetic"] + E["Ps_loc"] + E["Ps_nloc"] + E["Hartree"] + E["XC"] + E["NN"]
+    E["mTS"] = getattr(Ham, "mTS", 0.0)
+    E["Total"] = E["Kinetic"] + E["Ps_loc"] + E["Ps_nloc"] + E["Hartree"] + E["XC"] + E["NN"] + E["mTS"]
     return E

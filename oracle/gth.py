@@ -9,7 +9,7 @@ Oracle (test infrastructure only).  Restates PWDFT.jl:
 import math
 import numpy as np
 
-ZATOMS = {"H": 1, "He": 2, "Li": 3, "C": 6, "N": 7, "O": 8, "Na": 11, "Mg": 12,
+ZATOMS = {"Pt": 78, "H": 1, "He": 2, "Li": 3, "C": 6, "N": 7, "O": 8, "Na": 11, "Mg": 12,
           "Al": 13, "Si": 14, "P": 15, "S": 16, "Cl": 17, "Ga": 31, "Ge": 32}
 
 

@@ -1,7 +1,8 @@
 """Self-consistent field driver with Pulay density mixing.
 
 Oracle (test infrastructure only).  Restates PWDFT.jl:
-  KS_solve_SCF.jl:24-373   KS_solve_SCF! (Nspin = 1, LOBPCG, no smearing)
+  KS_solve_SCF.jl:24-373   KS_solve_SCF! (Nspin = 1, LOBPCG, optional Fermi-Dirac
+                           smearing: KS_solve_SCF.jl:218-223 with occupations.jl)
   mix_pulay.jl:1-41        mix_pulay!
   gen_wavefunc.jl:90-92    rand_Wavefunc (with a NumPy RNG: Julia's stream
                            cannot be reproduced)
@@ -11,6 +12,7 @@ import numpy as np
 from .lobpcg import diag_LOBPCG, ortho_sqrt
 from .ops import calc_rhoe
 from .energies import calc_energies
+from .occupations import calc_Focc, calc_entropy
 
 EPS = np.finfo(np.float64).eps
 
@@ -53,7 +55,7 @@ def mix_pulay(x, gx, beta, X, F, it, mixdim, state):
 
 def KS_solve_SCF(Ham, psiks=None, betamix=0.2, NiterMax=100, mix_method="pulay",
                  mixdim=5, etot_conv_thr=1e-6, ethr_evals_last=1e-5, verbose=False,
-                 diag=None, seed=1234, log=None):
+                 diag=None, seed=1234, log=None, use_smearing=False, kT=1e-3):
     """KS_solve_SCF.jl:24-373.  `diag(Ham, psiks, tol, Nstates_conv)` may
     replace the LOBPCG call (used to drive the GPU solver through the same
     loop); `log` collects (iter, Etot, diffE, diffRhoe) rows."""
@@ -82,6 +84,9 @@ def KS_solve_SCF(Ham, psiks=None, betamix=0.2, NiterMax=100, mix_method="pulay",
             evals = diag_LOBPCG(Ham, psiks, tol=ethr, Nstates_conv=Ham.Nstates_occ)
         else:
             evals = diag(Ham, psiks, ethr, Ham.Nstates_occ)
+        if use_smearing:
+            Ham.Focc, Ham.E_fermi = calc_Focc(Ham.Nelectrons, pw.kpoints.wk, kT, evals)
+            Ham.mTS = calc_entropy(pw.kpoints.wk, kT, evals, Ham.E_fermi)
         Rhoe_new = calc_rhoe(Ham, psiks)
         diffRhoe = float(np.sum(np.abs(Rhoe_new - Rhoe))) / N
         if mix_method == "simple":

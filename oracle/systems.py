@@ -6,6 +6,8 @@ Oracle (test infrastructure only).
   Si64      2x2x2 conventional diamond cells, a = 20.5262 bohr, Gamma
   Si216     3x3x3 conventional diamond cells, a = 30.7893 bohr, Gamma
   Al4       conventional fcc cell, a = 7.6524 bohr
+  Pt fcc    test/validations_old/Pt_fcc.jl:1-12 (a = 3.9231 angstrom, ecutwfc 30, 3x3x3 MP,
+            4 extra states)
 
 The pseudopotential files are shipped under tests/golden/psp (copied from the
 reference's pseudopotentials/ folder: they are data, read by both the oracle
@@ -50,6 +52,18 @@ def diamond_supercell(n, a_conv, displace=0.0, seed=0):
         rng = np.random.default_rng(seed)
         atoms.positions = atoms.positions + rng.uniform(-displace, displace, atoms.positions.shape)
     return atoms
+
+
+ANG2BOHR = 1.8897261254578281
+
+
+def pt_fcc_atoms():
+    LL = gen_lattice_fcc(3.9231 * ANG2BOHR)
+    return Atoms.from_frac(["Pt"], np.zeros((3, 1)), LL)
+
+
+def Ham_Pt_fcc(meshk=(3, 3, 3)):
+    return Hamiltonian(pt_fcc_atoms(), [psp("Pt-q10.gth")], 30.0, meshk=meshk, extra_states=4)
 
 
 def Ham_Si_fcc(meshk=(3, 3, 3), extra_states=None):

@@ -8,6 +8,8 @@ density mixing):
                            the call of electrons_scf.jl:150)
   calc_rhoe!               pw_calc_rhoe                   (device)
   mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
+  smearing (use_smearing)  KS_solve_SCF.jl:218-223, occupations.jl:6-245  (host: Fermi level
+                           by bisection over the Nstates x Nkpt eigenvalues, -TS)
   rho >= eps clamp         KS_solve_SCF.jl:277-281        (device)
   update!                  pw_update (Poisson, VWN, V_tot) (device)
   calc_energies            pw_update sums + pw_band_energies (device, FP64)
@@ -39,6 +41,48 @@ def occupations(Nelectrons, Nstates, Nkpt):
     F[:nocc - 1, :] = 2.0
     F[nocc - 1, :] = 1.0 if int(round(Nelectrons)) % 2 == 1 else 2.0
     return F, nocc
+
+
+def fermi_dirac(x):
+    """wgauss (occupations.jl:71-83): 1/(1 + e^-x), 0 below -200, 1 above 200."""
+    with np.errstate(over="ignore"):
+        f = 1.0 / (1.0 + np.exp(-x))
+    return np.where(x < -200.0, 0.0, np.where(x > 200.0, 1.0, f))
+
+
+def smeared_occupations(Nelectrons, wk, kT, evals):
+    """calc_Focc + calc_entropy (occupations.jl:6-32, 126-192, 222-245),
+    Nspin = 1: E_fermi by bisection of sum 2 wk f((E - evals)/kT) = Nelectrons
+    between min(evals) - 2kT and max(evals) + 2kT (stop at |N - Nel| < 1e-10
+    or a step below 1e-10, 300 steps at most); Focc = 2 f; mTS = sum 2 wk kT
+    (f log f + (1 - f) log(1 - f)) over |x| <= 36.  Returns (Focc, E_fermi, mTS)."""
+    wk = np.asarray(wk, dtype=np.float64)
+    count = lambda E: float(np.sum(2.0 * wk * fermi_dirac((E - evals) / kT).sum(axis=0)))
+    lo = evals[0, :].min() - 2 * kT
+    hi = evals[-1, :].max() + 2 * kT
+    eps = np.finfo(np.float64).eps
+    if count(hi) - Nelectrons < -eps or count(lo) - Nelectrons > eps:
+        raise ValueError("Bounds for E_fermi is not found")
+    Ef = Ef_old = 0.5 * (lo + hi)
+    for _ in range(300):
+        n = count(Ef)
+        if abs(n - Nelectrons) < 1e-10:
+            break
+        if n - Nelectrons < -1e-10:
+            lo = Ef
+        else:
+            hi = Ef
+        Ef = 0.5 * (lo + hi)
+        if abs(Ef - Ef_old) < 1e-10:
+            break
+        Ef_old = Ef
+    x = (Ef - evals) / kT
+    Focc = 2.0 * fermi_dirac(x)
+    ok = np.abs(x) <= 36.0
+    f = 1.0 / (1.0 + np.exp(-np.where(ok, x, 0.0)))
+    w1 = np.where(ok, f * np.log(f) + (1.0 - f) * np.log(1.0 - f), 0.0)
+    mTS = float(np.sum(2.0 * wk[None, :] * kT * w1))
+    return Focc, Ef, mTS
 
 
 def rand_psiks(Ham, Nstates, seed, dtype):
@@ -94,7 +138,7 @@ class PulayMixer:
 
 def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
-                 verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG"):
+                 verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3):
     """Runs the SCF loop; returns a dict with energies, eigenvalues, timings
     and the per-iteration log."""
     import torch
@@ -131,6 +175,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     t_start = time.perf_counter()
     t_diag = t_rho = t_upd = 0.0
     switched_at = None
+    E_fermi = None
     E = {}
     for it in range(1, NiterMax + 1):
         ethr = 0.1 if it == 1 else (0.01 if it == 2 else max(ethr / 5.0, ethr_evals_last))
@@ -144,6 +189,9 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             evals[:, ik] = ev
             nit.append(n)
         torch.cuda.synchronize()
+        mTS = 0.0
+        if use_smearing:
+            Focc, E_fermi, mTS = smeared_occupations(Nel, wk, kT, evals)
         t1 = time.perf_counter()
         for ik in range(b.Nkpt):
             ctx.calc_rhoe(ik, psiks[ik], wk[ik] * Focc[:, ik], rho_new, accumulate=(ik > 0))
@@ -163,7 +211,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             Ek += e2[0]
             En += e2[1]
         E = {"Kinetic": Ek, "Ps_loc": sums[1] * dVol, "Ps_nloc": En, "Hartree": 0.5 * sums[0] * dVol,
-             "XC": sums[2] * dVol, "NN": E_NN}
+             "XC": sums[2] * dVol, "NN": E_NN, "mTS": mTS}
         E["Total"] = sum(E.values())
         t3 = time.perf_counter()
         t_diag += t1 - t0
@@ -188,6 +236,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             switched_at = it
         Etot_old = E["Total"]
     torch.cuda.synchronize()
-    return {"energies": E, "evals": evals, "iterations": len(log), "log": log, "time_s": time.perf_counter() - t_start,
+    return {"energies": E, "evals": evals, "Focc": Focc, "E_fermi": E_fermi, "iterations": len(log), "log": log,
+            "time_s": time.perf_counter() - t_start,
             "time_diag_s": t_diag, "time_rhoe_s": t_rho, "time_update_s": t_upd, "switched_to_fp64_at": switched_at,
             "psiks": psiks, "rho": rho}

@@ -231,7 +231,7 @@ def projectors(system, basis, pspots, ik):
 
 
 ZATOMS = {"H": 1, "He": 2, "Li": 3, "C": 6, "N": 7, "O": 8, "Na": 11, "Mg": 12, "Al": 13, "Si": 14, "P": 15,
-          "S": 16, "Cl": 17, "Ga": 31, "Ge": 32}
+          "S": 16, "Cl": 17, "Ga": 31, "Ge": 32, "Pt": 78}
 
 
 def kpoint_grid(LatVecs, mesh, time_reversal=True):

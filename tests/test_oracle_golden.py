@@ -3,6 +3,9 @@
 Every constant below is quoted from the reference's tests or logs:
   test/validations_old/Si_fcc.jl:15        Etot(Si fcc, LDA) = -7.9110087934 (ABINIT, atol 1e-5)
   test/validations_old/Si_fcc.jl:94-101    the same Etot with the Davidson eigensolver
+  test/validations_old/Pt_fcc.jl:14         Pt fcc free energy -26.2945054360 (ABINIT, atol 1e-5),
+                                           Fermi-Dirac smearing kT = 1e-3
+  test/LOG_runtest_v.1.1.1:2643-2660       logged components, -TS and E_fermi of that run
   test/LOG_runtest_v.1.1.1:1171-1181       logged energy components of the same run
   test/test_energies.jl:19                 E_NN(Si fcc) = -8.397927400714764
   test/test_xc.jl:3-4                      VWN eps_xc / V_xc at rho = 0.1 .. 0.5 (atol 1e-5)
@@ -111,3 +114,24 @@ def test_si_fcc_total_energy_davidson():
     E, psiks, rho = scf.KS_solve_SCF(H, betamix=0.5, mix_method="pulay", etot_conv_thr=1e-8,
                                      diag=lambda Ham, ps, tol, nconv: davidson.diag_davidson_qe_all(Ham, ps, tol=tol))
     assert abs(E["Total"] - (-7.9110087934)) < 1e-5
+
+
+@pytest.mark.slow
+def test_pt_fcc_smearing_free_energy():
+    """Pt fcc (GTH Pt-q10 with d projectors, ecutwfc 30, 3x3x3 k, 4 extra
+    states), Fermi-Dirac kT = 1e-3, simple mixing beta 0.5
+    (test/validations_old/Pt_fcc.jl:1-50).  That log predates the G = 0
+    term of V_loc(G) (PsPot_GTH.jl:212, 'to match QE'): it reports that
+    term's energy separately (PspCore) and its eigenvalues and E_fermi sit
+    PspCore/Nelectrons lower."""
+    from oracle import scf
+    H = systems.Ham_Pt_fcc()
+    E, _, _ = scf.KS_solve_SCF(H, betamix=0.5, mix_method="simple", etot_conv_thr=1e-8, use_smearing=True, kT=1e-3)
+    assert abs(E["Total"] - (-26.2945054360)) < 1e-5
+    assert abs(E["mTS"] - (-0.0005158875)) < 1e-8
+    assert abs(E["Kinetic"] - 19.2060140731) < 1e-6
+    assert abs(E["Ps_loc"] - (-3.5178517592 + 6.3258423493)) < 1e-6
+    assert abs(E["Ps_nloc"] - (-14.7734350216)) < 1e-6
+    assert abs(E["Hartree"] - 1.8623453874) < 1e-6
+    assert abs(E["XC"] - (-4.4748717329)) < 1e-6
+    assert abs(H.E_fermi - (-0.0148842322 + 6.3258423493 / 10.0)) < 1e-6
