@@ -52,6 +52,7 @@ extern "C" {
 #define PW_OP_VNL      4u   /* op_V_Ps_nloc! op_V_Ps_nloc.jl:39-78 */
 #define PW_OP_H        7u   /* op_H!        op_H.jl:53-63          */
 #define PW_ACCUMULATE  0x100u
+#define PW_GRAPH       0x200u   /* pw_apply_multi: replay a captured CUDA graph */
 
 typedef struct pw_ctx pw_ctx;
 
@@ -107,6 +108,20 @@ int pw_set_nonlocal_coef(pw_ctx *ctx, int nnz, const int32_t *ibeta,
  * Replaces op_H!/op_K!/op_V_loc!/op_V_Ps_nloc! (op_H.jl:53-63). */
 int pw_apply(pw_ctx *ctx, int ik, int ispin, int dtype, const void *psi,
              void *Hpsi, int64_t ld, int nb, unsigned ops);
+
+/* The BlochWavefunc form op_H!(Ham, psiks, Hpsiks) (op_H.jl:4-35,
+ * op_K.jl:17-29, op_V_loc.jl:17-28, op_V_Ps_nloc.jl:22-37) for spin
+ * ispin: Hpsi[i] (+)= H(k = iks[i]) psi[i] for nk k-points in one launch
+ * per stage (their Ngw differ).  psi, Hpsi: host arrays of nk device
+ * pointers (Ngw x nb[i], leading dimension ld[i]).  ops must contain
+ * PW_OP_VLOC (op_K and op_V_Ps_nloc optional, PW_ACCUMULATE as pw_apply);
+ * cube grids of 27, 75 or 120 points, at most 65535 bands and 2048
+ * projectors.  With PW_GRAPH the launches are captured in a CUDA graph and
+ * a later call with the same k-points, blocks, flags and buffers replays
+ * it. */
+int pw_apply_multi(pw_ctx *ctx, int nk, const int *iks, int ispin, int dtype,
+                   void *const *psi, void *const *Hpsi, const int64_t *ld,
+                   const int *nb, unsigned ops);
 
 /* out = in / (1 + |G+k|^2)  (Kprec.jl:97-111; in == out allowed). */
 int pw_kprec(pw_ctx *ctx, int ik, int dtype, const void *in, void *out,

@@ -66,6 +66,16 @@ def Ham_Pt_fcc(meshk=(3, 3, 3)):
     return Hamiltonian(pt_fcc_atoms(), [psp("Pt-q10.gth")], 30.0, meshk=meshk, extra_states=4)
 
 
+def al4_atoms():
+    """Conventional fcc Al cell, a = 7.6524 bohr, 4 atoms."""
+    frac = np.array([[0.0, 0.0, 0.0], [0.0, 0.5, 0.5], [0.5, 0.0, 0.5], [0.5, 0.5, 0.0]]).T
+    return Atoms.from_frac(["Al"] * 4, frac, gen_lattice_cubic(7.6524))
+
+
+def Ham_Al4(meshk=(8, 8, 8), Nstates=10):
+    return Hamiltonian(al4_atoms(), [psp("Al-q3.gth")], 15.0, meshk=meshk, Nstates=Nstates)
+
+
 def Ham_Si_fcc(meshk=(3, 3, 3), extra_states=None):
     return Hamiltonian(si_fcc_atoms(), [psp("Si-q4.gth")], 15.0, meshk=meshk,
                        extra_states=extra_states)

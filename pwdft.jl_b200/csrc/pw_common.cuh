@@ -48,3 +48,16 @@ struct KPlan {
     const double *Gk2;     // [Ngw] |G+k|^2
     const float *Gk2f;     // [Ngw] |G+k|^2 (FP32 copy)
 };
+
+// One k-point of a batched op_H (every k-point and band in one launch per
+// stage): its plan, its blocks, where its bands start in the batch's band
+// list and in the intermediate A, and its projectors.
+struct MkK {
+    KPlan kp;
+    const void *psi;    // Ngw x nb (ld), launch precision
+    void *Hpsi;         // Ngw x nb (ld)
+    const void *beta;   // Ngw x nbeta projectors (ld Ngw), launch precision; null: no V_NL
+    int64_t ld;
+    size_t a_off;       // element offset of the k-point's band 0 in A
+    int band0, nb;
+};

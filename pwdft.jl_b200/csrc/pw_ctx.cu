@@ -101,6 +101,12 @@ struct pw_ctx {
     // vectors of the density sphere, 3 x Ng, for grad rho and div h)
     int xc = PW_XC_VWN;
     double *d_xcG = nullptr;
+    // batched op_H over k-points: device tables (MkK per k-point, band ->
+    // k-point map), and the CUDA graph of the last call made with PW_GRAPH
+    DevBuf mk_tab;
+    uint64_t mk_key = 0;
+    cudaGraphExec_t mk_exec = nullptr;
+    cudaStream_t cap_stream = nullptr;
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -547,6 +553,8 @@ extern "C" void pw_destroy(pw_ctx *c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->mk_exec) cudaGraphExecDestroy(c->mk_exec);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     for (void *p : c->allocs) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -689,6 +697,132 @@ extern "C" int pw_apply(pw_ctx *c, int ik, int ispin, int dtype, const void *psi
     CK(c, cudaSetDevice(c->device));
     return dtype == PW_C128 ? apply_T<double>(c, ik, ispin, psi, Hpsi, ld, nb, ops)
                             : apply_T<float>(c, ik, ispin, psi, Hpsi, ld, nb, ops);
+}
+
+// ------------------------------------------------- batched op_H (k-points)
+namespace {
+uint64_t fnv(uint64_t h, const void *p, size_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    return h;
+}
+
+template <typename T>
+int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi, void *const *Hpsi, const int64_t *ld,
+                  const int *nb, unsigned ops) {
+    const unsigned o = ops & PW_OP_H;
+    const size_t es = 2 * sizeof(T);
+    if (!(o & PW_OP_VLOC)) return fail(c, PW_ERR_UNSUPPORTED, "the batched op_H needs PW_OP_VLOC");
+    if (c->N1 != c->N2 || c->N2 != c->N3 || (c->N1 != 27 && c->N1 != 75 && c->N1 != 120))
+        return fail(c, PW_ERR_UNSUPPORTED, "the batched op_H runs on cube grids of 27, 75 or 120 points");
+    if (c->vloc_nspin <= 0) return fail(c, PW_ERR_STATE, "op_V_loc requested before pw_set_vloc");
+    if (ispin < 0 || ispin >= c->vloc_nspin) return fail(c, PW_ERR_ARG, "spin index %d outside [0, %d)", ispin, c->vloc_nspin);
+    const bool vnl = (o & PW_OP_VNL) != 0;
+    if (vnl && (c->nbeta <= 0 || !c->have_D)) return fail(c, PW_ERR_STATE, "op_V_Ps_nloc requested but projectors are not set");
+    if (vnl && c->nbeta > 2048) return fail(c, PW_ERR_UNSUPPORTED, "the batched op_V_Ps_nloc takes at most 2048 projectors");
+    std::vector<MkK> tab(nk);
+    std::vector<int> band_k;
+    size_t aoff = 0;
+    int maxcol = 0, kx = iks[0];
+    for (int i = 0; i < nk; ++i) {
+        const KData &kd = c->k[iks[i]];
+        const void *beta = sizeof(T) == 8 ? (const void *)kd.d_beta64 : (const void *)kd.d_beta32;
+        if (vnl && !beta) return fail(c, PW_ERR_STATE, "projectors of k-point %d are not set", iks[i]);
+        MkK &K = tab[i];
+        K.kp = make_launch<T>(c, iks[i]).kp;
+        K.psi = psi[i];
+        K.Hpsi = Hpsi[i];
+        K.beta = vnl ? beta : nullptr;
+        K.ld = ld[i];
+        K.a_off = aoff;
+        K.band0 = (int)band_k.size();
+        K.nb = nb[i];
+        aoff += (size_t)nb[i] * c->N3 * kd.Ncol;
+        band_k.insert(band_k.end(), nb[i], i);
+        maxcol = std::max(maxcol, kd.Ncol);
+        if (kd.Nxa > c->k[kx].Nxa) kx = iks[i];
+    }
+    const int nbands = (int)band_k.size();
+    if (nbands > 65535) return fail(c, PW_ERR_UNSUPPORTED, "the batched op_H takes at most 65535 bands per call");
+    int s;
+    if ((s = ensure(c, c->A, aoff * es))) return s;
+    const size_t tab_bytes = (size_t)nk * sizeof(MkK), bk_bytes = (size_t)nbands * sizeof(int);
+    const size_t bk_off = (tab_bytes + 255) / 256 * 256;
+    if ((s = ensure(c, c->mk_tab, bk_off + bk_bytes))) return s;
+    const void *V = sizeof(T) == 8 ? (const void *)(c->d_V64 + (size_t)ispin * c->N)
+                                   : (const void *)(c->d_V32 + (size_t)ispin * c->N);
+    const int flags = ((o & PW_OP_K) ? 2 : 0) | ((ops & PW_ACCUMULATE) ? 4 : 0);
+    const FftLaunch L = make_launch<T>(c, kx);
+    const MkK *d_tab = (const MkK *)c->mk_tab.p;
+    const int *d_bk = (const int *)((const char *)c->mk_tab.p + bk_off);
+    const int nlaunch = vnl ? 4 : 3;
+    // graph replay: same blocks, k-points, flags and buffers as the captured call
+    uint64_t key = 1469598103934665603ull;
+    key = fnv(key, tab.data(), tab_bytes);
+    key = fnv(key, &V, sizeof(V));
+    key = fnv(key, &c->A.p, sizeof(void *));
+    key = fnv(key, &c->mk_tab.p, sizeof(void *));
+    key = fnv(key, &flags, sizeof(flags));
+    key = fnv(key, &nbands, sizeof(nbands));
+    if ((ops & PW_GRAPH) && c->mk_exec && key == c->mk_key) {
+        CK(c, cudaGraphLaunch(c->mk_exec, c->stream));
+        c->launches += nlaunch;
+        return PW_OK;
+    }
+    CK(c, cudaMemcpyAsync(c->mk_tab.p, tab.data(), tab_bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync((char *)c->mk_tab.p + bk_off, band_k.data(), bk_bytes, cudaMemcpyHostToDevice, c->stream));
+    auto run = [&](cudaStream_t st) {
+        return launch_multik<T>(L, d_tab, d_bk, nbands, maxcol, V, c->A.p, flags, c->d_Drow, c->d_Dcol, c->d_Dval,
+                                vnl ? c->nbeta : 0, st);
+    };
+    CK(c, run(c->stream));
+    c->launches += nlaunch;
+    if (ops & PW_GRAPH) {
+        // capture the same launches for replay (the tables stay resident)
+        CK(c, cudaStreamSynchronize(c->stream));
+        if (!c->cap_stream) CK(c, cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+        if (c->mk_exec) {
+            CK(c, cudaGraphExecDestroy(c->mk_exec));
+            c->mk_exec = nullptr;
+            c->mk_key = 0;
+        }
+        cudaGraph_t g = nullptr;
+        CK(c, cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed));
+        const cudaError_t e = run(c->cap_stream);
+        const cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(c, PW_ERR_CUDA, "capturing the batched op_H failed: %s",
+                        cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&c->mk_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            c->mk_exec = nullptr;
+            return fail(c, PW_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(e3));
+        }
+        c->mk_key = key;
+    }
+    return PW_OK;
+}
+}  // namespace
+
+extern "C" int pw_apply_multi(pw_ctx *c, int nk, const int *iks, int ispin, int dtype, void *const *psi,
+                              void *const *Hpsi, const int64_t *ld, const int *nb, unsigned ops) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_dtype(c, dtype))) return s;
+    if (nk <= 0 || !iks || !psi || !Hpsi || !ld || !nb) return fail(c, PW_ERR_ARG, "bad pw_apply_multi arguments");
+    if (ops & ~(PW_OP_H | PW_ACCUMULATE | PW_GRAPH)) return fail(c, PW_ERR_ARG, "unknown op flags 0x%x", ops);
+    for (int i = 0; i < nk; ++i) {
+        if ((s = check_k(c, iks[i]))) return s;
+        if (!psi[i] || !Hpsi[i]) return fail(c, PW_ERR_ARG, "NULL wavefunction pointer (entry %d)", i);
+        if (psi[i] == Hpsi[i]) return fail(c, PW_ERR_ARG, "psi and Hpsi must not alias (entry %d)", i);
+        if (nb[i] <= 0 || ld[i] < c->k[iks[i]].Ngw) return fail(c, PW_ERR_ARG, "bad shape of entry %d", i);
+    }
+    CK(c, cudaSetDevice(c->device));
+    return dtype == PW_C128 ? apply_multi_T<double>(c, nk, iks, ispin, psi, Hpsi, ld, nb, ops)
+                            : apply_multi_T<float>(c, nk, iks, ispin, psi, Hpsi, ld, nb, ops);
 }
 
 extern "C" int pw_kprec(pw_ctx *c, int ik, int dtype, const void *in, void *out, int64_t ld, int nb) {

@@ -264,14 +264,14 @@ template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int v = 2; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
 
+// z-pass bodies for one band: ps / hs its sphere coefficients, Ab its
+// [z][column] block of the intermediate, column group blockIdx.x
 template <typename T, int N3>
-__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
-kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, int64_t ld, Cx<T> *__restrict__ A,
-        int Cg) {
+__device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ ps,
+                                          Cx<T> *__restrict__ Ab, int Cg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *Z = tw + N3;
-    const int b = blockIdx.y;
     const int c0 = blockIdx.x * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -279,35 +279,38 @@ kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, 
     for (int i = threadIdx.x; i < N3 * Cg; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
     __syncthreads();
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
-    const Cx<T> *ps = psi + (size_t)b * ld;
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0] = ps[kp.ent_igw[e]];
     __syncthreads();
     line_fft<T, N3, false>(Z, cn, Cg, 1, tw, +1);
-    Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol + c0;
+    Ab += c0;
     for (int kz = warp; kz < N3; kz += nw)
         for (int cl = lane; cl < cn; cl += 32) Ab[(size_t)kz * kp.Ncol + cl] = Z[kz * Cg + cl];
 }
 
 template <typename T, int N3>
 __global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
-kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, const Cx<T> *__restrict__ psi,
-        Cx<T> *__restrict__ Hpsi, int64_t ld, int Cg, int flags) {
+kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, int64_t ld, Cx<T> *__restrict__ A,
+        int Cg) {
+    const int b = blockIdx.y;
+    zinv_band<T, N3>(kp, twz, psi + (size_t)b * ld, A + (size_t)b * N3 * kp.Ncol, Cg);
+}
+
+template <typename T, int N3>
+__device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ Ab,
+                                          const Cx<T> *__restrict__ ps, Cx<T> *__restrict__ hs, int Cg, int flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *Z = tw + N3;
-    const int b = blockIdx.y;
     const int c0 = blockIdx.x * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
-    const Cx<T> *Ab = A + (size_t)b * N3 * kp.Ncol + c0;
+    Ab += c0;
     for (int kz = warp; kz < N3; kz += nw)
         for (int cl = lane; cl < cn; cl += 32) Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + cl];
     __syncthreads();
     line_fft<T, N3, false>(Z, cn, Cg, 1, tw, -1);
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
-    const Cx<T> *ps = psi + (size_t)b * ld;
-    Cx<T> *hs = Hpsi + (size_t)b * ld;
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int igw = kp.ent_igw[e];
         Cx<T> out = Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0];
@@ -318,6 +321,14 @@ kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, co
         if (flags & 4) out = cadd(out, hs[igw]);
         hs[igw] = out;
     }
+}
+
+template <typename T, int N3>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, const Cx<T> *__restrict__ psi,
+        Cx<T> *__restrict__ Hpsi, int64_t ld, int Cg, int flags) {
+    const int b = blockIdx.y;
+    zfwd_band<T, N3>(kp, twz, A + (size_t)b * N3 * kp.Ncol, psi + (size_t)b * ld, Hpsi + (size_t)b * ld, Cg, flags);
 }
 
 template <typename T, int N1, int N2>
@@ -334,22 +345,22 @@ __device__ __forceinline__ void plane_to_real(const KPlan &kp, Cx<T> *S, Cx<T> *
 }
 
 template <typename T, int N1, int N2>
-__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
-kf_plane_vloc(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
-              Cx<T> *__restrict__ A, int Jc) {
+__device__ __forceinline__ void plane_vloc_band(const KPlan &kp, const Cx<T> *__restrict__ twx,
+                                                const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
+                                                Cx<T> *__restrict__ Ab, int Jc) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    const int Nxa = kp.Nxa, Ncol = kp.Ncol;
     Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *ty = tx + N1;
     Cx<T> *S = ty + N2;
     Cx<T> *X = S + Nxa * N2;
-    const int kz = blockIdx.x, b = blockIdx.y;
+    const int kz = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
     for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
     for (int i = threadIdx.x; i < Nxa * N2; i += blockDim.x) S[i] = cmake((T)0, (T)0);
     __syncthreads();
-    Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+    Cx<T> *Ap = Ab + (size_t)kz * Ncol;
     for (int c = threadIdx.x; c < Ncol; c += blockDim.x) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
     __syncthreads();
     line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);
@@ -368,6 +379,13 @@ kf_plane_vloc(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__
     }
     line_fft<T, N2, true>(S, Nxa, 1, N2, ty, -1);
     for (int c = threadIdx.x; c < Ncol; c += blockDim.x) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+kf_plane_vloc(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
+              Cx<T> *__restrict__ A, int Jc) {
+    plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + (size_t)blockIdx.y * kp.N3 * kp.Ncol, Jc);
 }
 
 template <typename T, int N1, int N2>
@@ -431,13 +449,13 @@ struct PlaneXSmem {
 };
 
 template <int N1, int N2, bool VS>
-__global__ void __launch_bounds__(FFT_THREADS, 2)
-kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
-              float2 *__restrict__ A) {
+__device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 *__restrict__ twx,
+                                                  const float2 *__restrict__ twy, const float *__restrict__ Vr,
+                                                  float2 *__restrict__ Ab) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = float;
     constexpr int G = pwf::fp_group<N1>();
-    const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
+    const int Nxa = kp.Nxa, Ncol = kp.Ncol;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = FFT_THREADS / 32;
     Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
@@ -446,7 +464,7 @@ kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict
     Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * N1;
     float *Vs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * N1);
     short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
-    const int kz = blockIdx.x, b = blockIdx.y;
+    const int kz = blockIdx.x;
     const float *Vp = Vr + (size_t)kz * N1 * N2;
     if constexpr (VS)
         for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[i], &Vp[i]);
@@ -458,7 +476,7 @@ kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict
     for (int i = threadIdx.x; i < Nxa * N2; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
     __syncthreads();
     for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
-    Cx<T> *Ap = A + ((size_t)b * N3 + kz) * Ncol;
+    Cx<T> *Ap = Ab + (size_t)kz * Ncol;
 #pragma unroll 4
     for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
     __syncthreads();
@@ -489,6 +507,13 @@ kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict
     line_fft<T, N2, true>(S, Nxa, 1, N2, ty, -1);
 #pragma unroll 4
     for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
+}
+
+template <int N1, int N2, bool VS>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
+              float2 *__restrict__ A) {
+    plane_vloc_x_band<N1, N2, VS>(kp, twx, twy, Vr, A + (size_t)blockIdx.y * kp.N3 * kp.Ncol);
 }
 
 // calc_rhoe: bands [g*Bg, min(nb, (g+1)*Bg)) of plane kz; the weighted
@@ -545,6 +570,108 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
     }
     if constexpr (RS)
         for (int i = threadIdx.x; i < N12; i += FFT_THREADS) rp[i] = Rs[i];
+}
+
+// ------------------------------------------ batched op_H over k-points
+// One launch per stage for the bands of many k-points (their Ngw, columns
+// and active x differ): blockIdx.y is a band of the batch, band_k its
+// k-point, whose plan, blocks and offset in A come from ks.  The band
+// bodies are the single-k-point kernels' own.
+template <typename T, int N3>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+mk_zinv(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> *__restrict__ twz, Cx<T> *__restrict__ A,
+        int Cg) {
+    const MkK &K = ks[band_k[blockIdx.y]];
+    const KPlan kp = K.kp;
+    if (blockIdx.x * Cg >= kp.Ncol) return;
+    const int b = blockIdx.y - K.band0;
+    zinv_band<T, N3>(kp, twz, (const Cx<T> *)K.psi + (size_t)b * K.ld, A + K.a_off + (size_t)b * N3 * kp.Ncol, Cg);
+}
+
+template <typename T, int N3>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+mk_zfwd(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> *__restrict__ twz,
+        const Cx<T> *__restrict__ A, int Cg, int flags) {
+    const MkK &K = ks[band_k[blockIdx.y]];
+    const KPlan kp = K.kp;
+    if (blockIdx.x * Cg >= kp.Ncol) return;
+    const int b = blockIdx.y - K.band0;
+    zfwd_band<T, N3>(kp, twz, A + K.a_off + (size_t)b * N3 * kp.Ncol, (const Cx<T> *)K.psi + (size_t)b * K.ld,
+                     (Cx<T> *)K.Hpsi + (size_t)b * K.ld, Cg, flags);
+}
+
+template <int N1, int N2, bool VS>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+mk_plane_vloc_x(const MkK *__restrict__ ks, const int *__restrict__ band_k, const float2 *__restrict__ twx,
+                const float2 *__restrict__ twy, const float *__restrict__ Vr, float2 *__restrict__ A) {
+    const MkK &K = ks[band_k[blockIdx.y]];
+    const KPlan kp = K.kp;
+    const int b = blockIdx.y - K.band0;
+    plane_vloc_x_band<N1, N2, VS>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol);
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+mk_plane_vloc(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> *__restrict__ twx,
+              const Cx<T> *__restrict__ twy, const T *__restrict__ Vr, Cx<T> *__restrict__ A, int Jc) {
+    const MkK &K = ks[band_k[blockIdx.y]];
+    const KPlan kp = K.kp;
+    const int b = blockIdx.y - K.band0;
+    plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, Jc);
+}
+
+// op_V_Ps_nloc for small projector sets, one CTA per band of the batch:
+// P = betaNL' psi (FP64 sums, one warp per projector), P2 = D P (the
+// (ibeta, jbeta, h) list as CSR), Hpsi += betaNL P2
+template <typename T>
+__global__ void __launch_bounds__(256)
+mk_vnl(const MkK *__restrict__ ks, const int *__restrict__ band_k, const int *__restrict__ Drow,
+       const int *__restrict__ Dcol, const double *__restrict__ Dval, int nbeta) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *P = reinterpret_cast<double2 *>(smem_raw);
+    double2 *P2 = P + nbeta;
+    const MkK &K = ks[band_k[blockIdx.x]];
+    const int b = blockIdx.x - K.band0;
+    const int ngw = K.kp.Ngw;
+    const Cx<T> *beta = (const Cx<T> *)K.beta;
+    const Cx<T> *ps = (const Cx<T> *)K.psi + (size_t)b * K.ld;
+    Cx<T> *hs = (Cx<T> *)K.Hpsi + (size_t)b * K.ld;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int j = warp; j < nbeta; j += nw) {
+        const Cx<T> *bj = beta + (size_t)j * ngw;
+        double re = 0.0, im = 0.0;
+        for (int g = lane; g < ngw; g += 32) {
+            const Cx<T> u = bj[g], v = ps[g];
+            re += (double)u.x * v.x + (double)u.y * v.y;
+            im += (double)u.x * v.y - (double)u.y * v.x;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, o);
+            im += __shfl_xor_sync(0xffffffffu, im, o);
+        }
+        if (lane == 0) P[j] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nbeta; i += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int e = Drow[i]; e < Drow[i + 1]; ++e) {
+            re += Dval[e] * P[Dcol[e]].x;
+            im += Dval[e] * P[Dcol[e]].y;
+        }
+        P2[i] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < ngw; g += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int i = 0; i < nbeta; ++i) {
+            const Cx<T> u = beta[(size_t)i * ngw + g];
+            const double2 q = P2[i];
+            re += (double)u.x * q.x - (double)u.y * q.y;
+            im += (double)u.x * q.y + (double)u.y * q.x;
+        }
+        const Cx<T> h = hs[g];
+        hs[g] = cmake((T)(h.x + re), (T)(h.y + im));
+    }
 }
 
 }  // namespace pwk
@@ -652,6 +779,57 @@ static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb,
     return cudaGetLastError();
 }
 
+// Batched op_H stages over the bands of many k-points (cube grids of the
+// compiled sizes).  L: twiddles, Cg and Jc of the k-point with the most
+// active x (sizes the plane pass's shared memory); max_ncol sizes the z
+// grids.  flags as kf_zfwd (2: + op_K, 4: accumulate).
+template <typename T>
+cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, int nbands, int max_ncol,
+                          const void *Vr, void *A, int flags, const int *Drow, const int *Dcol, const double *Dval,
+                          int nbeta, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    if (kp.N1 != kp.N2 || kp.N2 != kp.N3) return cudaErrorNotSupported;
+    const int Cg = L.Cg;
+    const size_t zsm = (size_t)(kp.N3 + kp.N3 * Cg) * sizeof(Cx<T>);
+    const dim3 zgrid((max_ncol + Cg - 1) / Cg, nbands);
+    cudaError_t e = cudaErrorNotSupported;
+#define PW_CASE(NN)                                                                                                  \
+    if (kp.N1 == NN) {                                                                                               \
+        if ((e = set_smem<T>((const void *)mk_zinv<T, NN>, zsm)) != cudaSuccess) return e;                          \
+        mk_zinv<T, NN><<<zgrid, FFT_THREADS, zsm, st>>>(ks, band_k, (const Cx<T> *)L.twz, (Cx<T> *)A, Cg);           \
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;                                                       \
+        if constexpr (sizeof(T) == 4) {                                                                              \
+            constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
+            const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};           \
+            const size_t psm = ps.elems() * sizeof(float2);                                                          \
+            if ((e = set_smem<float>((const void *)mk_plane_vloc_x<NN, NN, VS>, psm)) != cudaSuccess) return e;     \
+            mk_plane_vloc_x<NN, NN, VS><<<dim3(NN, nbands), FFT_THREADS, psm, st>>>(                                 \
+                ks, band_k, (const float2 *)L.twx, (const float2 *)L.twy, (const float *)Vr, (float2 *)A);          \
+        } else {                                                                                                     \
+            const PlaneSmem ps{NN, NN, kp.Nxa, L.Jc};                                                                \
+            const size_t psm = ps.elems() * sizeof(Cx<T>);                                                           \
+            if ((e = set_smem<T>((const void *)mk_plane_vloc<T, NN, NN>, psm)) != cudaSuccess) return e;            \
+            mk_plane_vloc<T, NN, NN><<<dim3(NN, nbands), FFT_THREADS, psm, st>>>(                                    \
+                ks, band_k, (const Cx<T> *)L.twx, (const Cx<T> *)L.twy, (const T *)Vr, (Cx<T> *)A, L.Jc);           \
+        }                                                                                                            \
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;                                                       \
+        if ((e = set_smem<T>((const void *)mk_zfwd<T, NN>, zsm)) != cudaSuccess) return e;                          \
+        mk_zfwd<T, NN><<<zgrid, FFT_THREADS, zsm, st>>>(ks, band_k, (const Cx<T> *)L.twz, (const Cx<T> *)A, Cg,      \
+                                                        flags);                                                      \
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;                                                       \
+    }
+    FIXED_SIZES(PW_CASE)
+#undef PW_CASE
+    if (e != cudaSuccess) return e;
+    if (nbeta > 0) {
+        const size_t vsm = 2 * (size_t)nbeta * sizeof(double2);
+        if ((e = set_smem<T>((const void *)mk_vnl<T>, vsm)) != cudaSuccess) return e;
+        mk_vnl<T><<<nbands, 256, vsm, st>>>(ks, band_k, Drow, Dcol, Dval, nbeta);
+        e = cudaGetLastError();
+    }
+    return e;
+}
+
 template <typename T>
 cudaError_t launch_plane_vloc(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
     const KPlan &kp = L.kp;
@@ -752,6 +930,8 @@ cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t st) {
     template cudaError_t launch_zfwd<T>(const FftLaunch &, const void *, const void *, void *, int64_t, int, int,  \
                                         cudaStream_t);                                                               \
     template cudaError_t launch_plane_vloc<T>(const FftLaunch &, const void *, void *, int, cudaStream_t);          \
+    template cudaError_t launch_multik<T>(const FftLaunch &, const MkK *, const int *, int, int, const void *, void *,  \
+                                          int, const int *, const int *, const double *, int, cudaStream_t);         \
     template cudaError_t launch_plane_rho<T>(const FftLaunch &, const void *, int, int, int, const double *, void *, \
                                              cudaStream_t);                                                          \
     template cudaError_t launch_rho_reduce<T>(const void *, int, size_t, double *, int, cudaStream_t);              \

@@ -15,6 +15,7 @@ PW_OK, PW_ERR_ARG, PW_ERR_CUDA, PW_ERR_NOMEM, PW_ERR_NOT_POSDEF, PW_ERR_NAN, PW_
 PW_C128, PW_C64 = 0, 1
 PW_OP_K, PW_OP_VLOC, PW_OP_VNL, PW_OP_H = 1, 2, 4, 7
 PW_ACCUMULATE = 0x100
+PW_GRAPH = 0x200
 PW_XC_VWN, PW_XC_PBE = 0, 1
 
 STATUS_NAMES = {0: "PW_OK", 1: "PW_ERR_ARG", 2: "PW_ERR_CUDA", 3: "PW_ERR_NOMEM", 4: "PW_ERR_NOT_POSDEF",
@@ -56,6 +57,7 @@ SIGNATURES = {
     "pw_set_nonlocal": (_i, [_vp, _i, _dp, _i]),
     "pw_set_nonlocal_coef": (_i, [_vp, _i, _i32p, _i32p, _dp]),
     "pw_apply": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _u]),
+    "pw_apply_multi": (_i, [_vp, _i, _i32p, _i, _i, C.POINTER(_vp), C.POINTER(_vp), _i64p, _i32p, _u]),
     "pw_apply_vloc_noalloc": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _u]),
     "pw_noalloc_scratch_bytes": (C.c_uint64, []),
     "pw_kprec": (_i, [_vp, _i, _i, _vp, _vp, _i64, _i]),

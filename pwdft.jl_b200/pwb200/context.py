@@ -9,7 +9,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (lib, check, pw_grid_desc, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE)
+from ._lib import (lib, check, pw_grid_desc, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE, PW_GRAPH)
 
 _dp = C.POINTER(C.c_double)
 
@@ -123,6 +123,25 @@ class Context:
         self.use_torch_stream()
         self._chk(self._L.pw_apply(self.h, ik, ispin, dtype_code(psi), C.c_void_p(psi.data_ptr()),
                                    C.c_void_p(Hpsi.data_ptr()), ld, nb, ops))
+
+    def apply_multi(self, iks, ispin, psis, Hpsis, ops=PW_OP_H, graph=False):
+        """pw_apply_multi: Hpsis[i] (+)= H(k = iks[i]) psis[i] for every k-point
+        in one launch per stage; psis / Hpsis: lists of torch (nb, Ngw)
+        blocks of one dtype.  graph=True replays a captured CUDA graph when
+        the k-points, blocks and flags repeat."""
+        n = len(iks)
+        assert n == len(psis) == len(Hpsis) and n > 0
+        k = np.ascontiguousarray(np.asarray(iks, dtype=np.int32))
+        P = (C.c_void_p * n)(*[p.data_ptr() for p in psis])
+        H = (C.c_void_p * n)(*[h.data_ptr() for h in Hpsis])
+        ld = np.ascontiguousarray(np.array([p.shape[1] for p in psis], dtype=np.int64))
+        nb = np.ascontiguousarray(np.array([p.shape[0] for p in psis], dtype=np.int32))
+        for p, h in zip(psis, Hpsis):
+            assert p.dtype == psis[0].dtype == h.dtype and p.is_contiguous() and h.is_contiguous()
+        self.use_torch_stream()
+        self._chk(self._L.pw_apply_multi(self.h, n, k.ctypes.data_as(C.POINTER(C.c_int32)), ispin,
+                                         dtype_code(psis[0]), P, H, ld.ctypes.data_as(C.POINTER(C.c_int64)),
+                                         nb.ctypes.data_as(C.POINTER(C.c_int32)), ops | (PW_GRAPH if graph else 0)))
 
     def apply_vloc_noalloc(self, ik, ispin, psi, Hpsi, ops):
         """pw_apply_vloc_noalloc: the V_loc (+K) round trip using the library's
