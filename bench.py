@@ -45,6 +45,7 @@ A_SI = 10.2631
 NBANDS = 160
 SEED = 20261203
 PSP = os.path.join(ROOT, "tests", "golden", "psp", "Si-q4.gth")
+PSP_AL = os.path.join(ROOT, "tests", "golden", "psp", "Al-q3.gth")
 DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -266,6 +267,64 @@ def time_device(ctx, x, y, ops, steps, warmup, flush):
     return [s.elapsed_time(e) for s, e in ev]
 
 
+def multik_comparison(device, steps, flush):
+    """Batched op_H over uneven k-points: Al4 conventional fcc cell
+    (a = 7.6524 bohr, GTH Al-q3, ecutwfc 15 Ha, 27^3 grid), 8x8x8 k-mesh
+    reduced by time reversal, 10 bands per k-point, V_loc = V_Ps_loc + a
+    seeded smooth field, psi seeded and orthonormal (FP32).  Three arms on
+    the same blocks: a host loop of pw_apply per k-point, one pw_apply_multi
+    (one launch per stage for all k-points), and its CUDA-graph replay;
+    device time per full op_H, L2 flushed between steps."""
+    import torch
+    import pwb200
+    from pwb200.system import kpoint_grid
+    LL = 7.6524 * np.eye(3)
+    frac = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]]).T
+    k, w = kpoint_grid(LL, (8, 8, 8))
+    H = pwb200.Hamiltonian(pwb200.System(["Al"] * 4, LL @ frac, LL), [PSP_AL], 15.0, kpts=k, wk=w, device=device)
+    rng = np.random.default_rng(SEED + 3)
+    b = H.basis
+    H.update_vloc(H.V_Ps_loc + 0.01 * smooth_field(b.Ns, b.G2, b.idx_g2r, rng))
+    nb = 10
+    dev = f"cuda:{device}"
+    X = [torch.from_numpy(np.ascontiguousarray(orthonormal_psi(b.Ngw[ik], nb, rng).T)).to(dev).to(torch.complex64)
+         .contiguous() for ik in range(b.Nkpt)]
+    Y = [torch.empty_like(x) for x in X]
+    iks = list(range(b.Nkpt))
+    nbytes = sum(nb * byte_model(b.Ns, b.idx_gw2r[ik], nb)[0] for ik in iks)
+    ctx = H.ctx
+
+    def loop():
+        for ik in iks:
+            ctx.apply(ik, 0, X[ik], Y[ik])
+
+    arms = {"per_k_loop": loop, "batched": lambda: ctx.apply_multi(iks, 0, X, Y),
+            "batched_graph": lambda: ctx.apply_multi(iks, 0, X, Y, graph=True)}
+    res = {}
+    stream = torch.cuda.current_stream()
+    for name, fn in arms.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        n0 = ctx.launch_count()
+        ts = []
+        for _ in range(steps):
+            flush.add_(1)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            torch.cuda.synchronize()
+            ts.append(s.elapsed_time(e))
+        ms = sum(ts) / len(ts)
+        res[name] = {"ms": ms, "GB_s": nbytes / (ms * 1e-3) / 1e9,
+                     "launches_per_op_H": (ctx.launch_count() - n0) // steps}
+    ctx.close()
+    return {"workload": "Al4 fcc conventional, 8x8x8 k-mesh (time reversal: %d k-points, Ngw %d-%d), %d bands/k, "
+                        "27^3 grid, NbetaNL %d, FP32" % (b.Nkpt, min(b.Ngw), max(b.Ngw), nb, H.NbetaNL),
+            "bytes_per_op_H": nbytes, **res}
+
+
 def cpu_reference(psi, steps, warmup, budget_s):
     """The FP64 oracle op_H on the host cores: bounded band sample per step."""
     from oracle import systems, ops
@@ -429,6 +488,8 @@ def main():
     }
     if scf_out is not None:
         out["scf"] = scf_out
+    if os.environ.get("PW_BENCH_NO_MULTIK") != "1" and world == 1:
+        out["multik"] = multik_comparison(local, max(5, args.steps // 20), flush)
     if rank == 0 and world == 1 and args.workload == "si64" and os.environ.get("PW_BENCH_NO_CPU") != "1":
         dt, nsamp, reps = cpu_reference(psi, 1000, 1, args.cpu_budget)
         v = nsamp * bpb / dt / 1e9
