@@ -723,7 +723,7 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
     std::vector<MkK> tab(nk);
     std::vector<int> band_k;
     size_t aoff = 0;
-    int maxcol = 0, kx = iks[0];
+    int maxcol = 0, maxnb = 0, kx = iks[0];
     for (int i = 0; i < nk; ++i) {
         const KData &kd = c->k[iks[i]];
         const void *beta = sizeof(T) == 8 ? (const void *)kd.d_beta64 : (const void *)kd.d_beta32;
@@ -740,6 +740,7 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
         aoff += (size_t)nb[i] * c->N3 * kd.Ncol;
         band_k.insert(band_k.end(), nb[i], i);
         maxcol = std::max(maxcol, kd.Ncol);
+        maxnb = std::max(maxnb, nb[i]);
         if (kd.Nxa > c->k[kx].Nxa) kx = iks[i];
     }
     const int nbands = (int)band_k.size();
@@ -772,8 +773,8 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
     CK(c, cudaMemcpyAsync(c->mk_tab.p, tab.data(), tab_bytes, cudaMemcpyHostToDevice, c->stream));
     CK(c, cudaMemcpyAsync((char *)c->mk_tab.p + bk_off, band_k.data(), bk_bytes, cudaMemcpyHostToDevice, c->stream));
     auto run = [&](cudaStream_t st) {
-        return launch_multik<T>(L, d_tab, d_bk, nbands, maxcol, V, c->A.p, flags, c->d_Drow, c->d_Dcol, c->d_Dval,
-                                vnl ? c->nbeta : 0, st);
+        return launch_multik<T>(L, d_tab, d_bk, nk, nbands, maxnb, maxcol, V, c->A.p, flags, c->d_Drow, c->d_Dcol,
+                                c->d_Dval, vnl ? c->nbeta : 0, st);
     };
     CK(c, run(c->stream));
     c->launches += nlaunch;

@@ -620,6 +620,72 @@ mk_plane_vloc(const MkK *__restrict__ ks, const int *__restrict__ band_k, const 
     plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, Jc);
 }
 
+// Small cube grids whose lines fit one lane (single-stage register FFT, a
+// warp holds all N lines of a direction): one warp per band, NW bands of
+// the same z-plane per CTA sharing V(r) and the twiddles; every phase is
+// warp-synchronous.  Lane l owns line l in each pass (y lines are the rows
+// of the sub-plane S, x lines its columns), so no lane reads what another
+// writes within a pass.
+template <int N>
+__global__ void __launch_bounds__(FFT_THREADS)
+mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nbands, int nxa_max,
+                const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
+                float2 *__restrict__ A) {
+    static_assert(pwf::FPlan<N>::nst == 1 && pwf::fp_group<N>() >= N, "one line per lane");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using T = float;
+    constexpr int NW = FFT_THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *ty = tx + N;
+    float *Vs = reinterpret_cast<float *>(ty + N);
+    Cx<T> *wbase = reinterpret_cast<Cx<T> *>(Vs + (N * N + 1) / 2 * 2);
+    const size_t wsz = (size_t)nxa_max * N + (size_t)N * N + (N + 3) / 4;
+    Cx<T> *S = wbase + (size_t)warp * wsz;
+    Cx<T> *Xw = S + (size_t)nxa_max * N;
+    short *iax = reinterpret_cast<short *>(Xw + N * N);
+    const int kz = blockIdx.x;
+    for (int i = threadIdx.x; i < N * N; i += FFT_THREADS) Vs[i] = Vr[(size_t)kz * N * N + i];
+    for (int i = threadIdx.x; i < N; i += FFT_THREADS) {
+        tx[i] = twx[i];
+        ty[i] = twy[i];
+    }
+    __syncthreads();
+    const int gb = blockIdx.y * NW + warp;
+    if (gb >= nbands) return;
+    const MkK &K = ks[band_k[gb]];
+    const KPlan kp = K.kp;
+    const int Nxa = kp.Nxa, Ncol = kp.Ncol;
+    Cx<T> *Ap = A + K.a_off + ((size_t)(gb - K.band0) * N + kz) * Ncol;
+    for (int x = lane; x < N; x += 32) iax[x] = -1;
+    for (int i = lane; i < Nxa * N; i += 32) S[i] = cmake((T)0, (T)0);
+    __syncwarp();
+    for (int i = lane; i < Nxa; i += 32) iax[kp.xa[i]] = (short)i;
+    for (int c = lane; c < Ncol; c += 32) S[kp.col_ia[c] * N + kp.col_j[c]] = Ap[c];
+    __syncwarp();
+    auto ld_row = [&](int line, int x) { return S[line * N + x]; };
+    auto st_row = [&](int line, int x, Cx<T> v) { S[line * N + x] = v; };
+    pwf::group_fft<T, N>(Xw, Nxa, ty, +1, lane, ld_row, st_row);
+    __syncwarp();
+    auto ld_s = [&](int line, int x) {
+        const int ia = iax[x];
+        return ia >= 0 ? S[ia * N + line] : cmake((T)0, (T)0);
+    };
+    auto st_v = [&](int line, int x, Cx<T> v) { Xw[line * N + x] = cscale(v, Vs[line * N + x]); };
+    auto ld_x = [&](int line, int x) { return Xw[line * N + x]; };
+    auto st_s = [&](int line, int x, Cx<T> v) {
+        const int ia = iax[x];
+        if (ia >= 0) S[ia * N + line] = v;
+    };
+    pwf::group_fft<T, N>(Xw, N, tx, +1, lane, ld_s, st_v);
+    __syncwarp();
+    pwf::group_fft<T, N>(Xw, N, tx, -1, lane, ld_x, st_s);
+    __syncwarp();
+    pwf::group_fft<T, N>(Xw, Nxa, ty, -1, lane, ld_row, st_row);
+    __syncwarp();
+    for (int c = lane; c < Ncol; c += 32) Ap[c] = S[kp.col_ia[c] * N + kp.col_j[c]];
+}
+
 // op_V_Ps_nloc for small projector sets, one CTA per band of the batch:
 // P = betaNL' psi (FP64 sums, one warp per projector), P2 = D P (the
 // (ibeta, jbeta, h) list as CSR), Hpsi += betaNL P2
@@ -639,12 +705,23 @@ mk_vnl(const MkK *__restrict__ ks, const int *__restrict__ band_k, const int *__
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int j = warp; j < nbeta; j += nw) {
         const Cx<T> *bj = beta + (size_t)j * ngw;
-        double re = 0.0, im = 0.0;
-        for (int g = lane; g < ngw; g += 32) {
-            const Cx<T> u = bj[g], v = ps[g];
-            re += (double)u.x * v.x + (double)u.y * v.y;
-            im += (double)u.x * v.y - (double)u.y * v.x;
+        // four independent partial sums per lane (latency, not bandwidth, bounds this loop)
+        double r4[4] = {0.0, 0.0, 0.0, 0.0}, i4[4] = {0.0, 0.0, 0.0, 0.0};
+        int g = lane;
+        for (; g + 96 < ngw; g += 128) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const Cx<T> u = bj[g + 32 * t], v = ps[g + 32 * t];
+                r4[t] += (double)u.x * v.x + (double)u.y * v.y;
+                i4[t] += (double)u.x * v.y - (double)u.y * v.x;
+            }
         }
+        for (; g < ngw; g += 32) {
+            const Cx<T> u = bj[g], v = ps[g];
+            r4[0] += (double)u.x * v.x + (double)u.y * v.y;
+            i4[0] += (double)u.x * v.y - (double)u.y * v.x;
+        }
+        double re = (r4[0] + r4[1]) + (r4[2] + r4[3]), im = (i4[0] + i4[1]) + (i4[2] + i4[3]);
         for (int o = 16; o > 0; o >>= 1) {
             re += __shfl_xor_sync(0xffffffffu, re, o);
             im += __shfl_xor_sync(0xffffffffu, im, o);
@@ -662,15 +739,24 @@ mk_vnl(const MkK *__restrict__ ks, const int *__restrict__ band_k, const int *__
     }
     __syncthreads();
     for (int g = threadIdx.x; g < ngw; g += blockDim.x) {
-        double re = 0.0, im = 0.0;
-        for (int i = 0; i < nbeta; ++i) {
+        double re0 = 0.0, im0 = 0.0, re1 = 0.0, im1 = 0.0;
+        int i = 0;
+        for (; i + 1 < nbeta; i += 2) {
+            const Cx<T> u = beta[(size_t)i * ngw + g], w = beta[(size_t)(i + 1) * ngw + g];
+            const double2 q = P2[i], r = P2[i + 1];
+            re0 += (double)u.x * q.x - (double)u.y * q.y;
+            im0 += (double)u.x * q.y + (double)u.y * q.x;
+            re1 += (double)w.x * r.x - (double)w.y * r.y;
+            im1 += (double)w.x * r.y + (double)w.y * r.x;
+        }
+        if (i < nbeta) {
             const Cx<T> u = beta[(size_t)i * ngw + g];
             const double2 q = P2[i];
-            re += (double)u.x * q.x - (double)u.y * q.y;
-            im += (double)u.x * q.y + (double)u.y * q.x;
+            re0 += (double)u.x * q.x - (double)u.y * q.y;
+            im0 += (double)u.x * q.y + (double)u.y * q.x;
         }
         const Cx<T> h = hs[g];
-        hs[g] = cmake((T)(h.x + re), (T)(h.y + im));
+        hs[g] = cmake((T)(h.x + (re0 + re1)), (T)(h.y + (im0 + im1)));
     }
 }
 
@@ -784,9 +870,9 @@ static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb,
 // active x (sizes the plane pass's shared memory); max_ncol sizes the z
 // grids.  flags as kf_zfwd (2: + op_K, 4: accumulate).
 template <typename T>
-cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, int nbands, int max_ncol,
-                          const void *Vr, void *A, int flags, const int *Drow, const int *Dcol, const double *Dval,
-                          int nbeta, cudaStream_t st) {
+cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, int nk, int nbands, int max_nb,
+                          int max_ncol, const void *Vr, void *A, int flags, const int *Drow, const int *Dcol,
+                          const double *Dval, int nbeta, cudaStream_t st) {
     const KPlan &kp = L.kp;
     if (kp.N1 != kp.N2 || kp.N2 != kp.N3) return cudaErrorNotSupported;
     const int Cg = L.Cg;
@@ -798,7 +884,14 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
         if ((e = set_smem<T>((const void *)mk_zinv<T, NN>, zsm)) != cudaSuccess) return e;                          \
         mk_zinv<T, NN><<<zgrid, FFT_THREADS, zsm, st>>>(ks, band_k, (const Cx<T> *)L.twz, (Cx<T> *)A, Cg);           \
         if ((e = cudaGetLastError()) != cudaSuccess) return e;                                                       \
-        if constexpr (sizeof(T) == 4) {                                                                              \
+        if constexpr (sizeof(T) == 4 && pwf::FPlan<NN>::nst == 1 && pwf::fp_group<NN>() >= NN) {                    \
+            const size_t psm = (2 * NN + (NN * NN + 1) / 2) * sizeof(float2) +                                       \
+                               (FFT_THREADS / 32) * ((size_t)kp.Nxa * NN + NN * NN + (NN + 3) / 4) * sizeof(float2); \
+            if ((e = set_smem<float>((const void *)mk_plane_vloc_w<NN>, psm)) != cudaSuccess) return e;             \
+            mk_plane_vloc_w<NN><<<dim3(NN, (nbands + FFT_THREADS / 32 - 1) / (FFT_THREADS / 32)), FFT_THREADS, psm,  \
+                                  st>>>(ks, band_k, nbands, kp.Nxa, (const float2 *)L.twx, (const float2 *)L.twy,   \
+                                        (const float *)Vr, (float2 *)A);                                             \
+        } else if constexpr (sizeof(T) == 4) {                                                                       \
             constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
             const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};           \
             const size_t psm = ps.elems() * sizeof(float2);                                                          \
@@ -930,8 +1023,9 @@ cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t st) {
     template cudaError_t launch_zfwd<T>(const FftLaunch &, const void *, const void *, void *, int64_t, int, int,  \
                                         cudaStream_t);                                                               \
     template cudaError_t launch_plane_vloc<T>(const FftLaunch &, const void *, void *, int, cudaStream_t);          \
-    template cudaError_t launch_multik<T>(const FftLaunch &, const MkK *, const int *, int, int, const void *, void *,  \
-                                          int, const int *, const int *, const double *, int, cudaStream_t);         \
+    template cudaError_t launch_multik<T>(const FftLaunch &, const MkK *, const int *, int, int, int, int,           \
+                                          const void *, void *, int, const int *, const int *, const double *, int,  \
+                                          cudaStream_t);                                                             \
     template cudaError_t launch_plane_rho<T>(const FftLaunch &, const void *, int, int, int, const double *, void *, \
                                              cudaStream_t);                                                          \
     template cudaError_t launch_rho_reduce<T>(const void *, int, size_t, double *, int, cudaStream_t);              \

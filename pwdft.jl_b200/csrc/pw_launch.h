@@ -41,9 +41,9 @@ cudaError_t launch_zfwd(const FftLaunch &, const void *A, const void *psi, void 
                         cudaStream_t);
 template <typename T> cudaError_t launch_plane_vloc(const FftLaunch &, const void *Vr, void *A, int nb, cudaStream_t);
 template <typename T>
-cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, int nbands, int max_ncol, const void *Vr,
-                          void *A, int flags, const int *Drow, const int *Dcol, const double *Dval, int nbeta,
-                          cudaStream_t st);
+cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, int nk, int nbands, int max_nb,
+                          int max_ncol, const void *Vr, void *A, int flags, const int *Drow, const int *Dcol,
+                          const double *Dval, int nbeta, cudaStream_t st);
 template <typename T>
 cudaError_t launch_plane_rho(const FftLaunch &, const void *A, int nb, int G, int Bg, const double *w, void *rho_part,
                              cudaStream_t);
