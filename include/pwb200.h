@@ -213,6 +213,20 @@ int pw_set_density_sphere(pw_ctx *ctx, int64_t Ng, const int64_t *idx_g2r,
 #define PW_XC_VWN 0
 #define PW_XC_PBE 1
 int pw_set_xc(pw_ctx *ctx, int xc, const double *G);
+/* RhoeSymmetrizer (RhoeSymmetrizer.jl:14-110) for symmetrize_rhoe!: the
+ * orbits of the density sphere under the crystal's rotations, each given
+ * as nsym entries (host): isg (nshell x nsym, 0-based sphere index of
+ * inv_s g0 for each operation, g0 the orbit's first member) and phase
+ * (nshell x nsym x 2: cos, sin of G_isg . ft_cartesian; 1, 0 for
+ * symmorphic operations), in the reference's operation order. */
+int pw_set_symmetry(pw_ctx *ctx, int nshell, int nsym, const int32_t *isg,
+                    const double *phase);
+/* symmetrize_rhoe! (RhoeSymmetrizer.jl:114-236), one spin channel, in
+ * place on the device density rhoe (N): each orbit's rho(G) averaged with
+ * the fractional-translation phases; grid components outside the density
+ * sphere are kept. */
+int pw_symmetrize_rhoe(pw_ctx *ctx, double *rhoe);
+
 /* Poisson_solve! (Poisson_solve.jl:22-40): V_H(r) from rho(r), device FP64
  * arrays of N points. */
 int pw_poisson(pw_ctx *ctx, const double *rho, double *VH);

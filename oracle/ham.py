@@ -206,7 +206,7 @@ class Hamiltonian:
     Hamiltonian.jl:270-277)."""
 
     def __init__(self, atoms, pspfiles, ecutwfc, meshk=(1, 1, 1), extra_states=None,
-                 Nstates=None, kpoints=None, Ns=None, xcfunc="VWN"):
+                 Nstates=None, kpoints=None, Ns=None, xcfunc="VWN", use_symmetry=False):
         if xcfunc not in ("VWN", "PBE"):
             raise ValueError("xcfunc must be 'VWN' or 'PBE'")
         self.xcfunc = xcfunc
@@ -215,12 +215,24 @@ class Hamiltonian:
         for isp, s in enumerate(atoms.SpeciesSymbols):
             if self.pspots[isp].atsymb != s:
                 raise ValueError("pseudopotential order does not match species")
+        self.sym = None
+        if use_symmetry:
+            # Hamiltonian.jl:53-85: SymmetryInfo(atoms), k-points reduced by its rotations
+            from .symmetry import SymmetryInfo, gen_kpoint_grid as gen_sym_grid
+            from .pwgrid import KPoints, recvecs_of
+            self.sym = SymmetryInfo(atoms.LatVecs, atoms.positions, atoms.atm2species)
+            if kpoints is None:
+                nk, xk, wk, _ = gen_sym_grid(atoms.LatVecs, meshk, self.sym.s)
+                kpoints = KPoints(nk, tuple(meshk), xk, wk, recvecs_of(atoms.LatVecs))
         if kpoints is None:
             if tuple(meshk) == (1, 1, 1):
                 kpoints = None
             else:
                 kpoints = gen_kpoint_grid(atoms.LatVecs, meshk)
         self.pw = pw = PWGrid(ecutwfc, atoms.LatVecs, kpoints=kpoints, Ns=Ns)
+        if self.sym is not None and self.sym.Nsyms > 1:
+            from .symmetry import RhoeSymmetrizer
+            self.symz = RhoeSymmetrizer(atoms.LatVecs, pw.gvec.G, self.sym)
         self.Zvals = np.array([float(p.zval) for p in self.pspots])
         N = pw.Npoints
         # local pseudopotential: Hamiltonian.jl:113-141

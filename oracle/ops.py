@@ -76,7 +76,8 @@ def Kprec(Ham, psi, ik=None):
 
 
 def calc_rhoe(Ham, psiks, Focc=None, chunk=32):
-    """calc_rhoe.jl:9-135 (Nspin = 1, no dual grid, no symmetrisation)."""
+    """calc_rhoe.jl:9-135 (Nspin = 1, no dual grid); symmetrize_rhoe! at the
+    end when the Hamiltonian was built with symmetry (calc_rhoe.jl:129-132)."""
     pw = Ham.pw
     Focc = Ham.Focc if Focc is None else Focc
     N = pw.Npoints
@@ -93,6 +94,10 @@ def calc_rhoe(Ham, psiks, Focc=None, chunk=32):
             ctmp = G_to_R(pw.Ns, ctmp) * scale
             w = pw.kpoints.wk[ik] * Focc[b0:b1, ik]
             rho += (w[:, None] * (ctmp.real ** 2 + ctmp.imag ** 2)).sum(axis=0)
+    sym = getattr(Ham, "sym", None)
+    if sym is not None and sym.Nsyms > 1:
+        from .symmetry import symmetrize_rhoe
+        rho = symmetrize_rhoe(pw, sym, Ham.symz, rho)
     return rho
 
 

@@ -103,6 +103,11 @@ struct pw_ctx {
     double *d_xcG = nullptr;
     // batched op_H over k-points: device tables (MkK per k-point, band ->
     // k-point map), and the CUDA graph of the last call made with PW_GRAPH
+    // symmetrize_rhoe!: orbits of the density sphere (nshell x nsym sphere
+    // indices and phases e^{i G.ft})
+    int *d_sym_isg = nullptr;
+    double2 *d_sym_ph = nullptr;
+    int sym_nshell = 0, sym_nsym = 0;
     DevBuf mk_tab;
     uint64_t mk_key = 0;
     cudaGraphExec_t mk_exec = nullptr;
@@ -1076,6 +1081,33 @@ extern "C" int pw_set_xc(pw_ctx *c, int xc, const double *G) {
     }
     c->xc = xc;
     return PW_OK;
+}
+extern "C" int pw_set_symmetry(pw_ctx *c, int nshell, int nsym, const int32_t *isg, const double *phase) {
+    if (!c) return PW_ERR_ARG;
+    if (!c->have_dens) return fail(c, PW_ERR_STATE, "call pw_set_density_sphere before pw_set_symmetry");
+    if (nshell <= 0 || nsym <= 0 || !isg || !phase) return fail(c, PW_ERR_ARG, "bad symmetry tables");
+    const size_t n = (size_t)nshell * nsym;
+    for (size_t i = 0; i < n; ++i)
+        if (isg[i] < 0 || isg[i] >= c->dens.Ngw) return fail(c, PW_ERR_ARG, "symmetry table index %d outside the sphere", isg[i]);
+    CK(c, cudaSetDevice(c->device));
+    dfree(c, c->d_sym_isg);
+    dfree(c, c->d_sym_ph);
+    c->d_sym_isg = nullptr;
+    c->d_sym_ph = nullptr;
+    int s;
+    if ((s = dalloc(c, &c->d_sym_isg, n)) || (s = dalloc(c, &c->d_sym_ph, n))) return s;
+    CK(c, cudaMemcpy(c->d_sym_isg, isg, n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(c, cudaMemcpy(c->d_sym_ph, phase, n * sizeof(double2), cudaMemcpyHostToDevice));
+    c->sym_nshell = nshell;
+    c->sym_nsym = nsym;
+    return PW_OK;
+}
+int pwk_symmetry(const pw_ctx *c, const int **isg, const double2 **ph, int *nshell, int *nsym) {
+    *isg = c->d_sym_isg;
+    *ph = c->d_sym_ph;
+    *nshell = c->sym_nshell;
+    *nsym = c->sym_nsym;
+    return c->d_sym_isg ? PW_OK : PW_ERR_STATE;
 }
 int pwk_xc(const pw_ctx *c, const double **G) {
     *G = c->d_xcG;

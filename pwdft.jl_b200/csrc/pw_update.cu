@@ -36,6 +36,7 @@ int pwk_projections(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, i
 int pwk_ngw(const pw_ctx *c, int ik);
 const double *pwk_gk2(const pw_ctx *c, int ik);
 int pwk_xc(const pw_ctx *c, const double **G);
+int pwk_symmetry(const pw_ctx *c, const int **isg, const double2 **ph, int *nshell, int *nsym);
 
 namespace pwk {
 namespace upd {
@@ -260,6 +261,33 @@ __global__ void k_pbe_point(const double *__restrict__ rho, double *__restrict__
         gz[i] = v2 * c;
     }
 }
+// symmetrize_rhoe! (RhoeSymmetrizer.jl:153-228), one thread per orbit of
+// the density sphere: rhosum = (1/nsym) sum_s rho(isg_s) conj(ph_s), then
+// rho(isg_s) := rhosum ph_s in operation order (a later operation that hits
+// the same G wins, as in the reference); written as the change delta(G).
+__global__ void k_sym_orbits(const double2 *__restrict__ rhoG, const int *__restrict__ isg,
+                             const double2 *__restrict__ ph, int nshell, int nsym, double2 *__restrict__ delta) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nshell) return;
+    const int *ix = isg + (size_t)o * nsym;
+    const double2 *p = ph + (size_t)o * nsym;
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < nsym; ++s) {
+        const double2 r = rhoG[ix[s]], q = p[s];
+        re += r.x * q.x + r.y * q.y;
+        im += r.y * q.x - r.x * q.y;
+    }
+    re /= nsym;
+    im /= nsym;
+    for (int s = 0; s < nsym; ++s) {
+        const double2 r = rhoG[ix[s]], q = p[s];
+        delta[ix[s]] = make_double2(re * q.x - im * q.y - r.x, re * q.y + im * q.x - r.y);
+    }
+}
+__global__ void k_add(double *__restrict__ y, const double *__restrict__ x, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) y[i] += x[i];
+}
+
 // V_xc -= div h; V_tot = V_ps + V_H + V_xc
 __global__ void k_pbe_vtot(double *__restrict__ Vxc, const double *__restrict__ dh, const double *__restrict__ Vps,
                            const double *__restrict__ VH, double *__restrict__ Vtot, size_t N) {
@@ -467,6 +495,34 @@ static int pbe(pw_ctx *c, const double *rho, const double *G, double *Vxc, doubl
         pwk_count_launches(c, 1);
     }
     RK(sphere_to_R(c, L, div, Ng, N, grad));   // div h(r) over h_x, no longer needed
+    return PW_OK;
+}
+
+extern "C" int pw_symmetrize_rhoe(pw_ctx *c, double *rho) {
+    if (!c) return PW_ERR_ARG;
+    if (!rho) return pwk_fail(c, PW_ERR_ARG, "NULL density");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    const int *isg = nullptr;
+    const double2 *ph = nullptr;
+    int nshell = 0, nsym = 0;
+    if (pwk_symmetry(c, &isg, &ph, &nshell, &nsym) != PW_OK)
+        return pwk_fail(c, PW_ERR_STATE, "symmetry tables are not set (pw_set_symmetry)");
+    FftLaunch L;
+    double2 *g = nullptr, *A = nullptr, *delta = nullptr;
+    int Ng = 0;
+    size_t N = 0;
+    const double *G2 = nullptr;
+    RK(density_to_G(c, rho, L, &g, &A, &Ng, &N, &G2));
+    cudaStream_t st = pwk_stream(c);
+    double *tmp = nullptr;
+    RK(pwk_scratch(c, SL_UPD_DIVG, (size_t)Ng * sizeof(double2), (void **)&delta));
+    RK(pwk_scratch(c, SL_UPD_GRAD, N * sizeof(double), (void **)&tmp));
+    k_sym_orbits<<<(nshell + 127) / 128, 128, 0, st>>>(g, isg, ph, nshell, nsym, delta);
+    CKU(c, cudaGetLastError());
+    RK(sphere_to_R(c, L, delta, Ng, N, tmp));
+    k_add<<<RED_BLOCKS, 256, 0, st>>>(rho, tmp, N);
+    CKU(c, cudaGetLastError());
+    pwk_count_launches(c, 2);
     return PW_OK;
 }
 

@@ -277,6 +277,20 @@ class Context:
         self._keep_xc = g
         self._chk(self._L.pw_set_xc(self.h, int(xc), None if g is None else _dptr(g)))
 
+    def set_symmetry(self, isg, phase):
+        """RhoeSymmetrizer tables: isg (nshell, nsym) sphere indices, phase
+        (nshell, nsym, 2) cos/sin of G.ft."""
+        i = np.ascontiguousarray(np.asarray(isg, dtype=np.int32))
+        p = np.ascontiguousarray(np.asarray(phase, dtype=np.float64))
+        self._keep_sym = (i, p)
+        self._chk(self._L.pw_set_symmetry(self.h, i.shape[0], i.shape[1], i.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          _dptr(p)))
+
+    def symmetrize_rhoe(self, rho):
+        """symmetrize_rhoe!: the device density rho (N, FP64) in place."""
+        self.use_torch_stream()
+        self._chk(self._L.pw_symmetrize_rhoe(self.h, C.c_void_p(rho.data_ptr())))
+
     def set_force_tables(self, VlocG, G):
         """VlocG (Ng, nspecies): eval_Vloc_G per species on the density sphere
         (no 1/Omega); G (Ng, 3) of that sphere, in its order."""

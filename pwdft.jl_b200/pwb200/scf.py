@@ -7,6 +7,7 @@ density mixing):
   diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson";
                            the call of electrons_scf.jl:150)
   calc_rhoe!               pw_calc_rhoe                   (device)
+  symmetrize_rhoe!         pw_symmetrize_rhoe             (device, Hamiltonians built with symmetry)
   mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
   smearing (use_smearing)  KS_solve_SCF.jl:218-223, occupations.jl:6-245  (host: Fermi level
                            by bisection over the Nstates x Nkpt eigenvalues, -TS)
@@ -195,6 +196,8 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         t1 = time.perf_counter()
         for ik in range(b.Nkpt):
             ctx.calc_rhoe(ik, psiks[ik], wk[ik] * Focc[:, ik], rho_new, accumulate=(ik > 0))
+        if Ham.sym is not None:
+            ctx.symmetrize_rhoe(rho_new)
         diffRhoe = float(torch.sum(torch.abs(rho_new - rho)).item()) / N
         torch.cuda.synchronize()
         t2 = time.perf_counter()

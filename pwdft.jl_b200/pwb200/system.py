@@ -330,11 +330,27 @@ class Hamiltonian:
     (ik, ispin) state of the reference (Hamiltonian.jl: Ham.ik, Ham.ispin)."""
 
     def __init__(self, system, pspfiles, ecutwfc, kpts=None, wk=None, device=0, Ns=None, V_loc=None,
-                 xcfunc="VWN"):
+                 xcfunc="VWN", meshk=None, use_symmetry=False):
+        """kpts (3, Nk) Cartesian with weights wk, or meshk: a Gamma-centred
+        Monkhorst-Pack mesh reduced by k ~ -k and, with use_symmetry, by the
+        crystal's rotations (Hamiltonian.jl:53-85); symmetry also makes
+        calc_rhoe symmetrise the density (calc_rhoe.jl:129-132)."""
         if xcfunc not in ("VWN", "PBE"):
             raise ValueError("xcfunc must be 'VWN' or 'PBE'")
         self.xcfunc = xcfunc
         self.system = system
+        self.sym = None
+        if use_symmetry:
+            from .symmetry import crystal_symmetry
+            s, ft = crystal_symmetry(system.LatVecs, system.positions, system.atm2species)
+            if s.shape[2] > 1:
+                self.sym = (s, ft)
+        if meshk is not None and kpts is None:
+            if self.sym is not None:
+                from .symmetry import kpoint_grid_sym
+                kpts, wk = kpoint_grid_sym(system.LatVecs, meshk, self.sym[0])
+            else:
+                kpts, wk = kpoint_grid(system.LatVecs, meshk)
         self.pspots = [GTH(f) for f in pspfiles]
         self.basis = b = Basis(system.LatVecs, ecutwfc, kpts=kpts, Ns=Ns)
         self.wk = np.ones(b.Nkpt) / b.Nkpt if wk is None else np.asarray(wk, dtype=np.float64)
@@ -367,6 +383,10 @@ class Hamiltonian:
         if self.xcfunc == "PBE":
             from ._lib import PW_XC_PBE
             self.ctx.set_xc(PW_XC_PBE, b.G)
+        if self.sym is not None:
+            from .symmetry import symmetrizer_tables
+            isg, ph = symmetrizer_tables(self.system.LatVecs, b.G, *self.sym)
+            self.ctx.set_symmetry(isg, ph)
         self._density_set = True
 
     def update_vloc(self, V):
