@@ -126,5 +126,11 @@ def calc_forces_NN(Ham):
 
 
 def calc_forces(Ham, psiks, Rhoe):
-    """calc_forces.jl:1-17 for GTH without symmetry: F_NN + F_Ps_loc + F_Ps_nloc."""
-    return calc_forces_NN(Ham) + calc_forces_Ps_loc(Ham, Rhoe) + calc_forces_Ps_nloc(Ham, psiks)
+    """calc_forces.jl:1-17 for GTH: F_NN + F_Ps_loc + F_Ps_nloc, the nonlocal
+    part symmetrised when the Hamiltonian uses symmetry (calc_forces.jl:11)."""
+    F_nl = calc_forces_Ps_nloc(Ham, psiks)
+    sym = getattr(Ham, "sym", None)
+    if sym is not None and sym.Nsyms > 1:
+        from .symmetry import symmetrize_vector
+        F_nl = symmetrize_vector(Ham.atoms.LatVecs, sym, F_nl)
+    return calc_forces_NN(Ham) + calc_forces_Ps_loc(Ham, Rhoe) + F_nl

@@ -7,7 +7,8 @@ Quantum ESPRESSO's symm_base):
                                                     fractional translations
   checksym! / eqvect       SymmetryInfo.jl:501-556
   copy_sym!                SymmetryInfo.jl:562-611
-  SymmetryInfo(atoms)      SymmetryInfo.jl:711-784  (Nsyms, s, inv_s, ft, non_symmorphic)
+  SymmetryInfo(atoms)      SymmetryInfo.jl:711-784  (Nsyms, s, inv_s, ft, non_symmorphic, irt)
+  symmetrize_vector!       SymmetryInfo.jl:923-966  (forces)
   gen_kpoint_grid          KPoints.jl:121-261       with the crystal's rotations
   RhoeSymmetrizer          RhoeSymmetrizer.jl:14-110  G-vector orbits
   symmetrize_rhoe!         RhoeSymmetrizer.jl:114-236
@@ -113,14 +114,31 @@ class SymmetryInfo:
 
     def __init__(self, LatVecs, positions, ityp):
         s_all = lattice_point_group(LatVecs)
-        sym, ft_all, _ = sgam_at(LatVecs, positions, ityp, s_all)
+        sym, ft_all, irt = sgam_at(LatVecs, positions, ityp, s_all)
         keep = [i for i in range(s_all.shape[2]) if sym[i]]        # copy_sym!: kept ones first, in order
         self.Nsyms = len(keep)
         self.s = s_all[:, :, keep]
         self.ft = ft_all[:, keep]
+        self.irt = irt[keep]
         self.inv_s = np.stack([np.round(np.linalg.inv(self.s[:, :, i])).astype(np.int64)
                                for i in range(self.Nsyms)], axis=2)
         self.non_symmorphic = np.abs(self.ft).max(axis=0) >= 1e-10
+
+
+def symmetrize_vector(LatVecs, sym, v):
+    """SymmetryInfo.jl:923-966: v (3, Natoms) Cartesian, averaged over the
+    operations (atom ia takes s applied to its image irt[isym, ia])."""
+    if sym.Nsyms == 1:
+        return v.copy()
+    L = np.asarray(LatVecs, dtype=np.float64)
+    L = L / np.linalg.norm(L[:, 0])
+    R = np.linalg.inv(L.T)
+    tmp = L.T @ v
+    out = np.zeros_like(v)
+    for i in range(v.shape[1]):
+        for isym in range(sym.Nsyms):
+            out[:, i] += sym.s[:, :, isym].astype(np.float64) @ tmp[:, sym.irt[isym, i]]
+    return R @ (out / sym.Nsyms)
 
 
 def gen_kpoint_grid(LatVecs, nk, s, shift=(0, 0, 0), time_reversal=True):

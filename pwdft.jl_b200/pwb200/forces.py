@@ -5,6 +5,8 @@ without symmetry, NLCC or SCF correction.
   F_Ps_loc    calc_forces_Ps_loc.jl:13-71        device (pw_forces_local)
   F_Ps_nloc   calc_forces_Ps_nloc.jl:291-411     device (pw_forces_nonlocal, per k-point)
   F_NN        calc_forces_NN.jl:1-142            host (Ewald sum, set-up arithmetic)
+With symmetry the nonlocal part is averaged over the crystal's operations
+(calc_forces.jl:11, symmetrize_vector!), as the reference does.
 """
 import numpy as np
 from scipy.special import erfc
@@ -83,6 +85,10 @@ def calc_forces(Ham, psiks, rho, Focc, parts=False):
     if Ham.NbetaNL > 0:
         for ik in range(b.Nkpt):
             F_nl += Ham.ctx.forces_nonlocal(ik, psiks[ik], Ham.wk[ik] * Focc[:, ik])
+    if getattr(Ham, "sym", None) is not None:
+        from .symmetry import atom_map, symmetrize_vectors
+        s, ft = Ham.sym
+        F_nl = symmetrize_vectors(b.LatVecs, s, atom_map(b.LatVecs, sysm.positions, sysm.atm2species, s, ft), F_nl)
     F = F_nn + F_loc + F_nl
     if parts:
         return F, {"NN": F_nn, "Ps_loc": F_loc, "Ps_nloc": F_nl}

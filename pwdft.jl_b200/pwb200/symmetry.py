@@ -87,6 +87,28 @@ def crystal_symmetry(LatVecs, positions, ityp):
     return np.stack(S, axis=2), np.stack(F, axis=1)
 
 
+def atom_map(LatVecs, positions, ityp, s, ft):
+    """irt (nsym, nat): the like atom each atom lands on under x -> s^T x - ft."""
+    ityp = np.asarray(ityp)
+    xa = np.linalg.inv(np.asarray(LatVecs, dtype=np.float64)) @ np.asarray(positions, dtype=np.float64)
+    irt = np.zeros((s.shape[2], xa.shape[1]), dtype=np.int64)
+    for i in range(s.shape[2]):
+        d = (s[:, :, i].T @ xa)[:, :, None] - xa[:, None, :] - ft[:, i][:, None, None]
+        ok = np.all(np.abs(d - np.round(d)) < 1e-5, axis=0) & (ityp[:, None] == ityp[None, :])
+        irt[i] = np.argmax(ok, axis=1)
+    return irt
+
+
+def symmetrize_vectors(LatVecs, s, irt, v):
+    """symmetrize_vector! (SymmetryInfo.jl:923-966): per-atom Cartesian
+    vectors v (3, nat) averaged over the operations, in crystal axes."""
+    L = np.asarray(LatVecs, dtype=np.float64)
+    L = L / np.linalg.norm(L[:, 0])
+    t = L.T @ v
+    acc = np.einsum("ijs,jsa->ia", s.astype(np.float64), t[:, irt])
+    return np.linalg.inv(L.T) @ (acc / s.shape[2])
+
+
 def kpoint_grid_sym(LatVecs, mesh, s, time_reversal=True):
     """Gamma-centred mesh reduced by the rotations s and k ~ -k (each class
     represented by its first mesh point, weight = class size); Cartesian k

@@ -134,3 +134,48 @@ def test_device_scf_si_fcc_with_symmetry(precision):
         assert abs(res["energies"]["Total"] - r2["energies"]["Total"]) < 2e-7
         H2.ctx.close()
     H.ctx.close()
+
+
+def test_host_vector_symmetrisation_matches_oracle():
+    from oracle import systems, symmetry
+    from pwb200 import symmetry as ps
+    at = systems.si_fcc_atoms()
+    pos = at.positions.copy()
+    pos[:, 1] += 0.03                     # along (1,1,1): C3v, 6 operations
+    o = symmetry.SymmetryInfo(at.LatVecs, pos, at.atm2species)
+    assert o.Nsyms == 6
+    s, ft = ps.crystal_symmetry(at.LatVecs, pos, at.atm2species)
+    irt = ps.atom_map(at.LatVecs, pos, at.atm2species, s, ft)
+    assert np.array_equal(irt, o.irt)
+    v = np.random.default_rng(1).standard_normal((3, 2))
+    ref = symmetry.symmetrize_vector(at.LatVecs, o, v)
+    got = ps.symmetrize_vectors(at.LatVecs, s, irt, v)
+    assert np.abs(got - ref).max() < 1e-14
+    assert np.abs(ref[:, 0] - ref[0, 0]).max() < 1e-14       # along (1,1,1)
+
+
+@pytest.mark.gpu
+def test_device_forces_with_symmetry_match_full_mesh():
+    """Si fcc with the second atom moved along (1,1,1) (6 operations): the
+    forces from the symmetry-reduced SCF (symmetrised density and nonlocal
+    force) equal those of the time-reversal-only mesh."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import pwb200
+    from pwb200 import scf, forces
+    from oracle import systems
+    at = systems.si_fcc_atoms()
+    pos = at.positions.copy()
+    pos[:, 1] += 0.03
+    out = []
+    for use_sym in (True, False):
+        H = pwb200.Hamiltonian(pwb200.System(["Si", "Si"], pos, at.LatVecs), [systems.psp("Si-q4.gth")], 15.0,
+                               meshk=(3, 3, 3), use_symmetry=use_sym)
+        res = scf.KS_solve_SCF(H, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-11, ethr_evals_last=1e-11)
+        out.append((H.basis.Nkpt, res["energies"]["Total"], forces.calc_forces(H, res["psiks"], res["rho"], res["Focc"])))
+        H.ctx.close()
+    (n1, e1, f1), (n2, e2, f2) = out
+    assert n1 < n2
+    assert abs(e1 - e2) < 1e-9
+    assert np.abs(f1 - f2).max() < 1e-7, (f1, f2)
+    assert np.abs(f1[:, 1]).max() > 1e-3
