@@ -95,6 +95,18 @@ int pw_set_vloc_device(pw_ctx *ctx, const double *V_dev, int nspin);
 
 /* betaNL[ik] (PsPotNL.jl:39-69): host ComplexF64 Ngw x nbeta column-major. */
 int pw_set_nonlocal(pw_ctx *ctx, int ik, const double *betaNL, int nbeta);
+/* betaNL[ik] built on the device (PsPotNL.jl:16-77 for GTH: eval_proj_G,
+ * PsPot_GTH.jl:338-391; Ylm_real, Ylm_real.jl:5-107; e^{-i(G+k).tau}) from
+ * the G+k vectors of pw_set_gkvec and a host table of nbeta columns in the
+ * reference's (atom, l, m, iprj) order: atom (0-based), l <= 3, m in
+ * [-l, l], iproj (1-based radial index), rc = r_l of the atom's species,
+ * pref = 4 pi^(5/4) sqrt(2^(l+1) r_l^(2l+3) / CellVolume); pos (host,
+ * 3 x natoms, bohr).  Replaces pw_set_nonlocal's host array, e.g. after the
+ * atoms moved. */
+int pw_build_nonlocal(pw_ctx *ctx, int ik, int nbeta, const int32_t *atom,
+                      const int32_t *l, const int32_t *m, const int32_t *iproj,
+                      const double *rc, const double *pref, int natoms,
+                      const double *pos);
 /* The (ibeta, jbeta, h_ij) pairs visited by op_V_Ps_nloc.jl:59-76
  * (0-based ibeta/jbeta; duplicates add). */
 int pw_set_nonlocal_coef(pw_ctx *ctx, int nnz, const int32_t *ibeta,

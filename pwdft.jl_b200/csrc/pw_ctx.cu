@@ -620,11 +620,14 @@ static int set_vloc_common(pw_ctx *c, const double *V, int nspin, bool on_device
 extern "C" int pw_set_vloc(pw_ctx *c, const double *V, int nspin) { return set_vloc_common(c, V, nspin, false); }
 extern "C" int pw_set_vloc_device(pw_ctx *c, const double *V, int nspin) { return set_vloc_common(c, V, nspin, true); }
 
-extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta) {
-    if (!c) return PW_ERR_ARG;
+int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out);
+
+namespace {
+// betaNL[ik] of nbeta columns: FP64 storage (allocated once), filled by `fill`
+// on the context stream, then its FP32 copy and the split-BF16 operands
+template <class Fill>
+int set_beta(pw_ctx *c, int ik, int nbeta, Fill fill) {
     int s;
-    if ((s = check_k(c, ik))) return s;
-    if (!beta || nbeta <= 0) return fail(c, PW_ERR_ARG, "empty betaNL");
     if (c->nbeta != 0 && c->nbeta != nbeta) return fail(c, PW_ERR_ARG, "nbeta %d differs from %d", nbeta, c->nbeta);
     CK(c, cudaSetDevice(c->device));
     KData &kd = c->k[ik];
@@ -632,7 +635,7 @@ extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta)
     if (!kd.d_beta64) {
         if ((s = dalloc(c, &kd.d_beta64, n)) || (s = dalloc(c, &kd.d_beta32, n))) return s;
     }
-    CK(c, cudaMemcpyAsync(kd.d_beta64, beta, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+    if ((s = fill(kd.d_beta64))) return s;
     CK(c, convert_c128_to_c64(kd.d_beta64, kd.d_beta32, n, c->stream));
     if (c->use_umma) {
         // split-BF16 copies of betaNL for both tensor-core products, built once
@@ -653,6 +656,51 @@ extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta)
     CK(c, cudaStreamSynchronize(c->stream));
     c->nbeta = nbeta;
     return PW_OK;
+}
+}  // namespace
+
+extern "C" int pw_set_nonlocal(pw_ctx *c, int ik, const double *beta, int nbeta) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik))) return s;
+    if (!beta || nbeta <= 0) return fail(c, PW_ERR_ARG, "empty betaNL");
+    const size_t n = (size_t)c->k[ik].Ngw * nbeta;
+    return set_beta(c, ik, nbeta, [&](double2 *d) {
+        CK(c, cudaMemcpyAsync(d, beta, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+        return (int)PW_OK;
+    });
+}
+
+extern "C" int pw_build_nonlocal(pw_ctx *c, int ik, int nbeta, const int32_t *atom, const int32_t *l, const int32_t *m,
+                                 const int32_t *iproj, const double *rc, const double *pref, int natoms,
+                                 const double *pos) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik))) return s;
+    if (nbeta <= 0 || natoms <= 0 || !atom || !l || !m || !iproj || !rc || !pref || !pos)
+        return fail(c, PW_ERR_ARG, "bad projector table");
+    if (!c->k[ik].d_gk) return fail(c, PW_ERR_STATE, "G+k vectors of k-point %d are not set (pw_set_gkvec)", ik);
+    std::vector<ProjCol> cols(nbeta);
+    for (int j = 0; j < nbeta; ++j) {
+        const bool ok = atom[j] >= 0 && atom[j] < natoms && l[j] >= 0 && l[j] <= 3 && m[j] >= -l[j] && m[j] <= l[j] &&
+                        iproj[j] >= 1 && iproj[j] <= (l[j] == 0 ? 3 : l[j] == 1 ? 3 : l[j] == 2 ? 2 : 1);
+        if (!ok) return fail(c, PW_ERR_ARG, "projector column %d: unsupported (atom, l, m, i)", j);
+        cols[j] = ProjCol{atom[j], l[j], m[j], iproj[j], rc[j], pref[j]};
+    }
+    CK(c, cudaSetDevice(c->device));
+    ProjCol *d_cols = nullptr;
+    double *d_pos = nullptr;
+    if ((s = pwk_scratch(c, SL_FRC_A, nbeta * sizeof(ProjCol), (void **)&d_cols)) ||
+        (s = pwk_scratch(c, SL_FRC_B, 3 * (size_t)natoms * sizeof(double), (void **)&d_pos)))
+        return s;
+    CK(c, cudaMemcpyAsync(d_cols, cols.data(), nbeta * sizeof(ProjCol), cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync(d_pos, pos, 3 * (size_t)natoms * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    const KData &kd = c->k[ik];
+    return set_beta(c, ik, nbeta, [&](double2 *d) {
+        CK(c, launch_build_beta(kd.d_gk, kd.Ngw, d_cols, nbeta, d_pos, d, c->stream));
+        c->launches += 1;
+        return (int)PW_OK;
+    });
 }
 
 extern "C" int pw_set_nonlocal_coef(pw_ctx *c, int nnz, const int32_t *ib, const int32_t *jb, const double *h) {

@@ -40,6 +40,16 @@ template <typename T>
 cudaError_t launch_zfwd(const FftLaunch &, const void *A, const void *psi, void *Hpsi, int64_t ld, int nb, int flags,
                         cudaStream_t);
 template <typename T> cudaError_t launch_plane_vloc(const FftLaunch &, const void *Vr, void *A, int nb, cudaStream_t);
+// One projector column of betaNL (PsPotNL.jl:147-195 order): its atom,
+// angular momentum l, m in [-l, l], radial index i (1-based), r_l and the
+// normalisation of eval_proj_G.
+struct ProjCol {
+    int atom, l, m, i;
+    double rc, pref;
+};
+cudaError_t launch_build_beta(const double *gk, int ngw, const ProjCol *cols, int ncol, const double *pos, double2 *beta,
+                              cudaStream_t st);
+
 template <typename T>
 cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, int nk, int nbands, int max_nb,
                           int max_ncol, const void *Vr, void *A, int flags, const int *Drow, const int *Dcol,

@@ -78,6 +78,7 @@ SIGNATURES = {
     "pw_calc_grad": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _dp, _d]),
     "pw_set_force_tables": (_i, [_vp, _i, _dp, _dp]),
     "pw_set_xc": (_i, [_vp, _i, _dp]),
+    "pw_build_nonlocal": (_i, [_vp, _i, _i, _i32p, _i32p, _i32p, _i32p, _dp, _dp, _i, _dp]),
     "pw_set_symmetry": (_i, [_vp, _i, _i, _i32p, _dp]),
     "pw_symmetrize_rhoe": (_i, [_vp, _vp]),
     "pw_forces_local": (_i, [_vp, _vp, _i, _dp, _i32p, _dp]),

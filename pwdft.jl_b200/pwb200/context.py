@@ -277,6 +277,17 @@ class Context:
         self._keep_xc = g
         self._chk(self._L.pw_set_xc(self.h, int(xc), None if g is None else _dptr(g)))
 
+    def build_nonlocal(self, ik, table, positions):
+        """pw_build_nonlocal: betaNL of k-point ik evaluated on the device
+        from the G+k vectors (set_gkvec first), the column table of
+        system.projector_table and the atom positions (3, natoms)."""
+        t = {k: np.ascontiguousarray(v) for k, v in table.items()}
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float64).T)      # column-major 3 x natoms
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        self._chk(self._L.pw_build_nonlocal(self.h, ik, len(t["l"]), ip(t["atom"]), ip(t["l"]), ip(t["m"]),
+                                            ip(t["iproj"]), _dptr(t["rc"]), _dptr(t["pref"]), pos.shape[0],
+                                            _dptr(pos)))
+
     def set_symmetry(self, isg, phase):
         """RhoeSymmetrizer tables: isg (nshell, nsym) sphere indices, phase
         (nshell, nsym, 2) cos/sin of G.ft."""

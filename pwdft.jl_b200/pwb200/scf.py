@@ -139,7 +139,8 @@ class PulayMixer:
 
 def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
-                 verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3):
+                 verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3,
+                 savewfc=False, wfc_dir="."):
     """Runs the SCF loop; returns a dict with energies, eigenvalues, timings
     and the per-iteration log."""
     import torch
@@ -239,6 +240,10 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             switched_at = it
         Etot_old = E["Total"]
     torch.cuda.synchronize()
+    if savewfc:
+        # KS_solve_SCF_potmix.jl:301-307: WFC_ikspin_<n>.data per (k-point, spin)
+        from .io import write_psiks
+        write_psiks(psiks, wfc_dir)
     return {"energies": E, "evals": evals, "Focc": Focc, "E_fermi": E_fermi, "iterations": len(log), "log": log,
             "time_s": time.perf_counter() - t_start,
             "time_diag_s": t_diag, "time_rhoe_s": t_rho, "time_update_s": t_upd, "switched_to_fp64_at": switched_at,

@@ -205,6 +205,30 @@ def local_potential(system, basis, pspots):
     return V
 
 
+def projector_table(system, basis, pspots):
+    """The column table of betaNL in the reference's (atom, l, m, iprj) order
+    (PsPotNL.jl:147-195) for pw_build_nonlocal: atom, l, m, iproj (1-based),
+    r_l, and eval_proj_G's normalisation 4 pi^(5/4) sqrt(2^(l+1) r_l^(2l+3)
+    / Omega); plus the (ibeta, jbeta, h_ij) list (op_V_Ps_nloc.jl:59-76)."""
+    cols, trip = [], []
+    for ia in range(system.positions.shape[1]):
+        psp = pspots[system.atm2species[ia]]
+        for l in range(psp.lmax + 1):
+            r = psp.rc[l]
+            pref = 4.0 * np.pi ** 1.25 * math.sqrt(2.0 ** (l + 1) * r ** (2 * l + 3) / basis.CellVolume)
+            for m in range(-l, l + 1):
+                first = len(cols)
+                for i in range(psp.Nproj_l[l]):
+                    cols.append((ia, l, m, i + 1, r, pref))
+                for i in range(psp.Nproj_l[l]):
+                    for j in range(psp.Nproj_l[l]):
+                        trip.append((first + i, first + j, psp.h[l, i, j]))
+    t = np.array(cols, dtype=object).reshape(-1, 6) if cols else np.zeros((0, 6), dtype=object)
+    table = {"atom": t[:, 0].astype(np.int32), "l": t[:, 1].astype(np.int32), "m": t[:, 2].astype(np.int32),
+             "iproj": t[:, 3].astype(np.int32), "rc": t[:, 4].astype(np.float64), "pref": t[:, 5].astype(np.float64)}
+    return table, trip
+
+
 def projectors(system, basis, pspots, ik):
     """betaNL[ik] (Ngw, NbetaNL) and the (ibeta, jbeta, h_ij) list
     (PsPotNL.jl:40-69, 147-195; op_V_Ps_nloc.jl:59-76)."""
@@ -330,11 +354,13 @@ class Hamiltonian:
     (ik, ispin) state of the reference (Hamiltonian.jl: Ham.ik, Ham.ispin)."""
 
     def __init__(self, system, pspfiles, ecutwfc, kpts=None, wk=None, device=0, Ns=None, V_loc=None,
-                 xcfunc="VWN", meshk=None, use_symmetry=False):
+                 xcfunc="VWN", meshk=None, use_symmetry=False, device_projectors=False):
         """kpts (3, Nk) Cartesian with weights wk, or meshk: a Gamma-centred
         Monkhorst-Pack mesh reduced by k ~ -k and, with use_symmetry, by the
         crystal's rotations (Hamiltonian.jl:53-85); symmetry also makes
-        calc_rhoe symmetrise the density (calc_rhoe.jl:129-132)."""
+        calc_rhoe symmetrise the density (calc_rhoe.jl:129-132).
+        device_projectors: betaNL evaluated on the device (pw_build_nonlocal)
+        instead of on the host."""
         if xcfunc not in ("VWN", "PBE"):
             raise ValueError("xcfunc must be 'VWN' or 'PBE'")
         self.xcfunc = xcfunc
@@ -359,7 +385,15 @@ class Hamiltonian:
         self.V_Total = self.V_Ps_loc.copy() if V_loc is None else np.asarray(V_loc, dtype=np.float64)
         self.ctx.set_vloc(self.V_Total)
         self.NbetaNL = 0
-        for ik in range(b.Nkpt):
+        if device_projectors:
+            table, trip = projector_table(system, b, self.pspots)
+            if len(trip) > 0:
+                for ik in range(b.Nkpt):
+                    self.ctx.set_gkvec(ik, b.G[b.idx_gw2g[ik]] + b.kpts[:, ik][None, :])
+                    self.ctx.build_nonlocal(ik, table, system.positions)
+                self.NbetaNL = len(table["l"])
+                self.nl_triplets = trip
+        for ik in range(b.Nkpt if not device_projectors else 0):
             beta, trip = projectors(system, b, self.pspots, ik)
             if beta.shape[1] > 0:
                 self.ctx.set_nonlocal(ik, beta)
