@@ -15,6 +15,10 @@ density mixing):
   update!                  pw_update (Poisson, VWN, V_tot) (device)
   calc_energies            pw_update sums + pw_band_energies (device, FP64)
   convergence              |dE| < etot_conv_thr twice      (host scalar)
+With a torch.distributed process group the k-points are shared out over the
+ranks (pwb200.kshard): each rank solves and sums its own, and the density,
+band energies and eigenvalues are all-reduced; psiks then holds this rank's
+blocks only (None elsewhere).
 The starting density (guess_rhoe.jl) and E_NN (Ewald) are computed once on
 the host, as set-up.
 
@@ -86,14 +90,18 @@ def smeared_occupations(Nelectrons, wk, kT, evals):
     return Focc, Ef, mTS
 
 
-def rand_psiks(Ham, Nstates, seed, dtype):
-    """rand_BlochWavefunc (gen_wavefunc.jl:75-92): ortho_sqrt(rand(ComplexF64))."""
+def rand_psiks(Ham, Nstates, seed, dtype, keep=None):
+    """rand_BlochWavefunc (gen_wavefunc.jl:75-92): ortho_sqrt(rand(ComplexF64)),
+    one seeded stream over all k-points; blocks outside `keep` are None."""
     import torch
     rng = np.random.default_rng(seed)
     out = []
     for ik in range(Ham.basis.Nkpt):
         ngw = Ham.basis.Ngw[ik]
         psi = rng.random((ngw, Nstates)) + 1j * rng.random((ngw, Nstates))
+        if keep is not None and ik not in keep:
+            out.append(None)
+            continue
         w, U = np.linalg.eigh(psi.conj().T @ psi)
         psi = psi @ ((U / np.sqrt(w)) @ U.conj().T)
         out.append(torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{Ham.ctx.device}").to(dtype).contiguous())
@@ -159,10 +167,15 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         raise ValueError("update_psi must be 'LOBPCG' or 'davidson'")
     mixed = precision == "mixed"
     dt = torch.complex64 if mixed else torch.complex128
+    from .kshard import KShards
+    shards = KShards(b.Ngw, Nstates)
+    mine = shards.mine
+    if savewfc and shards.world > 1:
+        raise ValueError("savewfc with k-point sharding: write each rank's blocks with pwb200.io instead")
     if psiks is None:
-        psiks = rand_psiks(Ham, Nstates, seed, dt)
+        psiks = rand_psiks(Ham, Nstates, seed, dt, keep=set(mine))
     else:
-        psiks = [p.to(dt).contiguous() for p in psiks]
+        psiks = [p.to(dt).contiguous() if (p is not None and ik in mine) else None for ik, p in enumerate(psiks)]
     Vps = torch.from_numpy(Ham.V_Ps_loc).to(dev)
     rho = torch.from_numpy(guess_rhoe(Ham.system, b, Ham.pspots, Nel)).to(dev)
     ctx.update(rho, Vps)
@@ -182,21 +195,26 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     for it in range(1, NiterMax + 1):
         ethr = 0.1 if it == 1 else (0.01 if it == 2 else max(ethr / 5.0, ethr_evals_last))
         t0 = time.perf_counter()
-        nit = []
-        for ik in range(b.Nkpt):
+        nit = [0]
+        evals[:] = 0.0
+        for ik in mine:
             if update_psi == "LOBPCG":
                 ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
             else:
                 ev, n = ctx.davidson(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter)
             evals[:, ik] = ev
             nit.append(n)
+        if shards.world > 1:
+            evals[:] = shards.sum_(torch.from_numpy(evals).to(dev)).cpu().numpy()
         torch.cuda.synchronize()
         mTS = 0.0
         if use_smearing:
             Focc, E_fermi, mTS = smeared_occupations(Nel, wk, kT, evals)
         t1 = time.perf_counter()
-        for ik in range(b.Nkpt):
-            ctx.calc_rhoe(ik, psiks[ik], wk[ik] * Focc[:, ik], rho_new, accumulate=(ik > 0))
+        rho_new.zero_()
+        for j, ik in enumerate(mine):
+            ctx.calc_rhoe(ik, psiks[ik], wk[ik] * Focc[:, ik], rho_new, accumulate=(j > 0))
+        shards.sum_(rho_new)
         if Ham.sym is not None:
             ctx.symmetrize_rhoe(rho_new)
         diffRhoe = float(torch.sum(torch.abs(rho_new - rho)).item()) / N
@@ -210,10 +228,12 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         rho = torch.clamp(rho, min=EPS)
         sums = ctx.update(rho, Vps)
         Ek = En = 0.0
-        for ik in range(b.Nkpt):
+        for ik in mine:
             e2 = ctx.band_energies(ik, psiks[ik], wk[ik] * Focc[:, ik])
             Ek += e2[0]
             En += e2[1]
+        if shards.world > 1:
+            Ek, En = [float(v) for v in shards.sum_(torch.tensor([Ek, En], dtype=torch.float64, device=dev)).tolist()]
         E = {"Kinetic": Ek, "Ps_loc": sums[1] * dVol, "Ps_nloc": En, "Hartree": 0.5 * sums[0] * dVol,
              "XC": sums[2] * dVol, "NN": E_NN, "mTS": mTS}
         E["Total"] = sum(E.values())
@@ -235,7 +255,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         nsw = nsw + 1 if diffE < fp64_switch else 0
         if mixed and nsw >= 2 and it > 2:
             # iterative refinement: finish in FP64
-            psiks = [p.to(torch.complex128).contiguous() for p in psiks]
+            psiks = [p.to(torch.complex128).contiguous() if p is not None else None for p in psiks]
             mixed = False
             switched_at = it
         Etot_old = E["Total"]
@@ -247,4 +267,4 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     return {"energies": E, "evals": evals, "Focc": Focc, "E_fermi": E_fermi, "iterations": len(log), "log": log,
             "time_s": time.perf_counter() - t_start,
             "time_diag_s": t_diag, "time_rhoe_s": t_rho, "time_update_s": t_upd, "switched_to_fp64_at": switched_at,
-            "psiks": psiks, "rho": rho}
+            "psiks": psiks, "rho": rho, "kpoints_local": mine}
