@@ -391,6 +391,12 @@ def main():
 
     import torch
     import pwb200
+    if os.environ.get("PW_BENCH_ONLY_MULTIK") == "1":
+        # the batched-k op_H arms alone (a short command for profiling them)
+        torch.cuda.set_device(local)
+        flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+        print(json.dumps({"multik": multik_comparison(local, max(5, args.steps // 20), flush)}))
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist
