@@ -257,6 +257,31 @@ def time_rayleigh_ritz(ctx, psi32, nb, steps, flush):
     return res
 
 
+def time_eigh(ctx, nb, steps):
+    """The FP64 generalized eigenproblem of every LOBPCG iteration at this
+    workload's size (diag_LOBPCG.jl:185: eigen(Hermitian(T), Hermitian(G)),
+    order 3nb, lowest nb pairs) on seeded Hermitian T and positive definite G."""
+    import torch
+    n = 3 * nb
+    g = torch.Generator().manual_seed(SEED)
+    A = torch.randn((n, n), dtype=torch.complex128, generator=g)
+    T0 = (A + A.conj().T).cuda()
+    B = torch.randn((n, n), dtype=torch.complex128, generator=g) / n ** 0.5
+    G0 = (B @ B.conj().T + torch.eye(n, dtype=torch.complex128)).cuda()
+    ts = []
+    for i in range(steps + 2):
+        T, G = T0.clone(), G0.clone()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        ctx.eigh(T, G, k=nb)
+        e.record()
+        torch.cuda.synchronize()
+        if i >= 2:
+            ts.append(s.elapsed_time(e))
+    return {"n": n, "k": nb, "ms": sum(ts) / len(ts)}
+
+
 def time_device(ctx, x, y, ops, steps, warmup, flush):
     import torch
     for _ in range(warmup):
@@ -440,6 +465,7 @@ def main():
         ms, ms_fft, ms64 = [float(v) for v in t.tolist()]
 
     rr = time_rayleigh_ritz(ctx, x32, nbands, max(5, args.steps // 20), flush)
+    rr["eigh"] = time_eigh(ctx, nbands, max(3, args.steps // 40))
 
     # SCF time to 1e-6 Ha/atom on Si216 (the large mixed-precision SCF
     # workload): mixed vs FP64 on this GPU, rank 0 of a single-process run
@@ -496,6 +522,7 @@ def main():
         "clocks": clk.summary(),
         "rayleigh_ritz": {"gram_3nb": rr["gram"], "rotate_3nb_to_nb": rr["rotate"], "unit": "TFLOP/s",
                           "peak_bf16_tflops": bf16_peak(), "gram_frac_of_bf16_peak": rr["gram"]["tflops"] / bf16_peak(),
+                          "eigh_fp64": rr["eigh"],
                           "note": "split-BF16x3: three BF16 products per logical product, one counted"},
     }
     if scf_out is not None:
