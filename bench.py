@@ -108,6 +108,33 @@ def scf_comparison(device, seed):
     return out
 
 
+def scf_al4(device):
+    """Config C3's SCF: Al4 conventional fcc cell, GTH Al-q3, LDA-VWN,
+    ecutwfc 15 Ha, 8x8x8 mesh reduced by symmetry (35 k-points), 10 states,
+    Fermi-Dirac kT 0.01 Ha, Pulay 0.2, to |dE| < 1e-6 Ha/atom twice; mixed
+    (FP64 switch at 1e-5 Ha/atom) vs FP64 after an untimed warm-up of each."""
+    import pwb200
+    from pwb200 import scf
+    LL = 7.6524 * np.eye(3)
+    frac = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]]).T
+    H = pwb200.Hamiltonian(pwb200.System(["Al"] * 4, LL @ frac, LL), [PSP_AL], 15.0, meshk=(8, 8, 8),
+                           use_symmetry=True, device=device)
+    kw = dict(Nstates=10, betamix=0.2, mix_method="pulay", use_smearing=True, kT=0.01, seed=SEED)
+    for prec in ("mixed", "fp64"):
+        scf.KS_solve_SCF(H, NiterMax=2, precision=prec, **kw)
+    runs = {prec: scf.KS_solve_SCF(H, etot_conv_thr=4e-6, fp64_switch=4e-5, precision=prec, **kw)
+            for prec in ("mixed", "fp64")}
+    rm, rd = runs["mixed"], runs["fp64"]
+    out = {"system": "Al4 fcc, 8x8x8 with symmetry (%d k-points, Ngw %d-%d), 10 states, kT 0.01, LDA-VWN" % (
+               H.basis.Nkpt, min(H.basis.Ngw), max(H.basis.Ngw)),
+           "mixed_s": rm["time_s"], "fp64_s": rd["time_s"], "speedup": rd["time_s"] / rm["time_s"],
+           "mixed_iterations": rm["iterations"], "fp64_iterations": rd["iterations"],
+           "Etot_mixed": rm["energies"]["Total"], "Etot_fp64": rd["energies"]["Total"],
+           "dEtot_per_atom": abs(rm["energies"]["Total"] - rd["energies"]["Total"]) / 4}
+    H.ctx.close()
+    return out
+
+
 def si64_geometry():
     frac = np.array([(b + np.array([i, j, k])) / 2.0 for i in range(2) for j in range(2) for k in range(2)
                      for b in DIAMOND]).T
@@ -527,6 +554,7 @@ def main():
     }
     if scf_out is not None:
         out["scf"] = scf_out
+        out["scf_al4"] = scf_al4(local)
     if os.environ.get("PW_BENCH_NO_MULTIK") != "1" and world == 1:
         out["multik"] = multik_comparison(local, max(5, args.steps // 20), flush)
     if rank == 0 and world == 1 and args.workload == "si64" and os.environ.get("PW_BENCH_NO_CPU") != "1":
