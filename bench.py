@@ -111,8 +111,10 @@ def scf_comparison(device, seed):
 def scf_al4(device):
     """Config C3's SCF: Al4 conventional fcc cell, GTH Al-q3, LDA-VWN,
     ecutwfc 15 Ha, 8x8x8 mesh reduced by symmetry (35 k-points), 10 states,
-    Fermi-Dirac kT 0.01 Ha, Pulay 0.2, to |dE| < 1e-6 Ha/atom twice; mixed
-    (FP64 switch at 1e-5 Ha/atom) vs FP64 after an untimed warm-up of each."""
+    Fermi-Dirac kT 0.01 Ha, Pulay 0.2, to |dE| < 1e-6 Ha/atom twice, with the
+    LOBPCG of all k-points advanced together (pw_lobpcg_multi): mixed (FP64
+    switch at 1e-5 Ha/atom) vs FP64, and the FP64 SCF with one LOBPCG per
+    k-point for comparison; an untimed warm-up of each first."""
     import pwb200
     from pwb200 import scf
     LL = 7.6524 * np.eye(3)
@@ -120,16 +122,19 @@ def scf_al4(device):
     H = pwb200.Hamiltonian(pwb200.System(["Al"] * 4, LL @ frac, LL), [PSP_AL], 15.0, meshk=(8, 8, 8),
                            use_symmetry=True, device=device)
     kw = dict(Nstates=10, betamix=0.2, mix_method="pulay", use_smearing=True, kT=0.01, seed=SEED)
-    for prec in ("mixed", "fp64"):
-        scf.KS_solve_SCF(H, NiterMax=2, precision=prec, **kw)
-    runs = {prec: scf.KS_solve_SCF(H, etot_conv_thr=4e-6, fp64_switch=4e-5, precision=prec, **kw)
-            for prec in ("mixed", "fp64")}
-    rm, rd = runs["mixed"], runs["fp64"]
+    arms = {"mixed": ("mixed", True), "fp64": ("fp64", True), "fp64_per_k": ("fp64", False)}
+    for prec, batched in arms.values():
+        scf.KS_solve_SCF(H, NiterMax=2, precision=prec, batched=batched, **kw)
+    runs = {name: scf.KS_solve_SCF(H, etot_conv_thr=4e-6, fp64_switch=4e-5, precision=prec, batched=batched, **kw)
+            for name, (prec, batched) in arms.items()}
+    rm, rd, rp = runs["mixed"], runs["fp64"], runs["fp64_per_k"]
     out = {"system": "Al4 fcc, 8x8x8 with symmetry (%d k-points, Ngw %d-%d), 10 states, kT 0.01, LDA-VWN" % (
                H.basis.Nkpt, min(H.basis.Ngw), max(H.basis.Ngw)),
            "mixed_s": rm["time_s"], "fp64_s": rd["time_s"], "speedup": rd["time_s"] / rm["time_s"],
+           "fp64_per_k_lobpcg_s": rp["time_s"], "batched_vs_per_k_fp64": rp["time_s"] / rd["time_s"],
            "mixed_iterations": rm["iterations"], "fp64_iterations": rd["iterations"],
            "Etot_mixed": rm["energies"]["Total"], "Etot_fp64": rd["energies"]["Total"],
+           "Etot_fp64_per_k": rp["energies"]["Total"],
            "dEtot_per_atom": abs(rm["energies"]["Total"] - rd["energies"]["Total"]) / 4}
     H.ctx.close()
     return out

@@ -210,6 +210,17 @@ int pw_lobpcg(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
 int pw_davidson(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
                 int nb, double tol, int nitermax, double *evals, int *niter);
 
+/* diag_LOBPCG! over many k-points at once (diag_LOBPCG.jl:1-28 with the
+ * per-k-point steps of :51-225, the FP64 path's order) for small blocks:
+ * X[i] (device, Ngw[iks[i]] x nb, ld[i]) overwritten with the Ritz vectors,
+ * evals (host, nb x nk, column i for k-point iks[i]).  Every step is one
+ * launch for all k-points; a k-point stops where its own test
+ * |lambda - lambda_old| < tol holds for nconv (nb if <= 0) values.
+ * Needs 3 nb <= 48.  niter: iterations of the slowest k-point. */
+int pw_lobpcg_multi(pw_ctx *ctx, int nk, const int *iks, int ispin, int dtype,
+                    void *const *X, const int64_t *ld, int nb, double tol,
+                    int nitermax, int nconv, double *evals, int *niter);
+
 /* ---- update! and energies on the device ----------------------------- */
 
 /* The density G-sphere (PWGrid.gvec: idx_g2r, G2, sorted by G2 so that

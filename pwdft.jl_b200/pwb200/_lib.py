@@ -58,6 +58,7 @@ SIGNATURES = {
     "pw_set_nonlocal_coef": (_i, [_vp, _i, _i32p, _i32p, _dp]),
     "pw_apply": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _u]),
     "pw_apply_multi": (_i, [_vp, _i, _i32p, _i, _i, C.POINTER(_vp), C.POINTER(_vp), _i64p, _i32p, _u]),
+    "pw_lobpcg_multi": (_i, [_vp, _i, _i32p, _i, _i, C.POINTER(_vp), _i64p, _i, _d, _i, _i, _dp, C.POINTER(C.c_int)]),
     "pw_apply_vloc_noalloc": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _u]),
     "pw_noalloc_scratch_bytes": (C.c_uint64, []),
     "pw_kprec": (_i, [_vp, _i, _i, _vp, _vp, _i64, _i]),

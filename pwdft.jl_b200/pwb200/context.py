@@ -143,6 +143,22 @@ class Context:
                                          dtype_code(psis[0]), P, H, ld.ctypes.data_as(C.POINTER(C.c_int64)),
                                          nb.ctypes.data_as(C.POINTER(C.c_int32)), ops | (PW_GRAPH if graph else 0)))
 
+    def lobpcg_multi(self, iks, ispin, Xs, tol=1e-5, nitermax=100, nconv=0):
+        """pw_lobpcg_multi: the blocks Xs (torch (nb, Ngw) per k-point, one
+        dtype) of k-points iks advanced together; returns (evals (nb, nk), niter)."""
+        n = len(iks)
+        nb = Xs[0].shape[0]
+        k = np.ascontiguousarray(np.asarray(iks, dtype=np.int32))
+        P = (C.c_void_p * n)(*[x.data_ptr() for x in Xs])
+        ld = np.ascontiguousarray(np.array([x.shape[1] for x in Xs], dtype=np.int64))
+        ev = np.zeros((n, nb))
+        nit = C.c_int(0)
+        self.use_torch_stream()
+        self._chk(self._L.pw_lobpcg_multi(self.h, n, k.ctypes.data_as(C.POINTER(C.c_int32)), ispin, dtype_code(Xs[0]),
+                                          P, ld.ctypes.data_as(C.POINTER(C.c_int64)), nb, float(tol), int(nitermax),
+                                          int(nconv), _dptr(ev), C.byref(nit)))
+        return ev.T.copy(), nit.value
+
     def apply_vloc_noalloc(self, ik, ispin, psi, Hpsi, ops):
         """pw_apply_vloc_noalloc: the V_loc (+K) round trip using the library's
         fixed device scratch instead of context-allocated buffers."""

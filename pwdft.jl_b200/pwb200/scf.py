@@ -3,7 +3,8 @@
 Mirrors KS_solve_SCF.jl:24-373 (Nspin = 1, no smearing, Pulay or simple
 density mixing):
   ethr schedule            KS_solve_SCF.jl:177-185
-  diag_LOBPCG!             pw_lobpcg per k-point          (device, update_psi="LOBPCG")
+  diag_LOBPCG!             pw_lobpcg per k-point          (device, update_psi="LOBPCG"), or
+                           pw_lobpcg_multi for all k-points together (batched=True, nb <= 16)
   diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson";
                            the call of electrons_scf.jl:150)
   calc_rhoe!               pw_calc_rhoe                   (device)
@@ -148,7 +149,7 @@ class PulayMixer:
 def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
                  verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3,
-                 savewfc=False, wfc_dir="."):
+                 savewfc=False, wfc_dir=".", batched=False):
     """Runs the SCF loop; returns a dict with energies, eigenvalues, timings
     and the per-iteration log."""
     import torch
@@ -197,7 +198,12 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         t0 = time.perf_counter()
         nit = [0]
         evals[:] = 0.0
-        for ik in mine:
+        if batched and update_psi == "LOBPCG" and mine:
+            # every k-point of this rank advanced together (pw_lobpcg_multi)
+            ev, n = ctx.lobpcg_multi(mine, 0, [psiks[ik] for ik in mine], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
+            evals[:, mine] = ev
+            nit.append(n)
+        for ik in ([] if (batched and update_psi == "LOBPCG") else mine):
             if update_psi == "LOBPCG":
                 ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
             else:
