@@ -112,6 +112,9 @@ struct pw_ctx {
     uint64_t mk_key = 0;
     cudaGraphExec_t mk_exec = nullptr;
     cudaStream_t cap_stream = nullptr;
+    // host drop-ins: copy streams and per-chunk events of the pipelined op_H
+    cudaStream_t cp_in = nullptr, cp_out = nullptr;
+    cudaEvent_t ev_in[8] = {}, ev_cmp[8] = {};
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
 };
 
@@ -560,6 +563,12 @@ extern "C" void pw_destroy(pw_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->mk_exec) cudaGraphExecDestroy(c->mk_exec);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    for (int i = 0; i < 8; ++i) {
+        if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
+        if (c->ev_cmp[i]) cudaEventDestroy(c->ev_cmp[i]);
+    }
+    if (c->cp_in) cudaStreamDestroy(c->cp_in);
+    if (c->cp_out) cudaStreamDestroy(c->cp_out);
     for (void *p : c->allocs) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -972,18 +981,47 @@ extern "C" int pw_op_H_host(pw_ctx *c, int ik, int ispin, const double *psi, dou
     const size_t n = (size_t)ld * nb;
     const bool acc = (ops & PW_ACCUMULATE) != 0;
     if ((s = ensure(c, c->st_in, n * sizeof(double2))) || (s = ensure(c, c->st_out, n * sizeof(double2)))) return s;
-    CK(c, cudaMemcpyAsync(c->st_in.p, psi, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    if (acc) CK(c, cudaMemcpyAsync(c->st_out.p, Hpsi, n * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-    if (dtype == PW_C128) {
-        if ((s = apply_T<double>(c, ik, ispin, c->st_in.p, c->st_out.p, ld, nb, ops))) return s;
-    } else {
-        if ((s = ensure(c, c->st_in32, n * sizeof(float2))) || (s = ensure(c, c->st_out32, n * sizeof(float2)))) return s;
-        CK(c, convert_c128_to_c64((const double2 *)c->st_in.p, (float2 *)c->st_in32.p, n, c->stream));
-        if (acc) CK(c, convert_c128_to_c64((const double2 *)c->st_out.p, (float2 *)c->st_out32.p, n, c->stream));
-        if ((s = apply_T<float>(c, ik, ispin, c->st_in32.p, c->st_out32.p, ld, nb, ops))) return s;
-        CK(c, convert_c64_to_c128((const float2 *)c->st_out32.p, (double2 *)c->st_out.p, n, c->stream));
+    if (dtype == PW_C64 && ((s = ensure(c, c->st_in32, n * sizeof(float2))) || (s = ensure(c, c->st_out32, n * sizeof(float2)))))
+        return s;
+    // Pipelined over band chunks: the host-to-device copy of chunk i+1 and the
+    // device-to-host copy of chunk i-1 run on their own streams while chunk i
+    // computes on the context stream (each chunk has its own slice of the
+    // staging buffers, so no slice is reused within a call).
+    const int nch = std::max(1, std::min(8, nb / 32));
+    const int cb = (nb + nch - 1) / nch;
+    if (!c->cp_in) {
+        CK(c, cudaStreamCreateWithFlags(&c->cp_in, cudaStreamNonBlocking));
+        CK(c, cudaStreamCreateWithFlags(&c->cp_out, cudaStreamNonBlocking));
+        for (int i = 0; i < 8; ++i) {
+            CK(c, cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming));
+            CK(c, cudaEventCreateWithFlags(&c->ev_cmp[i], cudaEventDisableTiming));
+        }
     }
-    CK(c, cudaMemcpyAsync(Hpsi, c->st_out.p, n * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+    // the copy streams must not start before work already queued on the context stream
+    CK(c, cudaEventRecord(c->ev_cmp[0], c->stream));
+    CK(c, cudaStreamWaitEvent(c->cp_in, c->ev_cmp[0], 0));
+    for (int i = 0; i * cb < nb; ++i) {
+        const int b0 = i * cb, cnt = std::min(cb, nb - b0);
+        const size_t off = (size_t)b0 * ld, m = (size_t)cnt * ld;
+        double2 *in64 = (double2 *)c->st_in.p + off, *out64 = (double2 *)c->st_out.p + off;
+        CK(c, cudaMemcpyAsync(in64, psi + 2 * off, m * sizeof(double2), cudaMemcpyHostToDevice, c->cp_in));
+        if (acc) CK(c, cudaMemcpyAsync(out64, Hpsi + 2 * off, m * sizeof(double2), cudaMemcpyHostToDevice, c->cp_in));
+        CK(c, cudaEventRecord(c->ev_in[i], c->cp_in));
+        CK(c, cudaStreamWaitEvent(c->stream, c->ev_in[i], 0));
+        if (dtype == PW_C128) {
+            if ((s = apply_T<double>(c, ik, ispin, in64, out64, ld, cnt, ops))) return s;
+        } else {
+            float2 *in32 = (float2 *)c->st_in32.p + off, *out32 = (float2 *)c->st_out32.p + off;
+            CK(c, convert_c128_to_c64(in64, in32, m, c->stream));
+            if (acc) CK(c, convert_c128_to_c64(out64, out32, m, c->stream));
+            if ((s = apply_T<float>(c, ik, ispin, in32, out32, ld, cnt, ops))) return s;
+            CK(c, convert_c64_to_c128(out32, out64, m, c->stream));
+        }
+        CK(c, cudaEventRecord(c->ev_cmp[i], c->stream));
+        CK(c, cudaStreamWaitEvent(c->cp_out, c->ev_cmp[i], 0));
+        CK(c, cudaMemcpyAsync(Hpsi + 2 * off, out64, m * sizeof(double2), cudaMemcpyDeviceToHost, c->cp_out));
+    }
+    CK(c, cudaStreamSynchronize(c->cp_out));
     CK(c, cudaStreamSynchronize(c->stream));
     return PW_OK;
 }
