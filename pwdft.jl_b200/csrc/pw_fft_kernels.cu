@@ -443,15 +443,20 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // shared-memory layout of the x-fused plane kernels (in float2 units)
 struct PlaneXSmem {
     int N1, N2, Nxa, nwarps, group, plane_f;  // plane_f: floats of a full plane kept in shared memory (0 or N1*N2)
+    int bands = 1;                            // sub-planes held at once (bands of the same z-plane)
     __host__ __device__ size_t elems() const {
-        return (size_t)N1 + N2 + (size_t)Nxa * N2 + (size_t)nwarps * group * N1 + (plane_f + 1) / 2 + (N1 + 3) / 4;
+        return (size_t)N1 + N2 + (size_t)bands * Nxa * N2 + (size_t)nwarps * group * N1 + (plane_f + 1) / 2 + (N1 + 3) / 4;
     }
 };
 
-template <int N1, int N2, bool VS>
+// BPC sub-planes (nbh <= BPC bands of the same z-plane, band stride astr in
+// A) go through every phase together: each block barrier then separates
+// twice the line FFTs, and V(r), the twiddles and the active-x map are
+// loaded once for all of them.
+template <int N1, int N2, bool VS, int BPC = 1>
 __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 *__restrict__ twx,
                                                   const float2 *__restrict__ twy, const float *__restrict__ Vr,
-                                                  float2 *__restrict__ Ab) {
+                                                  float2 *__restrict__ Ab, int nbh = 1, size_t astr = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = float;
     constexpr int G = pwf::fp_group<N1>();
@@ -461,8 +466,9 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
     Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *ty = tx + N1;
     Cx<T> *S = ty + N2;
-    Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * N1;
-    float *Vs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * N1);
+    const size_t SP = (size_t)Nxa * N2;   // one sub-plane
+    Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * N1;
+    float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * N1);
     short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
     const int kz = blockIdx.x;
     const float *Vp = Vr + (size_t)kz * N1 * N2;
@@ -473,23 +479,29 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         iax[i] = -1;
     }
     for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[i];
-    for (int i = threadIdx.x; i < Nxa * N2; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
+    for (int i = threadIdx.x; i < nbh * (int)SP; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
     __syncthreads();
     for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
-    Cx<T> *Ap = Ab + (size_t)kz * Ncol;
+    for (int bb = 0; bb < nbh; ++bb) {
+        const Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
+        Cx<T> *Sb = S + bb * SP;
 #pragma unroll 4
-    for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Sb[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+    }
     __syncthreads();
-    line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);  // ends with __syncthreads
+    line_fft<T, N2, true>(S, nbh * Nxa, 1, N2, ty, +1);  // ends with __syncthreads
     if constexpr (VS) {
         cp_async_wait_all();
         __syncthreads();
     }
-    for (int g0 = warp * G; g0 < N2; g0 += NW * G) {
+    constexpr int NGRP = (N2 + G - 1) / G;
+    for (int q = warp; q < nbh * NGRP; q += NW) {
+        const int g0 = (q % NGRP) * G;
+        Cx<T> *Sb = S + (q / NGRP) * SP;
         const int nl = min(G, N2 - g0);
         auto ld_s = [&](int line, int x) {
             const int ia = iax[x];
-            return ia >= 0 ? S[ia * N2 + g0 + line] : cmake((T)0, (T)0);
+            return ia >= 0 ? Sb[ia * N2 + g0 + line] : cmake((T)0, (T)0);
         };
         auto st_v = [&](int line, int x, Cx<T> v) {
             const float vv = VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]);
@@ -498,22 +510,28 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         auto ld_x = [&](int line, int x) { return Xw[line * N1 + x]; };
         auto st_s = [&](int line, int x, Cx<T> v) {
             const int ia = iax[x];
-            if (ia >= 0) S[ia * N2 + g0 + line] = v;
+            if (ia >= 0) Sb[ia * N2 + g0 + line] = v;
         };
         pwf::group_fft<T, N1>(Xw, nl, tx, +1, lane, ld_s, st_v);
         pwf::group_fft<T, N1>(Xw, nl, tx, -1, lane, ld_x, st_s);
     }
     __syncthreads();
-    line_fft<T, N2, true>(S, Nxa, 1, N2, ty, -1);
+    line_fft<T, N2, true>(S, nbh * Nxa, 1, N2, ty, -1);
+    for (int bb = 0; bb < nbh; ++bb) {
+        Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
+        const Cx<T> *Sb = S + bb * SP;
 #pragma unroll 4
-    for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = S[kp.col_ia[c] * N2 + kp.col_j[c]];
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = Sb[kp.col_ia[c] * N2 + kp.col_j[c]];
+    }
 }
 
-template <int N1, int N2, bool VS>
+template <int N1, int N2, bool VS, int BPC>
 __global__ void __launch_bounds__(FFT_THREADS, 2)
 kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
-              float2 *__restrict__ A) {
-    plane_vloc_x_band<N1, N2, VS>(kp, twx, twy, Vr, A + (size_t)blockIdx.y * kp.N3 * kp.Ncol);
+              float2 *__restrict__ A, int nb) {
+    const int b0 = blockIdx.y * BPC;
+    const size_t astr = (size_t)kp.N3 * kp.Ncol;
+    plane_vloc_x_band<N1, N2, VS, BPC>(kp, twx, twy, Vr, A + b0 * astr, min(BPC, nb - b0), astr);
 }
 
 // calc_rhoe: bands [g*Bg, min(nb, (g+1)*Bg)) of plane kz; the weighted
@@ -841,13 +859,17 @@ template <int NN>
 static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
     const KPlan &kp = L.kp;
     constexpr bool VS = NN * NN * 4 <= 32 * 1024;
-    const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
+    // sub-planes per CTA, measured: 3 on the 75-point grid (Si64 round trip
+    // 0.996 -> 0.843 ms), 2 on the 120-point grid (Si216 15.2 -> 13.7 ms)
+    constexpr int BPC = NN == 75 ? 3 : (NN == 120 ? 2 : 1);
+    PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
+    ps.bands = BPC;
     const size_t smem = ps.elems() * sizeof(float2);
-    cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS>, smem);
+    cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS, BPC>, smem);
     if (e != cudaSuccess) return e;
-    dim3 grid(kp.N3, nb);
-    kx_plane_vloc<NN, NN, VS><<<grid, FFT_THREADS, smem, st>>>(kp, (const float2 *)L.twx, (const float2 *)L.twy,
-                                                              (const float *)Vr, (float2 *)A);
+    dim3 grid(kp.N3, (nb + BPC - 1) / BPC);
+    kx_plane_vloc<NN, NN, VS, BPC><<<grid, FFT_THREADS, smem, st>>>(kp, (const float2 *)L.twx, (const float2 *)L.twy,
+                                                                   (const float *)Vr, (float2 *)A, nb);
     return cudaGetLastError();
 }
 template <int NN>
