@@ -52,9 +52,9 @@ MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) of one FP32 pruned-FFT round trip of the Si64
 # op_H (160 bands: kf_zinv + kx_plane_vloc + kf_zfwd over two band chunks),
 # from one capture of this bench:
-#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
+#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 PW_BENCH_NO_MULTIK=1 ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
 #     --clock-control none -k regex:"kf_z|kx_plane" -s 12 -c 6 python bench.py --steps 3 --warmup 3
-FFT_TRAFFIC_BYTES = {"si64": 277.9e6}
+FFT_TRAFFIC_BYTES = {"si64": 262.8e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
