@@ -453,6 +453,13 @@ struct PlaneXSmem {
 // A) go through every phase together: each block barrier then separates
 // twice the line FFTs, and V(r), the twiddles and the active-x map are
 // loaded once for all of them.
+// Row stride of the sub-plane S: first-stage groups read 5 consecutive
+// elements of each of several lines per half-warp, so a stride = 5 (mod 16)
+// eight-byte words tiles the banks; measured a gain on the 120-point grid
+// (stride 133: Si216 round trip 13.7 -> 13.35 ms), a loss on the 75-point
+// one (the padding costs the third sub-plane per CTA), none elsewhere.
+template <int N> __host__ __device__ constexpr int plane_ld() { return N == 120 ? 133 : N; }
+
 template <int N1, int N2, bool VS, int BPC = 1>
 __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 *__restrict__ twx,
                                                   const float2 *__restrict__ twy, const float *__restrict__ Vr,
@@ -466,7 +473,8 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
     Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *ty = tx + N1;
     Cx<T> *S = ty + N2;
-    const size_t SP = (size_t)Nxa * N2;   // one sub-plane
+    constexpr int LD = plane_ld<N2>();
+    const size_t SP = (size_t)Nxa * LD;   // one sub-plane
     Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * N1;
     float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * N1);
     short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
@@ -486,10 +494,10 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         const Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
         Cx<T> *Sb = S + bb * SP;
 #pragma unroll 4
-        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Sb[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Sb[kp.col_ia[c] * LD + kp.col_j[c]] = Ap[c];
     }
     __syncthreads();
-    line_fft<T, N2, true>(S, nbh * Nxa, 1, N2, ty, +1);  // ends with __syncthreads
+    line_fft<T, N2, true>(S, nbh * Nxa, 1, LD, ty, +1);  // ends with __syncthreads
     if constexpr (VS) {
         cp_async_wait_all();
         __syncthreads();
@@ -501,7 +509,7 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         const int nl = min(G, N2 - g0);
         auto ld_s = [&](int line, int x) {
             const int ia = iax[x];
-            return ia >= 0 ? Sb[ia * N2 + g0 + line] : cmake((T)0, (T)0);
+            return ia >= 0 ? Sb[ia * LD + g0 + line] : cmake((T)0, (T)0);
         };
         auto st_v = [&](int line, int x, Cx<T> v) {
             const float vv = VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]);
@@ -510,18 +518,18 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         auto ld_x = [&](int line, int x) { return Xw[line * N1 + x]; };
         auto st_s = [&](int line, int x, Cx<T> v) {
             const int ia = iax[x];
-            if (ia >= 0) Sb[ia * N2 + g0 + line] = v;
+            if (ia >= 0) Sb[ia * LD + g0 + line] = v;
         };
         pwf::group_fft<T, N1>(Xw, nl, tx, +1, lane, ld_s, st_v);
         pwf::group_fft<T, N1>(Xw, nl, tx, -1, lane, ld_x, st_s);
     }
     __syncthreads();
-    line_fft<T, N2, true>(S, nbh * Nxa, 1, N2, ty, -1);
+    line_fft<T, N2, true>(S, nbh * Nxa, 1, LD, ty, -1);
     for (int bb = 0; bb < nbh; ++bb) {
         Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
         const Cx<T> *Sb = S + bb * SP;
 #pragma unroll 4
-        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = Sb[kp.col_ia[c] * N2 + kp.col_j[c]];
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = Sb[kp.col_ia[c] * LD + kp.col_j[c]];
     }
 }
 
@@ -862,7 +870,7 @@ static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void 
     // sub-planes per CTA, measured: 3 on the 75-point grid (Si64 round trip
     // 0.996 -> 0.843 ms), 2 on the 120-point grid (Si216 15.2 -> 13.7 ms)
     constexpr int BPC = NN == 75 ? 3 : (NN == 120 ? 2 : 1);
-    PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
+    PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
     ps.bands = BPC;
     const size_t smem = ps.elems() * sizeof(float2);
     cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS, BPC>, smem);
@@ -915,7 +923,7 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
                                         (const float *)Vr, (float2 *)A);                                             \
         } else if constexpr (sizeof(T) == 4) {                                                                       \
             constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
-            const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};           \
+            const PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0}; \
             const size_t psm = ps.elems() * sizeof(float2);                                                          \
             if ((e = set_smem<float>((const void *)mk_plane_vloc_x<NN, NN, VS>, psm)) != cudaSuccess) return e;     \
             mk_plane_vloc_x<NN, NN, VS><<<dim3(NN, nbands), FFT_THREADS, psm, st>>>(                                 \
