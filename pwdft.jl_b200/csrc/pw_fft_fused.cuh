@@ -208,4 +208,90 @@ __device__ __forceinline__ void group_fft(Cx<T> *buf, int nl, const Cx<T> *tw, i
     }
 }
 
+// Inverse N-point FFT, pointwise scale, forward FFT of nl <= fp_group<N>()
+// lines held by one warp: the op_V_loc x-pass.  The inverse's last stage
+// leaves lane (line, j) holding f[j + R0 r], r < R1 (N = R0 R1), which is
+// exactly the input of a decimation-in-frequency forward step,
+//   F[k2 + R1 k1] = sum_j w_R0^(j k1) [w_N^(j k2) sum_r f[j + R0 r] w_R1^(r k2)],
+// so the scale (vsc(line, x)), the forward radix-R1 DFT and its twiddles
+// stay in registers and one shared-memory exchange (buf) precedes the
+// radix-R0 DFTs, whose outputs go out through st(line, x, v).  One-stage
+// plans (one line per lane) never touch buf.
+template <typename T, int N, class LD0, class VS, class ST>
+__device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> *tw, int lane, LD0 &ld0, VS &vsc,
+                                                ST &st) {
+    constexpr int NST = FPlan<N>::nst;
+    static_assert(NST == 1 || NST == 2, "fused plans have one or two stages");
+    if constexpr (NST == 1) {
+        if (lane < nl) {
+            Cx<T> v[N];
+#pragma unroll
+            for (int r = 0; r < N; ++r) v[r] = ld0(lane, r);
+            Dft<T, N>::run(v, (T)1, tw, 1);
+#pragma unroll
+            for (int r = 0; r < N; ++r) v[r] = cscale(v[r], vsc(lane, r));
+            Dft<T, N>::run(v, (T)-1, tw, 1);
+#pragma unroll
+            for (int k = 0; k < N; ++k) st(lane, k, v[k]);
+        }
+        __syncwarp();
+    } else {
+        constexpr int R0 = FPlan<N>::r(0), R1 = FPlan<N>::r(1);
+        constexpr int G = fp_group<N>();
+        auto bst = [&](int line, int x, Cx<T> v) { buf[line * N + x] = v; };
+        fstage_io<T, N, 0>(nl, tw, 1, lane, ld0, bst);   // inverse stage 0 into buf
+        constexpr int MAXB = (G * R0 + 31) / 32;          // stage-1 butterflies: R0 per line
+        const int total = nl * R0;
+        Cx<T> v[MAXB][R1];
+#pragma unroll
+        for (int t = 0; t < MAXB; ++t) {
+            const int id = lane + 32 * t;
+            if (id < total) {
+                const int line = id / R0, j = id % R0;
+#pragma unroll
+                for (int r = 0; r < R1; ++r) v[t][r] = buf[line * N + j + r * R0];
+#pragma unroll
+                for (int r = 1; r < R1; ++r) {
+                    Cx<T> w = tw[r * j];
+                    w.y = -w.y;
+                    v[t][r] = cmul(v[t][r], w);
+                }
+                Dft<T, R1>::run(v[t], (T)1, tw, N / R1);      // v[r] = f[j + R0 r]
+#pragma unroll
+                for (int r = 0; r < R1; ++r) v[t][r] = cscale(v[t][r], vsc(line, j + R0 * r));
+                Dft<T, R1>::run(v[t], (T)-1, tw, N / R1);     // sum_r f[j + R0 r] w_R1^(r k2)
+#pragma unroll
+                for (int k2 = 1; k2 < R1; ++k2) v[t][k2] = cmul(v[t][k2], tw[(j * k2) % N]);
+            }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int t = 0; t < MAXB; ++t) {
+            const int id = lane + 32 * t;
+            if (id < total) {
+                const int line = id / R0, j = id % R0;
+#pragma unroll
+                for (int k2 = 0; k2 < R1; ++k2) buf[line * N + k2 * R0 + j] = v[t][k2];
+            }
+        }
+        __syncwarp();
+        constexpr int MAXB2 = (G * R1 + 31) / 32;
+        const int total2 = nl * R1;
+#pragma unroll
+        for (int t = 0; t < MAXB2; ++t) {
+            const int id = lane + 32 * t;
+            if (id < total2) {
+                const int line = id / R1, k2 = id % R1;
+                Cx<T> u[R0];
+#pragma unroll
+                for (int j = 0; j < R0; ++j) u[j] = buf[line * N + k2 * R0 + j];
+                Dft<T, R0>::run(u, (T)-1, tw, N / R0);
+#pragma unroll
+                for (int k1 = 0; k1 < R0; ++k1) st(line, k2 + R1 * k1, u[k1]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace pwf

@@ -511,17 +511,12 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
             const int ia = iax[x];
             return ia >= 0 ? Sb[ia * LD + g0 + line] : cmake((T)0, (T)0);
         };
-        auto st_v = [&](int line, int x, Cx<T> v) {
-            const float vv = VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]);
-            Xw[line * N1 + x] = cscale(v, vv);
-        };
-        auto ld_x = [&](int line, int x) { return Xw[line * N1 + x]; };
+        auto vsc = [&](int line, int x) { return VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]); };
         auto st_s = [&](int line, int x, Cx<T> v) {
             const int ia = iax[x];
             if (ia >= 0) Sb[ia * LD + g0 + line] = v;
         };
-        pwf::group_fft<T, N1>(Xw, nl, tx, +1, lane, ld_s, st_v);
-        pwf::group_fft<T, N1>(Xw, nl, tx, -1, lane, ld_x, st_s);
+        pwf::group_fft_vpair<T, N1>(Xw, nl, tx, lane, ld_s, vsc, st_s);
     }
     __syncthreads();
     line_fft<T, N2, true>(S, nbh * Nxa, 1, LD, ty, -1);
@@ -697,15 +692,12 @@ mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int 
         const int ia = iax[x];
         return ia >= 0 ? S[ia * N + line] : cmake((T)0, (T)0);
     };
-    auto st_v = [&](int line, int x, Cx<T> v) { Xw[line * N + x] = cscale(v, Vs[line * N + x]); };
-    auto ld_x = [&](int line, int x) { return Xw[line * N + x]; };
+    auto vsc = [&](int line, int x) { return Vs[line * N + x]; };
     auto st_s = [&](int line, int x, Cx<T> v) {
         const int ia = iax[x];
         if (ia >= 0) S[ia * N + line] = v;
     };
-    pwf::group_fft<T, N>(Xw, N, tx, +1, lane, ld_s, st_v);
-    __syncwarp();
-    pwf::group_fft<T, N>(Xw, N, tx, -1, lane, ld_x, st_s);
+    pwf::group_fft_vpair<T, N>(Xw, N, tx, lane, ld_s, vsc, st_s);
     __syncwarp();
     pwf::group_fft<T, N>(Xw, Nxa, ty, -1, lane, ld_row, st_row);
     __syncwarp();

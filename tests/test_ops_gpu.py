@@ -74,6 +74,49 @@ def test_op_H(system, prec):
         assert rel_err(to_host(y), ref) < TOL[prec]
 
 
+@pytest.fixture(scope="module")
+def si216():
+    """Si216 (3x3x3 diamond cells, 120^3 grid, Ngw 80797): the 120-point
+    plane kernels (two bands per CTA, padded sub-plane rows).  Five bands,
+    so the last CTA holds one band; the oracle set-up takes about 30 s."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import pwb200
+    from oracle import systems
+    H = systems.Hamiltonian(systems.diamond_supercell(3, 10.2631), [systems.psp("Si-q4.gth")], 15.0, Nstates=432)
+    rng = np.random.default_rng(12)
+    N = H.pw.Npoints
+    dV = rng.standard_normal(N)
+    H.V_Total = H.V_Ps_loc + 0.01 * dV / np.abs(dV).max()
+    pw = H.pw
+    ctx = pwb200.Context(pw.Ns, pw.CellVolume, pw.gvecw.idx_gw2r, [pw.Gk2(0)])
+    ctx.set_vloc(H.V_Total)
+    ctx.set_nonlocal(0, H.betaNL[0])
+    ctx.set_nonlocal_coef(H.nl_triplets)
+    ngw = pw.gvecw.Ngw[0]
+    psi = (rng.standard_normal((ngw, 5)) + 1j * rng.standard_normal((ngw, 5))) / np.sqrt(ngw)
+    yield H, ctx, psi
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_op_H_120_grid(si216, prec):
+    import torch
+    import pwb200
+    from oracle import ops
+    H, ctx, psi = si216
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    ref = ops.op_H(H, psi, 0)
+    x = to_dev(psi, dt)
+    y = torch.empty_like(x)
+    ctx.apply(0, 0, x, y, pwb200.PW_OP_H)
+    assert rel_err(to_host(y), ref) < TOL[prec]
+    rho = torch.zeros(H.pw.Npoints, dtype=torch.float64, device="cuda")
+    w = np.array([2.0, 2.0, 1.5, 0.5, 0.25])
+    ctx.calc_rhoe(0, x, w, rho)
+    assert rel_err(rho.cpu().numpy(), ops.calc_rhoe(H, [psi], Focc=w[:, None])) < TOL[prec]
+
+
 @pytest.mark.parametrize("prec", ["c128", "c64"])
 @pytest.mark.parametrize("term", ["K", "VLOC", "VNL"])
 def test_op_terms_accumulate(system, prec, term):
