@@ -79,6 +79,43 @@ template <int N> __host__ __device__ constexpr int fp_group() {
     return 32 / mn > 0 ? 32 / mn : 1;
 }
 
+// Shared-memory twiddle layout of the fused plans.  One-stage plans keep
+// tw[m] = exp(-2 pi i m / N).  Two-stage plans (N = R0 R1) store
+//   tw[m]                     = exp(-2 pi i m / R0)   for m < R0, the roots the
+//                               radix-R0 DFT reads at compile-time indexes
+//                               (one word per warp: a broadcast);
+//   tw[R0 + (r - 1) R0 + j]   = exp(-2 pi i r j / N)  for 1 <= r < R1, j < R0,
+//                               the stage-1 twiddles, which lanes with
+//                               consecutive j read from consecutive words
+// (the natural table read at r j puts 2 and 4 lanes of a half-warp on one
+// bank for r = 2 and 4).  N entries either way; tw_src(i) is the natural
+// index of entry i, for filling the table from tw[m] = exp(-2 pi i m / N).
+template <int N> __host__ __device__ constexpr int tw_src(int i) {
+    if constexpr (FPlan<N>::nst == 1) {
+        return i;
+    } else {
+        constexpr int R0 = FPlan<N>::r(0);
+        return i < R0 ? i * (N / R0) : ((i - R0) / R0 + 1) * ((i - R0) % R0);
+    }
+}
+// step argument of the DFT of stage S: the radix-R0 roots sit at stride 1;
+// the stage-1 radix of a two-stage plan reads no table
+template <int R> constexpr bool direct_radix() { return R == 2 || R == 3 || R == 4 || R == 5 || R == 8; }
+template <int N, int S> __host__ __device__ constexpr int tw_step() {
+    static_assert(FPlan<N>::nst == 1 || direct_radix<FPlan<N>::r(1)>(), "two-stage plans end on a direct radix");
+    return (FPlan<N>::nst == 2 && S == 0) ? 1 : N / FPlan<N>::r(S);
+}
+// twiddle of element r of stage-S butterfly jm (jm < N_S, the stage's span)
+template <int N, int S> __device__ __forceinline__ int tw_at(int r, int jm) {
+    if constexpr (FPlan<N>::nst == 2 && S == 1) {
+        constexpr int R0 = FPlan<N>::r(0);
+        return R0 + (r - 1) * R0 + jm;
+    } else {
+        constexpr int R = FPlan<N>::r(S);
+        return r * jm * (N / (fp_ns<N>(S) * R));
+    }
+}
+
 template <typename T, int N, int S, bool JFAST>
 __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int ls, const Cx<T> *tw, int sign, int lane) {
     constexpr int R = FPlan<N>::r(S);
@@ -86,7 +123,6 @@ __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int l
     constexpr int NBF = N / R;
     constexpr int G = fp_group<N>();
     constexpr int MAXB = (G * NBF + 31) / 32;
-    constexpr int TWS = N / (NS * R);
     const int total = nl * NBF;
     const T sg = (T)sign;
     Cx<T> v[MAXB][R];
@@ -103,12 +139,12 @@ __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int l
             if (NS > 1) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    Cx<T> w = tw[r * jm * TWS];
+                    Cx<T> w = tw[tw_at<N, S>(r, jm)];
                     if (sign > 0) w.y = -w.y;
                     v[t][r] = cmul(v[t][r], w);
                 }
             }
-            Dft<T, R>::run(v[t], sg, tw, N / R);
+            Dft<T, R>::run(v[t], sg, tw, tw_step<N, S>());
         }
     }
     __syncwarp();
@@ -155,7 +191,6 @@ __device__ __forceinline__ void fstage_io(int nl, const Cx<T> *tw, int sign, int
     constexpr int NBF = N / R;
     constexpr int G = fp_group<N>();
     constexpr int MAXB = (G * NBF + 31) / 32;
-    constexpr int TWS = N / (NS * R);
     const int total = nl * NBF;
     const T sg = (T)sign;
     Cx<T> v[MAXB][R];
@@ -169,12 +204,12 @@ __device__ __forceinline__ void fstage_io(int nl, const Cx<T> *tw, int sign, int
             if (NS > 1) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    Cx<T> w = tw[r * jm * TWS];
+                    Cx<T> w = tw[tw_at<N, S>(r, jm)];
                     if (sign > 0) w.y = -w.y;
                     v[t][r] = cmul(v[t][r], w);
                 }
             }
-            Dft<T, R>::run(v[t], sg, tw, N / R);
+            Dft<T, R>::run(v[t], sg, tw, tw_step<N, S>());
         }
     }
     __syncwarp();
@@ -252,7 +287,7 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
                 for (int r = 0; r < R1; ++r) v[t][r] = buf[line * N + j + r * R0];
 #pragma unroll
                 for (int r = 1; r < R1; ++r) {
-                    Cx<T> w = tw[r * j];
+                    Cx<T> w = tw[tw_at<N, 1>(r, j)];
                     w.y = -w.y;
                     v[t][r] = cmul(v[t][r], w);
                 }
@@ -261,7 +296,7 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
                 for (int r = 0; r < R1; ++r) v[t][r] = cscale(v[t][r], vsc(line, j + R0 * r));
                 Dft<T, R1>::run(v[t], (T)-1, tw, N / R1);     // sum_r f[j + R0 r] w_R1^(r k2)
 #pragma unroll
-                for (int k2 = 1; k2 < R1; ++k2) v[t][k2] = cmul(v[t][k2], tw[(j * k2) % N]);
+                for (int k2 = 1; k2 < R1; ++k2) v[t][k2] = cmul(v[t][k2], tw[tw_at<N, 1>(k2, j)]);
             }
         }
         __syncwarp();
@@ -285,7 +320,7 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
                 Cx<T> u[R0];
 #pragma unroll
                 for (int j = 0; j < R0; ++j) u[j] = buf[line * N + k2 * R0 + j];
-                Dft<T, R0>::run(u, (T)-1, tw, N / R0);
+                Dft<T, R0>::run(u, (T)-1, tw, tw_step<N, 0>());
 #pragma unroll
                 for (int k1 = 0; k1 < R0; ++k1) st(line, k2 + R1 * k1, u[k1]);
             }

@@ -260,6 +260,16 @@ __device__ __forceinline__ void line_fft(Cx<T> *buf, int nl, int es, int ls, con
         pwt::lines<T, N, MaxV<T>::v, JF>(buf, nl, es, ls, tw, sign);
 }
 
+// natural index of shared twiddle entry i of an N-point line FFT of type T:
+// the fused FP32 plans use their own layout (pwf::tw_src), the FP64 ones the
+// natural table
+template <typename T, int N> __device__ __forceinline__ int tw_src(int i) {
+    if constexpr (sizeof(T) == 4)
+        return pwf::tw_src<N>(i);
+    else
+        return i;
+}
+
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int v = 2; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
@@ -275,7 +285,7 @@ __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restri
     const int c0 = blockIdx.x * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[tw_src<T, N3>(i)];
     for (int i = threadIdx.x; i < N3 * Cg; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
     __syncthreads();
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
@@ -304,7 +314,7 @@ __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restri
     const int c0 = blockIdx.x * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[i];
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[tw_src<T, N3>(i)];
     Ab += c0;
     for (int kz = warp; kz < N3; kz += nw)
         for (int cl = lane; cl < cn; cl += 32) Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + cl];
@@ -356,8 +366,8 @@ __device__ __forceinline__ void plane_vloc_band(const KPlan &kp, const Cx<T> *__
     Cx<T> *X = S + Nxa * N2;
     const int kz = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
-    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[tw_src<T, N1>(i)];
+    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[tw_src<T, N2>(i)];
     for (int i = threadIdx.x; i < Nxa * N2; i += blockDim.x) S[i] = cmake((T)0, (T)0);
     __syncthreads();
     Cx<T> *Ap = Ab + (size_t)kz * Ncol;
@@ -401,8 +411,8 @@ kf_plane_rho(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ 
     const int kz = blockIdx.x, g = blockIdx.y;
     constexpr int N12 = N1 * N2;
     T *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
-    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[i];
-    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[tw_src<T, N1>(i)];
+    for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[tw_src<T, N2>(i)];
     for (int i = threadIdx.x; i < N12; i += blockDim.x) rp[i] = (T)0;
     const int b0 = g * Bg, b1 = min(nb, b0 + Bg);
     for (int b = b0; b < b1; ++b) {
@@ -483,10 +493,10 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
     if constexpr (VS)
         for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[i], &Vp[i]);
     for (int i = threadIdx.x; i < N1; i += FFT_THREADS) {
-        tx[i] = twx[i];
+        tx[i] = twx[tw_src<float, N1>(i)];
         iax[i] = -1;
     }
-    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[tw_src<float, N2>(i)];
     for (int i = threadIdx.x; i < nbh * (int)SP; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
     __syncthreads();
     for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
@@ -560,10 +570,10 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
     const int kz = blockIdx.x, g = blockIdx.y;
     float *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
     for (int i = threadIdx.x; i < N1; i += FFT_THREADS) {
-        tx[i] = twx[i];
+        tx[i] = twx[tw_src<float, N1>(i)];
         iax[i] = -1;
     }
-    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[i];
+    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[tw_src<float, N2>(i)];
     float *acc = RS ? Rs : rp;
     for (int i = threadIdx.x; i < N12; i += FFT_THREADS) acc[i] = 0.0f;
     __syncthreads();
@@ -668,8 +678,8 @@ mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int 
     const int kz = blockIdx.x;
     for (int i = threadIdx.x; i < N * N; i += FFT_THREADS) Vs[i] = Vr[(size_t)kz * N * N + i];
     for (int i = threadIdx.x; i < N; i += FFT_THREADS) {
-        tx[i] = twx[i];
-        ty[i] = twy[i];
+        tx[i] = twx[tw_src<float, N>(i)];
+        ty[i] = twy[tw_src<float, N>(i)];
     }
     __syncthreads();
     const int gb = blockIdx.y * NW + warp;
