@@ -270,6 +270,21 @@ template <typename T, int N> __device__ __forceinline__ int tw_src(int i) {
         return i;
 }
 
+// Row stride (in elements) of the z-pass tile Z[kz][column] for Cg columns.
+// The FP32 line FFTs run G = fp_group lines per warp with the line index
+// fastest, so lane (line, j) reads word line + stride * j: a stride = G
+// (mod 16) tiles the 16 eight-byte bank pairs for G < 16; with G >= 16
+// (one line per lane) an odd stride keeps the entry scatter/gather, which
+// walks kz down a column, off a single bank.  FP64 keeps Cg.
+template <typename T, int N> __host__ __device__ constexpr int zrow(int Cg) {
+    if constexpr (sizeof(T) == 8) {
+        return Cg;
+    } else {
+        constexpr int G = pwf::fp_group<N>();
+        return G >= 16 ? (Cg | 1) : Cg + ((G - Cg) % 16 + 16) % 16;
+    }
+}
+
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int v = 2; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
@@ -285,16 +300,17 @@ __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restri
     const int c0 = blockIdx.x * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int Zs = zrow<T, N3>(Cg);
     for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[tw_src<T, N3>(i)];
-    for (int i = threadIdx.x; i < N3 * Cg; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
+    for (int i = threadIdx.x; i < N3 * Zs; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
     __syncthreads();
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0] = ps[kp.ent_igw[e]];
+    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) Z[kp.ent_kz[e] * Zs + kp.ent_col[e] - c0] = ps[kp.ent_igw[e]];
     __syncthreads();
-    line_fft<T, N3, false>(Z, cn, Cg, 1, tw, +1);
+    line_fft<T, N3, false>(Z, cn, Zs, 1, tw, +1);
     Ab += c0;
     for (int kz = warp; kz < N3; kz += nw)
-        for (int cl = lane; cl < cn; cl += 32) Ab[(size_t)kz * kp.Ncol + cl] = Z[kz * Cg + cl];
+        for (int cl = lane; cl < cn; cl += 32) Ab[(size_t)kz * kp.Ncol + cl] = Z[kz * Zs + cl];
 }
 
 template <typename T, int N3>
@@ -314,16 +330,17 @@ __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restri
     const int c0 = blockIdx.x * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int Zs = zrow<T, N3>(Cg);
     for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[tw_src<T, N3>(i)];
     Ab += c0;
     for (int kz = warp; kz < N3; kz += nw)
-        for (int cl = lane; cl < cn; cl += 32) Z[kz * Cg + cl] = Ab[(size_t)kz * kp.Ncol + cl];
+        for (int cl = lane; cl < cn; cl += 32) Z[kz * Zs + cl] = Ab[(size_t)kz * kp.Ncol + cl];
     __syncthreads();
-    line_fft<T, N3, false>(Z, cn, Cg, 1, tw, -1);
+    line_fft<T, N3, false>(Z, cn, Zs, 1, tw, -1);
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
     for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const int igw = kp.ent_igw[e];
-        Cx<T> out = Z[kp.ent_kz[e] * Cg + kp.ent_col[e] - c0];
+        Cx<T> out = Z[kp.ent_kz[e] * Zs + kp.ent_col[e] - c0];
         if (flags & 2) {
             const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[igw] : (T)kp.Gk2f[igw];
             out = cadd(out, cscale(ps[igw], (T)0.5 * g2));
@@ -821,9 +838,10 @@ cudaError_t launch_zinv(const FftLaunch &L, const void *psi, int64_t ld, int nb,
         dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
 #define PW_CASE(NN)                                                                                                  \
     if (kp.N3 == NN) {                                                                                               \
-        cudaError_t e = set_smem<T>((const void *)kf_zinv<T, NN>, smem);                                             \
+        const size_t zsm = (size_t)(NN + NN * zrow<T, NN>(Cg)) * sizeof(Cx<T>);                                      \
+        cudaError_t e = set_smem<T>((const void *)kf_zinv<T, NN>, zsm);                                              \
         if (e != cudaSuccess) return e;                                                                              \
-        kf_zinv<T, NN><<<grid, FFT_THREADS, smem, st>>>(kp, (const Cx<T> *)L.twz, (const Cx<T> *)psi, ld, (Cx<T> *)A, Cg); \
+        kf_zinv<T, NN><<<grid, FFT_THREADS, zsm, st>>>(kp, (const Cx<T> *)L.twz, (const Cx<T> *)psi, ld, (Cx<T> *)A, Cg); \
         return cudaGetLastError();                                                                                   \
     }
         FIXED_SIZES(PW_CASE)
@@ -846,9 +864,10 @@ cudaError_t launch_zfwd(const FftLaunch &L, const void *A, const void *psi, void
         dim3 grid((kp.Ncol + Cg - 1) / Cg, nb);
 #define PW_CASE(NN)                                                                                                  \
     if (kp.N3 == NN) {                                                                                               \
-        cudaError_t e = set_smem<T>((const void *)kf_zfwd<T, NN>, smem);                                             \
+        const size_t zsm = (size_t)(NN + NN * zrow<T, NN>(Cg)) * sizeof(Cx<T>);                                      \
+        cudaError_t e = set_smem<T>((const void *)kf_zfwd<T, NN>, zsm);                                              \
         if (e != cudaSuccess) return e;                                                                              \
-        kf_zfwd<T, NN><<<grid, FFT_THREADS, smem, st>>>(kp, (const Cx<T> *)L.twz, (const Cx<T> *)A, (const Cx<T> *)psi, \
+        kf_zfwd<T, NN><<<grid, FFT_THREADS, zsm, st>>>(kp, (const Cx<T> *)L.twz, (const Cx<T> *)A, (const Cx<T> *)psi, \
                                                         (Cx<T> *)Hpsi, ld, Cg, flags);                               \
         return cudaGetLastError();                                                                                   \
     }
@@ -908,11 +927,11 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
     const KPlan &kp = L.kp;
     if (kp.N1 != kp.N2 || kp.N2 != kp.N3) return cudaErrorNotSupported;
     const int Cg = L.Cg;
-    const size_t zsm = (size_t)(kp.N3 + kp.N3 * Cg) * sizeof(Cx<T>);
     const dim3 zgrid((max_ncol + Cg - 1) / Cg, nbands);
     cudaError_t e = cudaErrorNotSupported;
 #define PW_CASE(NN)                                                                                                  \
     if (kp.N1 == NN) {                                                                                               \
+        const size_t zsm = (size_t)(NN + NN * zrow<T, NN>(Cg)) * sizeof(Cx<T>);                                      \
         if ((e = set_smem<T>((const void *)mk_zinv<T, NN>, zsm)) != cudaSuccess) return e;                          \
         mk_zinv<T, NN><<<zgrid, FFT_THREADS, zsm, st>>>(ks, band_k, (const Cx<T> *)L.twz, (Cx<T> *)A, Cg);           \
         if ((e = cudaGetLastError()) != cudaSuccess) return e;                                                       \
