@@ -106,6 +106,22 @@ template <int N, int S> __host__ __device__ constexpr int tw_step() {
     return (FPlan<N>::nst == 2 && S == 0) ? 1 : N / FPlan<N>::r(S);
 }
 // twiddle of element r of stage-S butterfly jm (jm < N_S, the stage's span)
+// Padded element positions of a line held in shared memory.  With R0 = 24
+// (120 = 24 * 5) the first stage's outputs x = 24 j + r put lanes j = 0, 2,
+// 4 of a line on one bank; one spare word after every R0 elements
+// (pos(x) = x + x / R0) and a line stride fp_xs = 125 (13 mod 16) put the 16
+// lanes of a half-warp on 16 bank pairs in the first stage and cost at most
+// a 2-way conflict in the second.  Other plans are unpadded.
+template <int N> __host__ __device__ constexpr int fp_pad() { return N == 120 ? 1 : 0; }
+template <int N> __host__ __device__ constexpr int fp_pos(int x) {
+    if constexpr (fp_pad<N>() == 0)
+        return x;
+    else
+        return x + (x / FPlan<N>::r(0)) * fp_pad<N>();
+}
+template <int N> __host__ __device__ constexpr int fp_xs() { return fp_pad<N>() == 0 ? N : 125; }
+static_assert(fp_xs<120>() >= fp_pos<120>(119) + 1, "padded line fits its stride");
+
 template <int N, int S> __device__ __forceinline__ int tw_at(int r, int jm) {
     if constexpr (FPlan<N>::nst == 2 && S == 1) {
         constexpr int R0 = FPlan<N>::r(0);
@@ -116,7 +132,8 @@ template <int N, int S> __device__ __forceinline__ int tw_at(int r, int jm) {
     }
 }
 
-template <typename T, int N, int S, bool JFAST>
+// PAD: elements at fp_pos(x) (es must be 1)
+template <typename T, int N, int S, bool JFAST, bool PAD>
 __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int ls, const Cx<T> *tw, int sign, int lane) {
     constexpr int R = FPlan<N>::r(S);
     constexpr int NS = fp_ns<N>(S);
@@ -135,7 +152,7 @@ __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int l
             const int jm = j % NS;
             const Cx<T> *p = buf + line * ls + j * es;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[t][r] = p[r * NBF * es];
+            for (int r = 0; r < R; ++r) v[t][r] = PAD ? buf[line * ls + fp_pos<N>(j + r * NBF)] : p[r * NBF * es];
             if (NS > 1) {
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
@@ -155,23 +172,29 @@ __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int l
             const int line = JFAST ? l0 + id / NBF : l0 + id % nl;
             const int j = JFAST ? id % NBF : id / nl;
             const int jm = j % NS;
-            Cx<T> *q = buf + line * ls + ((j / NS) * NS * R + jm) * es;
+            const int x0 = (j / NS) * NS * R + jm;
+            Cx<T> *q = buf + line * ls + x0 * es;
 #pragma unroll
-            for (int r = 0; r < R; ++r) q[r * NS * es] = v[t][r];
+            for (int r = 0; r < R; ++r) {
+                if (PAD)
+                    buf[line * ls + fp_pos<N>(x0 + r * NS)] = v[t][r];
+                else
+                    q[r * NS * es] = v[t][r];
+            }
         }
     }
     __syncwarp();
-    if constexpr (S + 1 < FPlan<N>::nst) fstage<T, N, S + 1, JFAST>(buf, l0, nl, es, ls, tw, sign, lane);
+    if constexpr (S + 1 < FPlan<N>::nst) fstage<T, N, S + 1, JFAST, PAD>(buf, l0, nl, es, ls, tw, sign, lane);
 }
 
 // All lines [0, nlines) of length N; ends with __syncthreads().
-template <typename T, int N, bool JFAST>
+template <typename T, int N, bool JFAST, bool PAD = false>
 __device__ __forceinline__ void lines(Cx<T> *buf, int nlines, int es, int ls, const Cx<T> *tw, int sign) {
     constexpr int G = fp_group<N>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int l0 = warp * G; l0 < nlines; l0 += nw * G) {
         const int nl = min(G, nlines - l0);
-        fstage<T, N, 0, JFAST>(buf, l0, nl, es, ls, tw, sign, lane);
+        fstage<T, N, 0, JFAST, PAD>(buf, l0, nl, es, ls, tw, sign, lane);
     }
     __syncthreads();
 }
@@ -227,12 +250,13 @@ __device__ __forceinline__ void fstage_io(int nl, const Cx<T> *tw, int sign, int
 }
 
 // Whole N-point FFT of nl <= fp_group<N>() lines held by one warp in buf
-// (line stride N): the first stage reads through ld0, the last writes
-// through stl, the stages between use buf.
+// (line stride fp_xs, padded positions): the first stage reads through ld0,
+// the last writes through stl, the stages between use buf.
 template <typename T, int N, class LD0, class STL>
 __device__ __forceinline__ void group_fft(Cx<T> *buf, int nl, const Cx<T> *tw, int sign, int lane, LD0 &ld0, STL &stl) {
-    auto bld = [&](int line, int x) { return buf[line * N + x]; };
-    auto bst = [&](int line, int x, Cx<T> v) { buf[line * N + x] = v; };
+    constexpr int XS = fp_xs<N>();
+    auto bld = [&](int line, int x) { return buf[line * XS + fp_pos<N>(x)]; };
+    auto bst = [&](int line, int x, Cx<T> v) { buf[line * XS + fp_pos<N>(x)] = v; };
     constexpr int NST = FPlan<N>::nst;
     static_assert(NST == 1 || NST == 2, "fused plans have one or two stages");
     if constexpr (NST == 1) {
@@ -273,7 +297,8 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
     } else {
         constexpr int R0 = FPlan<N>::r(0), R1 = FPlan<N>::r(1);
         constexpr int G = fp_group<N>();
-        auto bst = [&](int line, int x, Cx<T> v) { buf[line * N + x] = v; };
+        constexpr int XS = fp_xs<N>(), RP = R0 + fp_pad<N>();   // fp_pos(j + R0 r) = j + RP r for j < R0
+        auto bst = [&](int line, int x, Cx<T> v) { buf[line * XS + fp_pos<N>(x)] = v; };
         fstage_io<T, N, 0>(nl, tw, 1, lane, ld0, bst);   // inverse stage 0 into buf
         constexpr int MAXB = (G * R0 + 31) / 32;          // stage-1 butterflies: R0 per line
         const int total = nl * R0;
@@ -284,7 +309,7 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
             if (id < total) {
                 const int line = id / R0, j = id % R0;
 #pragma unroll
-                for (int r = 0; r < R1; ++r) v[t][r] = buf[line * N + j + r * R0];
+                for (int r = 0; r < R1; ++r) v[t][r] = buf[line * XS + j + r * RP];
 #pragma unroll
                 for (int r = 1; r < R1; ++r) {
                     Cx<T> w = tw[tw_at<N, 1>(r, j)];
@@ -306,7 +331,7 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
             if (id < total) {
                 const int line = id / R0, j = id % R0;
 #pragma unroll
-                for (int k2 = 0; k2 < R1; ++k2) buf[line * N + k2 * R0 + j] = v[t][k2];
+                for (int k2 = 0; k2 < R1; ++k2) buf[line * XS + k2 * RP + j] = v[t][k2];
             }
         }
         __syncwarp();
@@ -319,7 +344,7 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
                 const int line = id / R1, k2 = id % R1;
                 Cx<T> u[R0];
 #pragma unroll
-                for (int j = 0; j < R0; ++j) u[j] = buf[line * N + k2 * R0 + j];
+                for (int j = 0; j < R0; ++j) u[j] = buf[line * XS + k2 * RP + j];
                 Dft<T, R0>::run(u, (T)-1, tw, tw_step<N, 0>());
 #pragma unroll
                 for (int k1 = 0; k1 < R0; ++k1) st(line, k2 + R1 * k1, u[k1]);

@@ -252,10 +252,11 @@ __global__ void k_zero(Cx<T> *p, int Ngw, int nb, int64_t ld) {
 // the run-time kernels above serve every other {2,3,5}-smooth size.
 // FP32 lines use the register-fused composite radices (fewer shared-memory
 // passes); FP64 lines keep the 2/3/4/5/8 stages (register pressure).
-template <typename T, int N, bool JF>
+template <typename T, int N, bool JF, bool PAD = false>
 __device__ __forceinline__ void line_fft(Cx<T> *buf, int nl, int es, int ls, const Cx<T> *tw, int sign) {
+    static_assert(!PAD || sizeof(T) == 4, "padded lines are FP32 only");
     if constexpr (sizeof(T) == 4)
-        pwf::lines<T, N, JF>(buf, nl, es, ls, tw, sign);
+        pwf::lines<T, N, JF, PAD>(buf, nl, es, ls, tw, sign);
     else
         pwt::lines<T, N, MaxV<T>::v, JF>(buf, nl, es, ls, tw, sign);
 }
@@ -471,8 +472,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 struct PlaneXSmem {
     int N1, N2, Nxa, nwarps, group, plane_f;  // plane_f: floats of a full plane kept in shared memory (0 or N1*N2)
     int bands = 1;                            // sub-planes held at once (bands of the same z-plane)
+    int xs = 0;                               // line stride of the per-warp x-line buffers (0: N1)
     __host__ __device__ size_t elems() const {
-        return (size_t)N1 + N2 + (size_t)bands * Nxa * N2 + (size_t)nwarps * group * N1 + (plane_f + 1) / 2 + (N1 + 3) / 4;
+        return (size_t)N1 + N2 + (size_t)bands * Nxa * N2 + (size_t)nwarps * group * (xs ? xs : N1) + (plane_f + 1) / 2 +
+               (N1 + 3) / 4;
     }
 };
 
@@ -480,12 +483,11 @@ struct PlaneXSmem {
 // A) go through every phase together: each block barrier then separates
 // twice the line FFTs, and V(r), the twiddles and the active-x map are
 // loaded once for all of them.
-// Row stride of the sub-plane S: first-stage groups read 5 consecutive
-// elements of each of several lines per half-warp, so a stride = 5 (mod 16)
-// eight-byte words tiles the banks; measured a gain on the 120-point grid
-// (stride 133: Si216 round trip 13.7 -> 13.35 ms), a loss on the 75-point
-// one (the padding costs the third sub-plane per CTA), none elsewhere.
-template <int N> __host__ __device__ constexpr int plane_ld() { return N == 120 ? 133 : N; }
+// Row stride of the sub-plane S: the padded line stride of the fused plan
+// (elements of row ia at ia * LD + fp_pos(y)); 125 on the 120-point grid,
+// unpadded elsewhere (on the 75-point grid padding would cost the third
+// sub-plane per CTA).
+template <int N> __host__ __device__ constexpr int plane_ld() { return pwf::fp_xs<N>(); }
 
 template <int N1, int N2, bool VS, int BPC = 1>
 __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 *__restrict__ twx,
@@ -501,9 +503,10 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
     Cx<T> *ty = tx + N1;
     Cx<T> *S = ty + N2;
     constexpr int LD = plane_ld<N2>();
+    constexpr int XS = pwf::fp_xs<N1>();
     const size_t SP = (size_t)Nxa * LD;   // one sub-plane
-    Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * N1;
-    float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * N1);
+    Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * XS;
+    float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * XS);
     short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
     const int kz = blockIdx.x;
     const float *Vp = Vr + (size_t)kz * N1 * N2;
@@ -521,10 +524,10 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         const Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
         Cx<T> *Sb = S + bb * SP;
 #pragma unroll 4
-        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Sb[kp.col_ia[c] * LD + kp.col_j[c]] = Ap[c];
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Sb[kp.col_ia[c] * LD + pwf::fp_pos<N2>(kp.col_j[c])] = Ap[c];
     }
     __syncthreads();
-    line_fft<T, N2, true>(S, nbh * Nxa, 1, LD, ty, +1);  // ends with __syncthreads
+    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, ty, +1);  // ends with __syncthreads
     if constexpr (VS) {
         cp_async_wait_all();
         __syncthreads();
@@ -534,24 +537,27 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         const int g0 = (q % NGRP) * G;
         Cx<T> *Sb = S + (q / NGRP) * SP;
         const int nl = min(G, N2 - g0);
+        // rows g0 .. g0 + G - 1 lie in one padding block (G divides R0)
+        static_assert(pwf::fp_pad<N2>() == 0 || pwf::FPlan<N2>::r(0) % G == 0, "row groups inside a padding block");
+        const int yp = pwf::fp_pos<N2>(g0);
         auto ld_s = [&](int line, int x) {
             const int ia = iax[x];
-            return ia >= 0 ? Sb[ia * LD + g0 + line] : cmake((T)0, (T)0);
+            return ia >= 0 ? Sb[ia * LD + yp + line] : cmake((T)0, (T)0);
         };
         auto vsc = [&](int line, int x) { return VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]); };
         auto st_s = [&](int line, int x, Cx<T> v) {
             const int ia = iax[x];
-            if (ia >= 0) Sb[ia * LD + g0 + line] = v;
+            if (ia >= 0) Sb[ia * LD + yp + line] = v;
         };
         pwf::group_fft_vpair<T, N1>(Xw, nl, tx, lane, ld_s, vsc, st_s);
     }
     __syncthreads();
-    line_fft<T, N2, true>(S, nbh * Nxa, 1, LD, ty, -1);
+    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, ty, -1);
     for (int bb = 0; bb < nbh; ++bb) {
         Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
         const Cx<T> *Sb = S + bb * SP;
 #pragma unroll 4
-        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = Sb[kp.col_ia[c] * LD + kp.col_j[c]];
+        for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Ap[c] = Sb[kp.col_ia[c] * LD + pwf::fp_pos<N2>(kp.col_j[c])];
     }
 }
 
@@ -581,8 +587,9 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
     Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *ty = tx + N1;
     Cx<T> *S = ty + N2;
-    Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * N1;
-    float *Rs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * N1);
+    constexpr int XS = pwf::fp_xs<N1>();
+    Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * XS;
+    float *Rs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * XS);
     short *iax = reinterpret_cast<short *>(Rs + (RS ? N12 + (N12 & 1) : 0));
     const int kz = blockIdx.x, g = blockIdx.y;
     float *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
@@ -679,7 +686,7 @@ __global__ void __launch_bounds__(FFT_THREADS)
 mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nbands, int nxa_max,
                 const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
                 float2 *__restrict__ A) {
-    static_assert(pwf::FPlan<N>::nst == 1 && pwf::fp_group<N>() >= N, "one line per lane");
+    static_assert(pwf::FPlan<N>::nst == 1 && pwf::fp_group<N>() >= N && pwf::fp_xs<N>() == N, "one line per lane");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = float;
     constexpr int NW = FFT_THREADS / 32;
@@ -893,6 +900,7 @@ static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void 
     constexpr int BPC = NN == 75 ? 3 : (NN == 120 ? 2 : 1);
     PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
     ps.bands = BPC;
+    ps.xs = pwf::fp_xs<NN>();
     const size_t smem = ps.elems() * sizeof(float2);
     cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS, BPC>, smem);
     if (e != cudaSuccess) return e;
@@ -906,7 +914,8 @@ static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb,
                                       void *rho_part, cudaStream_t st) {
     const KPlan &kp = L.kp;
     constexpr bool RS = NN * NN * 4 <= 32 * 1024;
-    const PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), RS ? NN * NN : 0};
+    PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), RS ? NN * NN : 0};
+    ps.xs = pwf::fp_xs<NN>();
     const size_t smem = ps.elems() * sizeof(float2);
     cudaError_t e = set_smem<float>((const void *)kx_plane_rho<NN, NN, RS>, smem);
     if (e != cudaSuccess) return e;
@@ -944,7 +953,8 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
                                         (const float *)Vr, (float2 *)A);                                             \
         } else if constexpr (sizeof(T) == 4) {                                                                       \
             constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
-            const PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0}; \
+            PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};       \
+            ps.xs = pwf::fp_xs<NN>();                                                                                \
             const size_t psm = ps.elems() * sizeof(float2);                                                          \
             if ((e = set_smem<float>((const void *)mk_plane_vloc_x<NN, NN, VS>, psm)) != cudaSuccess) return e;     \
             mk_plane_vloc_x<NN, NN, VS><<<dim3(NN, nbands), FFT_THREADS, psm, st>>>(                                 \
