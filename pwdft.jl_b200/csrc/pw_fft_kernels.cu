@@ -896,8 +896,10 @@ static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void 
     const KPlan &kp = L.kp;
     constexpr bool VS = NN * NN * 4 <= 32 * 1024;
     // sub-planes per CTA, measured: 3 on the 75-point grid (Si64 round trip
-    // 0.996 -> 0.843 ms), 2 on the 120-point grid (Si216 15.2 -> 13.7 ms)
-    constexpr int BPC = NN == 75 ? 3 : (NN == 120 ? 2 : 1);
+    // 0.996 -> 0.843 ms); 1 on the 120-point grid, where two CTAs per SM
+    // (103 KB each) beat two sub-planes in one CTA once the padded layout
+    // removed the bank conflicts (Si216 10.0 -> 8.7 ms)
+    constexpr int BPC = NN == 75 ? 3 : 1;
     PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
     ps.bands = BPC;
     ps.xs = pwf::fp_xs<NN>();
