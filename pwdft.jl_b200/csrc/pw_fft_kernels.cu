@@ -292,6 +292,7 @@ template <> struct MinBlocks<double> { static constexpr int v = 2; };
 
 // z-pass bodies for one band: ps / hs its sphere coefficients, Ab its
 // [z][column] block of the intermediate, column group blockIdx.x
+constexpr int ZU = 4;   // sphere entries per thread per pass of the scatter / gather
 template <typename T, int N3>
 __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ ps,
                                           Cx<T> *__restrict__ Ab, int Cg) {
@@ -306,7 +307,23 @@ __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restri
     for (int i = threadIdx.x; i < N3 * Zs; i += blockDim.x) Z[i] = cmake((T)0, (T)0);
     __syncthreads();
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) Z[kp.ent_kz[e] * Zs + kp.ent_col[e] - c0] = ps[kp.ent_igw[e]];
+    // ZU entries per thread per pass, every load issued before the first
+    // use: the sphere reads are scattered and latency-bound
+    for (int eb = e0 + threadIdx.x; eb < e1; eb += ZU * blockDim.x) {
+        int ig[ZU], zi[ZU];
+#pragma unroll
+        for (int u = 0; u < ZU; ++u) {
+            const int e = min(eb + u * (int)blockDim.x, e1 - 1);
+            ig[u] = kp.ent_igw[e];
+            zi[u] = kp.ent_kz[e] * Zs + kp.ent_col[e] - c0;
+        }
+        Cx<T> pv[ZU];
+#pragma unroll
+        for (int u = 0; u < ZU; ++u) pv[u] = ps[ig[u]];
+#pragma unroll
+        for (int u = 0; u < ZU; ++u)
+            if (eb + u * (int)blockDim.x < e1) Z[zi[u]] = pv[u];
+    }
     __syncthreads();
     line_fft<T, N3, false>(Z, cn, Zs, 1, tw, +1);
     Ab += c0;
@@ -334,20 +351,39 @@ __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restri
     const int Zs = zrow<T, N3>(Cg);
     for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[tw_src<T, N3>(i)];
     Ab += c0;
+#pragma unroll 4
     for (int kz = warp; kz < N3; kz += nw)
         for (int cl = lane; cl < cn; cl += 32) Z[kz * Zs + cl] = Ab[(size_t)kz * kp.Ncol + cl];
     __syncthreads();
     line_fft<T, N3, false>(Z, cn, Zs, 1, tw, -1);
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const int igw = kp.ent_igw[e];
-        Cx<T> out = Z[kp.ent_kz[e] * Zs + kp.ent_col[e] - c0];
-        if (flags & 2) {
-            const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[igw] : (T)kp.Gk2f[igw];
-            out = cadd(out, cscale(ps[igw], (T)0.5 * g2));
+    for (int eb = e0 + threadIdx.x; eb < e1; eb += ZU * blockDim.x) {
+        int ig[ZU], zi[ZU];
+#pragma unroll
+        for (int u = 0; u < ZU; ++u) {
+            const int e = min(eb + u * (int)blockDim.x, e1 - 1);
+            ig[u] = kp.ent_igw[e];
+            zi[u] = kp.ent_kz[e] * Zs + kp.ent_col[e] - c0;
         }
-        if (flags & 4) out = cadd(out, hs[igw]);
-        hs[igw] = out;
+        Cx<T> kin[ZU], acc[ZU];
+#pragma unroll
+        for (int u = 0; u < ZU; ++u) {
+            kin[u] = cmake((T)0, (T)0);
+            acc[u] = cmake((T)0, (T)0);
+            if (flags & 2) {
+                const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[ig[u]] : (T)kp.Gk2f[ig[u]];
+                kin[u] = cscale(ps[ig[u]], (T)0.5 * g2);
+            }
+            if (flags & 4) acc[u] = hs[ig[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < ZU; ++u)
+            if (eb + u * (int)blockDim.x < e1) {
+                Cx<T> out = Z[zi[u]];
+                if (flags & 2) out = cadd(out, kin[u]);
+                if (flags & 4) out = cadd(out, acc[u]);
+                hs[ig[u]] = out;
+            }
     }
 }
 
