@@ -8,6 +8,7 @@
 // passes instead of three, 27 takes one.
 #pragma once
 #include "pw_fft.cuh"
+#include <type_traits>
 
 namespace pwf {
 
@@ -20,27 +21,56 @@ template <typename T> struct Dft<T, 4> { static __device__ __forceinline__ void 
 template <typename T> struct Dft<T, 5> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 5>::run(v, s); } };
 template <typename T> struct Dft<T, 8> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 8>::run(v, s); } };
 
-// R = R1*R2 in registers.  tw[m * step] = exp(-2 pi i m / R) for m < R.
+// exp(-2 pi i m / R) evaluated at compile time: Taylor series of sin and
+// cos about 0 after reduction to [-pi, pi] (30 terms: below 1e-17 there).
+__host__ __device__ constexpr double ce_trig(double x, bool sine) {
+    constexpr double PI = 3.14159265358979323846264338327950288;
+    while (x > PI) x -= 2 * PI;
+    while (x < -PI) x += 2 * PI;
+    double term = sine ? x : 1.0, sum = term;
+    for (int k = 1; k < 30; ++k) {
+        const int a = sine ? 2 * k : 2 * k - 1, b = sine ? 2 * k + 1 : 2 * k;
+        term *= -x * x / ((double)a * (double)b);
+        sum += term;
+    }
+    return sum;
+}
+template <int M, int R> struct Root {
+    static constexpr double ang = -2.0 * 3.14159265358979323846264338327950288 * (double)(M % R) / (double)R;
+    static constexpr double c = ce_trig(ang, false), s = ce_trig(ang, true);
+};
+
+// compile-time loop: f(std::integral_constant<int, I>) for I in [I0, I1)
+template <int I0, int I1, class F> __device__ __forceinline__ void sfor(F &&f) {
+    if constexpr (I0 < I1) {
+        f(std::integral_constant<int, I0>{});
+        sfor<I0 + 1, I1>(f);
+    }
+}
+
+// R = R1*R2 in registers, twiddles W_R^(n2 k1) as compile-time constants
+// (no table reads; tw and step pass through to the sub-DFTs, which ignore
+// them too).
 template <typename T, int R1, int R2> struct CompDft {
     static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
         constexpr int R = R1 * R2;
         Cx<T> a[R];
-#pragma unroll
-        for (int n2 = 0; n2 < R2; ++n2) {
+        sfor<0, R2>([&](auto n2c) {
+            constexpr int n2 = decltype(n2c)::value;
             Cx<T> t[R1];
 #pragma unroll
             for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[R2 * n1 + n2];
             Dft<T, R1>::run(t, s, tw, step * R2);
-#pragma unroll
-            for (int k1 = 0; k1 < R1; ++k1) {
-                if (n2 * k1 != 0) {
-                    Cx<T> w = tw[((n2 * k1) % R) * step];
-                    if (s > 0) w.y = -w.y;
-                    t[k1] = cmul(t[k1], w);
+            sfor<0, R1>([&](auto k1c) {
+                constexpr int k1 = decltype(k1c)::value;
+                if constexpr (n2 * k1 != 0) {
+                    using W = Root<n2 * k1, R>;
+                    const T wy = s > 0 ? (T)-W::s : (T)W::s;
+                    t[k1] = cmul(t[k1], cmake((T)W::c, wy));
                 }
                 a[n2 * R1 + k1] = t[k1];
-            }
-        }
+            });
+        });
 #pragma unroll
         for (int k1 = 0; k1 < R1; ++k1) {
             Cx<T> t[R2];
@@ -81,9 +111,9 @@ template <int N> __host__ __device__ constexpr int fp_group() {
 
 // Shared-memory twiddle layout of the fused plans.  One-stage plans keep
 // tw[m] = exp(-2 pi i m / N).  Two-stage plans (N = R0 R1) store
-//   tw[m]                     = exp(-2 pi i m / R0)   for m < R0, the roots the
-//                               radix-R0 DFT reads at compile-time indexes
-//                               (one word per warp: a broadcast);
+//   tw[m]                     = exp(-2 pi i m / R0)   for m < R0 (the
+//                               composite DFTs now hold their roots as
+//                               compile-time constants and do not read them);
 //   tw[R0 + (r - 1) R0 + j]   = exp(-2 pi i r j / N)  for 1 <= r < R1, j < R0,
 //                               the stage-1 twiddles, which lanes with
 //                               consecutive j read from consecutive words
