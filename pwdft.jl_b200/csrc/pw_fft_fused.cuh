@@ -130,7 +130,7 @@ template <int N> __host__ __device__ constexpr int tw_src(int i) {
 }
 // step argument of the DFT of stage S: the radix-R0 roots sit at stride 1;
 // the stage-1 radix of a two-stage plan reads no table
-template <int R> constexpr bool direct_radix() { return R == 2 || R == 3 || R == 4 || R == 5 || R == 8; }
+template <int R> __host__ __device__ constexpr bool direct_radix() { return R == 2 || R == 3 || R == 4 || R == 5 || R == 8; }
 template <int N, int S> __host__ __device__ constexpr int tw_step() {
     static_assert(FPlan<N>::nst == 1 || direct_radix<FPlan<N>::r(1)>(), "two-stage plans end on a direct radix");
     return (FPlan<N>::nst == 2 && S == 0) ? 1 : N / FPlan<N>::r(S);

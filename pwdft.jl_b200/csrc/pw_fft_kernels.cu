@@ -293,6 +293,27 @@ template <> struct MinBlocks<double> { static constexpr int v = 2; };
 // z-pass bodies for one band: ps / hs its sphere coefficients, Ab its
 // [z][column] block of the intermediate, column group blockIdx.x
 constexpr int ZU = 4;   // sphere entries per thread per pass of the scatter / gather
+
+// asynchronous global -> shared copies (no register staging, so a thread
+// keeps every copy of a phase in flight at once)
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// z-passes of these line lengths stage through cp.async (measured: Si64
+// round trip 0.657 -> 0.612 ms, Si216 8.50 -> 7.93 ms; the 27-point
+// batched path was faster with register copies)
+template <int N3> __host__ __device__ constexpr bool z_async() { return N3 >= 64; }
+
+// one complex value: 8 bytes (FP32) or 16 bytes (FP64)
+template <typename T> __device__ __forceinline__ void cp_async_cx(Cx<T> *smem, const Cx<T> *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+    else
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
 template <typename T, int N3>
 __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ ps,
                                           Cx<T> *__restrict__ Ab, int Cg) {
@@ -317,13 +338,20 @@ __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restri
             ig[u] = kp.ent_igw[e];
             zi[u] = kp.ent_kz[e] * Zs + kp.ent_col[e] - c0;
         }
-        Cx<T> pv[ZU];
+        if constexpr (z_async<N3>()) {
 #pragma unroll
-        for (int u = 0; u < ZU; ++u) pv[u] = ps[ig[u]];
+            for (int u = 0; u < ZU; ++u)
+                if (eb + u * (int)blockDim.x < e1) cp_async_cx<T>(&Z[zi[u]], &ps[ig[u]]);
+        } else {
+            Cx<T> pv[ZU];
 #pragma unroll
-        for (int u = 0; u < ZU; ++u)
-            if (eb + u * (int)blockDim.x < e1) Z[zi[u]] = pv[u];
+            for (int u = 0; u < ZU; ++u) pv[u] = ps[ig[u]];
+#pragma unroll
+            for (int u = 0; u < ZU; ++u)
+                if (eb + u * (int)blockDim.x < e1) Z[zi[u]] = pv[u];
+        }
     }
+    if constexpr (z_async<N3>()) cp_async_wait_all();
     __syncthreads();
     line_fft<T, N3, false>(Z, cn, Zs, 1, tw, +1);
     Ab += c0;
@@ -351,9 +379,15 @@ __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restri
     const int Zs = zrow<T, N3>(Cg);
     for (int i = threadIdx.x; i < N3; i += blockDim.x) tw[i] = twz[tw_src<T, N3>(i)];
     Ab += c0;
+    if constexpr (z_async<N3>()) {
+        for (int kz = warp; kz < N3; kz += nw)
+            for (int cl = lane; cl < cn; cl += 32) cp_async_cx<T>(&Z[kz * Zs + cl], &Ab[(size_t)kz * kp.Ncol + cl]);
+        cp_async_wait_all();
+    } else {
 #pragma unroll 4
-    for (int kz = warp; kz < N3; kz += nw)
-        for (int cl = lane; cl < cn; cl += 32) Z[kz * Zs + cl] = Ab[(size_t)kz * kp.Ncol + cl];
+        for (int kz = warp; kz < N3; kz += nw)
+            for (int cl = lane; cl < cn; cl += 32) Z[kz * Zs + cl] = Ab[(size_t)kz * kp.Ncol + cl];
+    }
     __syncthreads();
     line_fft<T, N3, false>(Z, cn, Zs, 1, tw, -1);
     const int e0 = kp.col_ptr[c0], e1 = kp.col_ptr[c0 + cn];
@@ -498,11 +532,6 @@ kf_plane_rho(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ 
 // the forward x-FFT writes only the active-x outputs back into S.  No block
 // barrier is needed inside the x-pass, and the zero-fill, scatter, V and
 // gather passes over the full plane disappear.
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // shared-memory layout of the x-fused plane kernels (in float2 units)
 struct PlaneXSmem {
