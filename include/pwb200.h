@@ -210,6 +210,29 @@ int pw_lobpcg(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
 int pw_davidson(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
                 int nb, double tol, int nitermax, double *evals, int *niter);
 
+/* chebyfilt(Ham, X, degree, lb, ub) for k-point ik (CheFSI.jl:36-67): the
+ * scaled Chebyshev filter of the given degree (>= 1) over [lb, ub]
+ * (ub > lb), Y = p(H) X with the three-term recurrence of the reference
+ * (sigma1 = e / (lb - ub) fixed, sigma_{i+1} = 1 / (2 / sigma1 - sigma_i)).
+ * X and Y: distinct device blocks Ngw x nb (ld) of dtype; X is left
+ * unchanged.  degree op_H applications plus one fused combination kernel
+ * per step. */
+int pw_chebyfilt(pw_ctx *ctx, int ik, int ispin, int dtype, const void *X,
+                 void *Y, int64_t ld, int nb, int degree, double lb,
+                 double ub);
+
+/* get_ub_lb_lanczos(Ham, nlancz) for k-point ik (CheFSI.jl:70-123, with
+ * norm_matrix_induced of :127-137): nlancz (even, <= Ngw) Lanczos steps
+ * from the start vector v0 (device, Ngw ComplexF64; the reference draws it
+ * with randn) with one step of full reorthogonalisation, in FP64.
+ * lb = the (nlancz/2)-th smallest eigenvalue of the Lanczos matrix T,
+ * ub = ||T 1/sqrt(nlancz)|| + ||f|| (host doubles).  T's eigenvalues come
+ * from the Hermitian device solver on its upper triangle, which equals the
+ * reference's general eigvals(T) to rounding.  PW_ERR_NAN on a Lanczos
+ * breakdown (zero residual). */
+int pw_lanczos_bounds(pw_ctx *ctx, int ik, int ispin, int nlancz,
+                      const double *v0, double *lb, double *ub);
+
 /* diag_LOBPCG! over many k-points at once (diag_LOBPCG.jl:1-28 with the
  * per-k-point steps of :51-225, the FP64 path's order) for small blocks:
  * X[i] (device, Ngw[iks[i]] x nb, ld[i]) overwritten with the Ritz vectors,

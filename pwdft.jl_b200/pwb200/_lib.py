@@ -71,6 +71,8 @@ SIGNATURES = {
     "pw_lobpcg_host": (_i, [_vp, _i, _i, _i, _dp, _i64, _i, _d, _i, _i, _dp, C.POINTER(C.c_int)]),
     "pw_davidson": (_i, [_vp, _i, _i, _i, _vp, _i64, _i, _d, _i, _dp, C.POINTER(C.c_int)]),
     "pw_davidson_host": (_i, [_vp, _i, _i, _i, _dp, _i64, _i, _d, _i, _dp, C.POINTER(C.c_int)]),
+    "pw_chebyfilt": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _i, _d, _d]),
+    "pw_lanczos_bounds": (_i, [_vp, _i, _i, _i, _vp, _dp, _dp]),
     "pw_set_density_sphere": (_i, [_vp, _i64, _i64p, _dp, _i]),
     "pw_poisson": (_i, [_vp, _vp, _vp]),
     "pw_update": (_i, [_vp, _vp, _vp, _vp, _vp, _dp]),

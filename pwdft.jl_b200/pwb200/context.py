@@ -221,6 +221,29 @@ class Context:
                                   C.c_void_p(S.data_ptr()) if S is not None else None))
         return lam, S
 
+    def chebyfilt(self, ik, ispin, X, Y, degree, lb, ub):
+        """chebyfilt (CheFSI.jl:36-67): Y = p(H) X, the scaled Chebyshev
+        filter of `degree` over [lb, ub]; X, Y distinct (nb, Ngw) device
+        blocks of one dtype, X unchanged."""
+        assert X.dtype == Y.dtype and X.shape == Y.shape and X.is_contiguous() and Y.is_contiguous()
+        nb, ld = X.shape
+        self.use_torch_stream()
+        self._chk(self._L.pw_chebyfilt(self.h, ik, ispin, dtype_code(X), C.c_void_p(X.data_ptr()),
+                                       C.c_void_p(Y.data_ptr()), ld, nb, int(degree), float(lb), float(ub)))
+
+    def lanczos_bounds(self, ik, ispin, nlancz, v0):
+        """get_ub_lb_lanczos (CheFSI.jl:70-123) from the start vector v0 (a
+        complex128 device tensor of Ngw); returns (ub, lb) in the
+        reference's order."""
+        import torch
+        assert v0.dtype == torch.complex128 and v0.is_contiguous()
+        lb = C.c_double(0.0)
+        ub = C.c_double(0.0)
+        self.use_torch_stream()
+        self._chk(self._L.pw_lanczos_bounds(self.h, ik, ispin, int(nlancz), C.c_void_p(v0.data_ptr()),
+                                            C.byref(lb), C.byref(ub)))
+        return ub.value, lb.value
+
     def ortho_sqrt(self, X):
         """ortho_sqrt!: X (nb, Ngw) device block made orthonormal in place."""
         nb, ld = X.shape

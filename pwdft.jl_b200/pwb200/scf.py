@@ -7,6 +7,8 @@ density mixing):
                            pw_lobpcg_multi for all k-points together (batched=True, nb <= 16)
   diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson";
                            the call of electrons_scf.jl:150)
+  diag_CheFSI!             pwb200.chefsi per k-point      (device, update_psi="CheFSI",
+                           cheby_degree; KS_solve_SCF.jl:205-208)
   calc_rhoe!               pw_calc_rhoe                   (device)
   symmetrize_rhoe!         pw_symmetrize_rhoe             (device, Hamiltonians built with symmetry)
   mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
@@ -149,7 +151,7 @@ class PulayMixer:
 def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
                  verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3,
-                 savewfc=False, wfc_dir=".", batched=False):
+                 savewfc=False, wfc_dir=".", batched=False, cheby_degree=8):
     """Runs the SCF loop; returns a dict with energies, eigenvalues, timings
     and the per-iteration log."""
     import torch
@@ -164,8 +166,9 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     Focc, Nocc = occupations(Nel, Nstates, b.Nkpt)
     wk = Ham.wk
     Ham.setup_density()
-    if update_psi not in ("LOBPCG", "davidson"):
-        raise ValueError("update_psi must be 'LOBPCG' or 'davidson'")
+    if update_psi not in ("LOBPCG", "davidson", "CheFSI"):
+        raise ValueError("update_psi must be 'LOBPCG', 'davidson' or 'CheFSI'")
+    crng = np.random.default_rng(seed + 1)   # Lanczos start vectors of CheFSI
     mixed = precision == "mixed"
     dt = torch.complex64 if mixed else torch.complex128
     from .kshard import KShards
@@ -206,8 +209,11 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         for ik in ([] if (batched and update_psi == "LOBPCG") else mine):
             if update_psi == "LOBPCG":
                 ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
-            else:
+            elif update_psi == "davidson":
                 ev, n = ctx.davidson(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter)
+            else:
+                from .chefsi import diag_chefsi_k
+                ev, n = diag_chefsi_k(ctx, ik, 0, psiks[ik], cheby_degree, crng), 0
             evals[:, ik] = ev
             nit.append(n)
         if shards.world > 1:
