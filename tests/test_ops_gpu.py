@@ -77,8 +77,9 @@ def test_op_H(system, prec):
 @pytest.fixture(scope="module")
 def si216():
     """Si216 (3x3x3 diamond cells, 120^3 grid, Ngw 80797): the 120-point
-    plane kernels (two bands per CTA, padded sub-plane rows).  Five bands,
-    so the last CTA holds one band; the oracle set-up takes about 30 s."""
+    plane kernels (one band per CTA, rows padded one word per 24 elements)
+    and z passes (cp.async tiles); five bands; the oracle set-up takes
+    about 30 s."""
     if not cuda_ok():
         pytest.skip("no CUDA device")
     import pwb200
