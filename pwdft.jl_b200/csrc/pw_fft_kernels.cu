@@ -289,6 +289,9 @@ template <typename T, int N> __host__ __device__ constexpr int zrow(int Cg) {
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int v = 2; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
+// z passes: three CTAs per SM (80 registers, no spills) where the radix
+// allows it; the radix-24 butterflies of the 120-point lines would spill
+template <typename T, int N3> struct ZBlocks { static constexpr int v = (sizeof(T) == 4 && N3 <= 75) ? 3 : 2; };
 
 // z-pass bodies for one band: ps / hs its sphere coefficients, Ab its
 // [z][column] block of the intermediate, column group blockIdx.x
@@ -360,7 +363,7 @@ __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restri
 }
 
 template <typename T, int N3>
-__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+__global__ void __launch_bounds__(FFT_THREADS, ZBlocks<T, N3>::v)
 kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, int64_t ld, Cx<T> *__restrict__ A,
         int Cg) {
     const int b = blockIdx.y;
@@ -422,7 +425,7 @@ __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restri
 }
 
 template <typename T, int N3>
-__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+__global__ void __launch_bounds__(FFT_THREADS, ZBlocks<T, N3>::v)
 kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, const Cx<T> *__restrict__ psi,
         Cx<T> *__restrict__ Hpsi, int64_t ld, int Cg, int flags) {
     const int b = blockIdx.y;
@@ -698,7 +701,7 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
 // k-point, whose plan, blocks and offset in A come from ks.  The band
 // bodies are the single-k-point kernels' own.
 template <typename T, int N3>
-__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+__global__ void __launch_bounds__(FFT_THREADS, ZBlocks<T, N3>::v)
 mk_zinv(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> *__restrict__ twz, Cx<T> *__restrict__ A,
         int Cg) {
     const MkK &K = ks[band_k[blockIdx.y]];
@@ -709,7 +712,7 @@ mk_zinv(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> 
 }
 
 template <typename T, int N3>
-__global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
+__global__ void __launch_bounds__(FFT_THREADS, ZBlocks<T, N3>::v)
 mk_zfwd(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> *__restrict__ twz,
         const Cx<T> *__restrict__ A, int Cg, int flags) {
     const MkK &K = ks[band_k[blockIdx.y]];
