@@ -74,3 +74,69 @@ def calc_rhoe_(Ham, psiks, Rhoe, Focc):
     for ik, psi in enumerate(psiks):
         w = Ham.wk[ik] * Focc[:, ik]
         Ham.ctx.calc_rhoe(ik, psi, w, Rhoe, accumulate=(ik > 0))
+
+
+# ---- eigensolvers and orthonormalisation under the reference's names ----
+# (Nspin = 1: psiks holds one (Nstates, Ngw) device block per k-point; the
+# returned evals are (Nstates, Nkpt) like the reference's (Nstates, Nkspin).)
+
+def diag_LOBPCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
+    """diag_LOBPCG!(Ham, psiks; tol, NiterMax, Nstates_conv) (diag_LOBPCG.jl:1-28):
+    every block replaced by its Ritz vectors; returns evals."""
+    import numpy as np
+    evals = np.zeros((psiks[0].shape[0], len(psiks)))
+    for ik, X in enumerate(psiks):
+        Ham.ik = ik
+        evals[:, ik], _ = Ham.ctx.lobpcg(ik, Ham.ispin, X, tol=tol, nitermax=NiterMax, nconv=Nstates_conv)
+    return evals
+
+
+def diag_davidson_qe_(Ham, psiks, tol=1e-5, NiterMax=100):
+    """diag_davidson_qe!(Ham, psiks; tol, NiterMax) (diag_davidson_qe_v2.jl:6-34)."""
+    import numpy as np
+    evals = np.zeros((psiks[0].shape[0], len(psiks)))
+    for ik, X in enumerate(psiks):
+        Ham.ik = ik
+        evals[:, ik], _ = Ham.ctx.davidson(ik, Ham.ispin, X, tol=tol, nitermax=NiterMax)
+    return evals
+
+
+def diag_CheFSI_(Ham, psiks, cheby_degree, seed=1234):
+    """diag_CheFSI!(Ham, psiks, cheby_degree) (CheFSI.jl:1-31); the Lanczos
+    start vectors come from a generator seeded with `seed`."""
+    import numpy as np
+    from .chefsi import diag_chefsi_k
+    rng = np.random.default_rng(seed)
+    evals = np.zeros((psiks[0].shape[0], len(psiks)))
+    for ik, X in enumerate(psiks):
+        Ham.ik = ik
+        evals[:, ik] = diag_chefsi_k(Ham.ctx, ik, Ham.ispin, X, cheby_degree, rng)
+    return evals
+
+
+def chebyfilt(Ham, X, degree, lb, ub):
+    """chebyfilt(Ham, X, degree, lb, ub) -> Y (CheFSI.jl:36-67) at Ham.ik."""
+    Y = _torch().empty_like(X)
+    Ham.ctx.chebyfilt(Ham.ik, Ham.ispin, X, Y, degree, lb, ub)
+    return Y
+
+
+def get_ub_lb_lanczos(Ham, nlancz, v0=None, seed=None):
+    """get_ub_lb_lanczos(Ham, nlancz) -> (ub, lb) (CheFSI.jl:70-123) at Ham.ik;
+    v0 (complex128 device vector of Ngw) defaults to a seeded normal draw,
+    where the reference calls randn."""
+    import numpy as np
+    if v0 is None:
+        ngw = Ham.ctx.Ngw[Ham.ik]
+        rng = np.random.default_rng(seed)
+        v0 = _torch().from_numpy(rng.standard_normal(ngw) + 1j * rng.standard_normal(ngw)).to(f"cuda:{Ham.ctx.device}")
+    return Ham.ctx.lanczos_bounds(Ham.ik, Ham.ispin, nlancz, v0)
+
+
+def ortho_sqrt_(Ham, psi):
+    """ortho_sqrt!(psi) (ortho_sqrt.jl:1-11), in place on the device (the
+    context of Ham runs it)."""
+    Ham.ctx.ortho_sqrt(psi)
+
+
+__all__ += ["diag_LOBPCG_", "diag_davidson_qe_", "diag_CheFSI_", "chebyfilt", "get_ub_lb_lanczos", "ortho_sqrt_"]
