@@ -6,7 +6,10 @@ density mixing):
   diag_LOBPCG!             pw_lobpcg per k-point          (device, update_psi="LOBPCG"), or
                            pw_lobpcg_multi for all k-points together (batched=True, nb <= 16)
   diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson";
-                           the call of electrons_scf.jl:150)
+                           the call of electrons_scf.jl:150; the reference's
+                           KS_solve_SCF.jl:194-198 calls the 2-block diag_davidson!
+                           there, which is not built: same eigenpairs, other
+                           iteration counts)
   diag_CheFSI!             pwb200.chefsi per k-point      (device, update_psi="CheFSI",
                            cheby_degree; KS_solve_SCF.jl:205-208)
   calc_rhoe!               pw_calc_rhoe                   (device)
