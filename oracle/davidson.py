@@ -99,3 +99,59 @@ def diag_davidson_qe_all(Ham, psiks, tol=1e-5, NiterMax=100):
         Ham.ik = ik
         evals[:, ik], _ = diag_davidson_qe(Ham, psiks[ik], ik, EBANDS_THR=tol, NiterMax=NiterMax)
     return evals
+
+
+def diag_davidson(Ham, X, ik=None, tol=1e-5, NiterMax=100, Nstates_conv=0, hop=None):
+    """The 2-block Davidson of diag_davidson.jl:52-206 for one k-point: the
+    basis is [X, R] with R the Kprec-preconditioned, normalised residuals;
+    X (Nbasis, Nstates), orthonormal on entry, is overwritten with the Ritz
+    vectors.  Returns (evals, iterations, converged)."""
+    ik = Ham.ik if ik is None else ik
+    H = hop if hop is not None else (lambda v: op_H(Ham, v, ik))
+    Nbasis, Nstates = X.shape
+    if Nstates_conv == 0:
+        Nstates_conv = Nstates
+    n = Nstates
+    s1, s2 = slice(0, n), slice(n, 2 * n)
+    HX = H(X)
+    evals = np.real(np.sum(X.conj() * HX, axis=0))                      # :82-85
+    R = evals[None, :] * X - HX                                          # :88-93
+    res = np.sqrt(np.real(np.sum(R.conj() * R, axis=0)))
+    EPS = np.finfo(np.float64).eps
+    evals_old = evals.copy()
+    Hred = np.zeros((2 * n, 2 * n), dtype=np.complex128)
+    Sred = np.zeros_like(Hred)
+    it = 0
+    converged = False
+    for it in range(1, NiterMax + 1):
+        res_norm = np.where(EPS < res, 1.0 / np.where(res > 0, res, 1.0), 1.0)   # :107-117
+        R = R * res_norm[None, :]
+        R = Kprec(Ham, R, ik)                                            # :119
+        HR = H(R)                                                        # :121
+        if it == 1:                                                      # :124-131
+            Hred[s1, s1] = X.conj().T @ HX
+        else:
+            Hred[s1, s1] = np.diag(evals.astype(np.complex128))
+        Hred[s1, s2] = X.conj().T @ HR                                   # :133-136
+        Hred[s2, s2] = R.conj().T @ HR
+        Hred[s2, s1] = Hred[s1, s2].conj().T
+        Sred[s1, s1] = np.eye(n)                                         # :138-141
+        Sred[s1, s2] = X.conj().T @ R
+        Sred[s2, s2] = R.conj().T @ R
+        Sred[s2, s1] = Sred[s1, s2].conj().T
+        Hred = 0.5 * (Hred + Hred.conj().T)                              # :143-144
+        Sred = 0.5 * (Sred + Sred.conj().T)
+        lam, Xr = sla.eigh(Hred, Sred, lower=False)                      # :146
+        evals = lam[:n].copy()
+        devals = np.abs(evals - evals_old)                               # :150-151
+        nconv = int(np.sum(devals < tol))
+        Xn = X @ Xr[s1, s1] + R @ Xr[s2, s1]                             # :153-154
+        HX = HX @ Xr[s1, s1] + HR @ Xr[s2, s1]
+        X[:, :] = Xn
+        R = evals[None, :] * X - HX                                      # :157-162
+        res = np.sqrt(np.real(np.sum(R.conj() * R, axis=0)))
+        if nconv >= Nstates_conv:                                        # :170-176
+            converged = True
+            break
+        evals_old = evals.copy()
+    return evals, it, converged

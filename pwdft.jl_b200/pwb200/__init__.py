@@ -140,3 +140,19 @@ def ortho_sqrt_(Ham, psi):
 
 
 __all__ += ["diag_LOBPCG_", "diag_davidson_qe_", "diag_CheFSI_", "chebyfilt", "get_ub_lb_lanczos", "ortho_sqrt_"]
+
+
+def diag_davidson_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
+    """diag_davidson!(Ham, psiks; tol, NiterMax, Nstates_conv) (diag_davidson.jl:12-38):
+    the 2-block Davidson per k-point on complex128 blocks (pwb200.davidson)."""
+    import numpy as np
+    from .davidson import diag_davidson_k
+    evals = np.zeros((psiks[0].shape[0], len(psiks)))
+    for ik, X in enumerate(psiks):
+        Ham.ik = ik
+        evals[:, ik], _ = diag_davidson_k(Ham.ctx, ik, Ham.ispin, X, tol=tol, NiterMax=NiterMax,
+                                          Nstates_conv=Nstates_conv)
+    return evals
+
+
+__all__ += ["diag_davidson_"]

@@ -69,10 +69,10 @@ def test_chefsi_converges(fcc_dense):
         v0 = rng.standard_normal(ngw) + 1j * rng.standard_normal(ngw)
         psi, ev = chefsi.diag_CheFSI_k(H, psi, 8, v0, 0)
         sums.append(ev.sum())
-    # Gamma of Si fcc with the bare pseudopotential: a gap of 0.53 Ha above
-    # the lowest state, 0.005 Ha above the 3-fold state at 0.585, so the
-    # lowest converges fast and the cluster slowly (as in the reference's
-    # CheFSI SCF, which needs ~100 iterations on this system)
+    # Gamma of Si fcc with V_Total = 0 (kinetic and nonlocal terms only): a
+    # gap of 0.53 Ha above the lowest state, 0.005 Ha above the 3-fold state
+    # at 0.585, so the lowest converges fast and the cluster slowly (as in the
+    # reference's CheFSI SCF, which needs ~100 iterations on this system)
     assert abs(ev[0] - lam[0]) < 1e-8
     assert sums[-1] >= lam[:4].sum() - 1e-10 and sums[-1] < sums[0]
     assert np.abs(psi.conj().T @ psi - np.eye(4)).max() < 1e-12
