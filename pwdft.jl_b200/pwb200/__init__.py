@@ -156,3 +156,21 @@ def diag_davidson_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
 
 
 __all__ += ["diag_davidson_"]
+
+
+def diag_Emin_PCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0, tol_ebands=1e-4, alpha_t=3e-5, I_CG_BETA=2):
+    """diag_Emin_PCG!(Ham, psiks; tol, NiterMax, Nstates_conv, tol_ebands, α_t, I_CG_BETA)
+    (diag_Emin_PCG.jl:17-47): all-band PCG per k-point on complex128 blocks
+    (pwb200.emin_pcg)."""
+    import numpy as np
+    from .emin_pcg import diag_Emin_PCG_k
+    evals = np.zeros((psiks[0].shape[0], len(psiks)))
+    for ik, X in enumerate(psiks):
+        Ham.ik = ik
+        evals[:, ik], _ = diag_Emin_PCG_k(Ham.ctx, ik, Ham.ispin, X, tol=tol, NiterMax=NiterMax,
+                                          Nstates_conv=Nstates_conv, tol_ebands=tol_ebands, alpha_t=alpha_t,
+                                          I_CG_BETA=I_CG_BETA)
+    return evals
+
+
+__all__ += ["diag_Emin_PCG_"]

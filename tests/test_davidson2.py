@@ -14,39 +14,7 @@ import pytest
 import scipy.linalg as sla
 
 from conftest import cuda_ok
-
-
-class NumpyCtx:
-    """The block operations diag_davidson_k uses, in NumPy on torch CPU tensors."""
-
-    def __init__(self, H):
-        self.H = H
-
-    def apply(self, ik, ispin, psi, Hpsi):
-        import torch
-        from oracle import ops
-        Hpsi.copy_(torch.from_numpy(np.ascontiguousarray(ops.op_H(self.H, psi.numpy().T, ik).T)))
-
-    def kprec(self, ik, x, out):
-        import torch
-        from oracle import ops
-        out.copy_(torch.from_numpy(np.ascontiguousarray(ops.Kprec(self.H, x.numpy().T, ik).T)))
-
-    def gram(self, A, B, out, accumulate=False):
-        import torch
-        C = A.numpy().conj() @ B.numpy().T          # (m, n) = A^H B
-        out.copy_(torch.from_numpy(np.ascontiguousarray(C.T)) + (out if accumulate else 0))
-
-    def rotate(self, A, U, out, accumulate=False):
-        import torch
-        R = (A.numpy().T @ U.numpy().T).T           # (n, M) = (A U)^T
-        out.copy_(torch.from_numpy(np.ascontiguousarray(R)) + (out if accumulate else 0))
-
-    def eigh(self, T, G=None, k=None, vectors=True):
-        import torch
-        Tm, Gm = T.numpy().T, G.numpy().T
-        lam, S = sla.eigh(Tm, Gm, lower=False)
-        return torch.from_numpy(lam[:k].copy()), torch.from_numpy(np.ascontiguousarray(S[:, :k].T))
+from numpy_ctx import NumpyCtx
 
 
 @pytest.fixture(scope="module")
