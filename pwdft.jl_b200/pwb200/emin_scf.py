@@ -19,13 +19,9 @@ import time
 
 import numpy as np
 
-from .scf import occupations, rand_psiks
+from .scf import occupations, rand_psiks, torch_device
 from .system import guess_rhoe, ewald_energy
 from .emin_pcg import _rtrace, _ortho, _rayleigh
-
-
-def _device(ctx):
-    return getattr(ctx, "torch_device", None) or f"cuda:{ctx.device}"
 
 
 def _density(Ham, psis, Focc, wk, rho):
@@ -59,7 +55,7 @@ def KS_solve_Emin_PCG(Ham, psiks=None, alpha_t=3e-5, NiterMax=200, i_cg_beta=2, 
     import torch
     ctx = Ham.ctx
     b = Ham.basis
-    dev = _device(ctx)
+    dev = torch_device(ctx)
     N = b.Npoints
     dVol = b.CellVolume / N
     Nel = Ham.Nelectrons

@@ -43,6 +43,12 @@ from .system import kpoint_grid, guess_rhoe, ewald_energy
 EPS = np.finfo(np.float64).eps
 
 
+def torch_device(ctx):
+    """The torch device of a context's blocks: cuda:<device>, or the
+    `torch_device` a host stand-in of the context declares (CPU tests)."""
+    return getattr(ctx, "torch_device", None) or f"cuda:{ctx.device}"
+
+
 def occupations(Nelectrons, Nstates, Nkpt):
     """Electrons.jl:120-262 for Nspin = 1 without smearing."""
     nocc = int(round(Nelectrons / 2))
@@ -110,7 +116,7 @@ def rand_psiks(Ham, Nstates, seed, dtype, keep=None):
             continue
         w, U = np.linalg.eigh(psi.conj().T @ psi)
         psi = psi @ ((U / np.sqrt(w)) @ U.conj().T)
-        out.append(torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{Ham.ctx.device}").to(dtype).contiguous())
+        out.append(torch.from_numpy(np.ascontiguousarray(psi.T)).to(torch_device(Ham.ctx)).to(dtype).contiguous())
     return out
 
 
@@ -160,7 +166,11 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     import torch
     ctx = Ham.ctx
     b = Ham.basis
-    dev = f"cuda:{ctx.device}"
+    dev = torch_device(ctx)
+
+    def sync():
+        if dev.startswith("cuda"):
+            torch.cuda.synchronize()
     N = b.Npoints
     dVol = b.CellVolume / N
     Nel = Ham.Nelectrons
@@ -221,7 +231,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             nit.append(n)
         if shards.world > 1:
             evals[:] = shards.sum_(torch.from_numpy(evals).to(dev)).cpu().numpy()
-        torch.cuda.synchronize()
+        sync()
         mTS = 0.0
         if use_smearing:
             Focc, E_fermi, mTS = smeared_occupations(Nel, wk, kT, evals)
@@ -233,7 +243,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         if Ham.sym is not None:
             ctx.symmetrize_rhoe(rho_new)
         diffRhoe = float(torch.sum(torch.abs(rho_new - rho)).item()) / N
-        torch.cuda.synchronize()
+        sync()
         t2 = time.perf_counter()
         imix += 1
         if mixer is not None:
@@ -274,7 +284,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             mixed = False
             switched_at = it
         Etot_old = E["Total"]
-    torch.cuda.synchronize()
+    sync()
     if savewfc:
         # KS_solve_SCF_potmix.jl:301-307: WFC_ikspin_<n>.data per (k-point, spin)
         from .io import write_psiks

@@ -131,3 +131,25 @@ def test_emin_pcg_gpu_si_fcc():
     finally:
         H.ctx.close()
     assert res["iterations"] < 60 and abs(res["energies"]["Total"] - ABINIT) < 1e-6, res["log"][-3:]
+
+
+def test_scf_driver_matches_oracle_driver():
+    """The device SCF driver (pwb200.scf.KS_solve_SCF, LOBPCG, Pulay 0.2) on
+    the NumPy stand-in reproduces the oracle's KS_solve_SCF step by step:
+    ethr schedule, Pulay mixing, the rho >= eps clamp, energies and the
+    convergence test (KS_solve_SCF.jl:24-373)."""
+    import torch
+    from oracle import systems, scf as oscf
+    from pwb200 import scf
+    Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    start = oscf.rand_BlochWavefunc(Ho, seed=11)
+    log_o = []
+    E_o, _, _ = oscf.KS_solve_SCF(Ho, psiks=[p.copy() for p in start], betamix=0.2, mix_method="pulay",
+                                  etot_conv_thr=1e-7, log=log_o)
+    Hd = HostHam(systems.Ham_Si_fcc(meshk=(2, 2, 2)), (2, 2, 2))
+    ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
+    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-7, precision="fp64", psiks=ps)
+    assert res["iterations"] == len(log_o)
+    for row_o, row_d in zip(log_o, res["log"]):
+        assert row_o[0] == row_d[0] and abs(row_o[1] - row_d[1]) < 1e-9, (row_o, row_d)
+    assert abs(res["energies"]["Total"] - E_o["Total"]) < 1e-9
