@@ -3,7 +3,8 @@
 CPU:
   - the oracle restatement on Si fcc (3x3x3 MP, 14 k) reaches ABINIT's total
     energy (test/validations_old/Si_fcc.jl:15) within 1e-7 Ha;
-  - the device driver (pwb200.emin_scf) run on the NumPy stand-in for the
+  - the device drivers (pwb200.emin_scf, and pwb200.scf with LOBPCG and
+    CheFSI) run on the NumPy stand-in for the
     library (the block operations, pw_update sums, pw_calc_rhoe and
     pw_band_energies through the oracle) reproduces the oracle driver's
     energies step by step (1e-9 Ha) on a 2x2x2 mesh.
@@ -153,3 +154,47 @@ def test_scf_driver_matches_oracle_driver():
     for row_o, row_d in zip(log_o, res["log"]):
         assert row_o[0] == row_d[0] and abs(row_o[1] - row_d[1]) < 1e-9, (row_o, row_d)
     assert abs(res["energies"]["Total"] - E_o["Total"]) < 1e-9
+
+
+def test_chefsi_scf_driver_matches_oracle():
+    """KS_solve_SCF(update_psi="CheFSI") on the NumPy stand-in follows the
+    oracle's SCF driven by diag_CheFSI (CheFSI.jl:1-31) step by step, with
+    the same Lanczos start vectors (first 12 iterations, 1e-9 Ha)."""
+    import torch
+    from oracle import systems, scf as oscf, chefsi
+    from pwb200 import scf
+
+    class CheCtx(SCFCtx):
+        def chebyfilt(self, ik, ispin, X, Y, degree, lb, ub):
+            Y.copy_(torch.from_numpy(np.ascontiguousarray(
+                chefsi.chebyfilt(self.H, X.numpy().T.copy(), degree, lb, ub, ik).T)))
+
+        def lanczos_bounds(self, ik, ispin, nlancz, v0):
+            ub, lb, _ = chefsi.get_ub_lb_lanczos(self.H, nlancz, v0.numpy(), ik)
+            return ub, lb
+
+    seed = 5
+    Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    start = oscf.rand_BlochWavefunc(Ho, seed=seed)
+    rng = np.random.default_rng(seed + 1)      # the driver's Lanczos generator
+
+    def diag(Ham, psiks, tol, nconv):
+        ev = []
+        for ik in range(len(psiks)):
+            ngw = psiks[ik].shape[0]
+            v0 = rng.standard_normal(ngw) + 1j * rng.standard_normal(ngw)
+            psiks[ik], e = chefsi.diag_CheFSI_k(Ham, psiks[ik], 8, v0, ik)
+            ev.append(e)
+        return np.stack(ev, axis=1)
+
+    log_o = []
+    oscf.KS_solve_SCF(Ho, psiks=[p.copy() for p in start], betamix=0.2, mix_method="pulay", NiterMax=12,
+                      etot_conv_thr=1e-12, diag=diag, log=log_o)
+    Hd = HostHam(systems.Ham_Si_fcc(meshk=(2, 2, 2)), (2, 2, 2))
+    Hd.ctx = CheCtx(Hd.ctx.H)
+    ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
+    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", NiterMax=12, etot_conv_thr=1e-12, precision="fp64",
+                           psiks=ps, update_psi="CheFSI", cheby_degree=8, seed=seed)
+    assert len(res["log"]) == len(log_o) == 12
+    for row_o, row_d in zip(log_o, res["log"]):
+        assert abs(row_o[1] - row_d[1]) < 1e-9, (row_o, row_d)
