@@ -1,13 +1,15 @@
-"""KS_solve_Emin_PCG! (KS_solve_Emin_PCG.jl:27-270), direct minimisation.
+"""The SCF-level drivers: KS_solve_Emin_PCG! (KS_solve_Emin_PCG.jl:27-270,
+direct minimisation) and the host logic of KS_solve_SCF.
 
 CPU:
-  - the oracle restatement on Si fcc (3x3x3 MP, 14 k) reaches ABINIT's total
-    energy (test/validations_old/Si_fcc.jl:15) within 1e-7 Ha;
-  - the device drivers (pwb200.emin_scf, and pwb200.scf with LOBPCG and
-    CheFSI) run on the NumPy stand-in for the
-    library (the block operations, pw_update sums, pw_calc_rhoe and
-    pw_band_energies through the oracle) reproduces the oracle driver's
-    energies step by step (1e-9 Ha) on a 2x2x2 mesh.
+  - the oracle's direct minimisation on Si fcc (3x3x3 MP, 14 k) reaches
+    ABINIT's total energy (test/validations_old/Si_fcc.jl:15) within 1e-7 Ha;
+  - the device drivers (pwb200.emin_scf, and pwb200.scf with LOBPCG and with
+    CheFSI), run on the NumPy stand-in for the library (block operations,
+    pw_update sums, pw_calc_rhoe and pw_band_energies through the oracle),
+    reproduce the oracle drivers' energies step by step (1e-9 Ha) on a 2x2x2
+    mesh.
+GPU: the direct minimisation on Si fcc 3x3x3 reaches ABINIT's energy.
 """
 import numpy as np
 import pytest
