@@ -12,6 +12,8 @@ density mixing):
                            iteration counts)
   diag_CheFSI!             pwb200.chefsi per k-point      (device, update_psi="CheFSI",
                            cheby_degree; KS_solve_SCF.jl:205-208)
+  diag_Emin_PCG!           pwb200.emin_pcg per k-point    (device, update_psi="PCG", FP64;
+                           KS_solve_SCF.jl:199-203)
   calc_rhoe!               pw_calc_rhoe                   (device)
   symmetrize_rhoe!         pw_symmetrize_rhoe             (device, Hamiltonians built with symmetry)
   mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
@@ -179,8 +181,10 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     Focc, Nocc = occupations(Nel, Nstates, b.Nkpt)
     wk = Ham.wk
     Ham.setup_density()
-    if update_psi not in ("LOBPCG", "davidson", "CheFSI"):
-        raise ValueError("update_psi must be 'LOBPCG', 'davidson' or 'CheFSI'")
+    if update_psi not in ("LOBPCG", "davidson", "CheFSI", "PCG"):
+        raise ValueError("update_psi must be 'LOBPCG', 'davidson', 'CheFSI' or 'PCG'")
+    if update_psi == "PCG" and precision != "fp64":
+        raise ValueError("update_psi='PCG' (diag_Emin_PCG!) runs on FP64 blocks only")
     crng = np.random.default_rng(seed + 1)   # Lanczos start vectors of CheFSI
     mixed = precision == "mixed"
     dt = torch.complex64 if mixed else torch.complex128
@@ -224,6 +228,9 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
                 ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
             elif update_psi == "davidson":
                 ev, n = ctx.davidson(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter)
+            elif update_psi == "PCG":
+                from .emin_pcg import diag_Emin_PCG_k
+                ev, n = diag_Emin_PCG_k(ctx, ik, 0, psiks[ik], tol=ethr, NiterMax=lobpcg_maxiter, Nstates_conv=Nocc)
             else:
                 from .chefsi import diag_chefsi_k
                 ev, n = diag_chefsi_k(ctx, ik, 0, psiks[ik], cheby_degree, crng), 0

@@ -200,3 +200,41 @@ def test_chefsi_scf_driver_matches_oracle():
     assert len(res["log"]) == len(log_o) == 12
     for row_o, row_d in zip(log_o, res["log"]):
         assert abs(row_o[1] - row_d[1]) < 1e-9, (row_o, row_d)
+
+
+def test_pcg_scf_driver_matches_oracle():
+    """KS_solve_SCF(update_psi="PCG") on the NumPy stand-in follows the
+    oracle's SCF driven by diag_Emin_PCG! (KS_solve_SCF.jl:199-203) step by
+    step, and converges to the LOBPCG SCF's energy.  The PCG's line search
+    amplifies rounding differences (traces of Grams against vdot) from step
+    to step, so the steps agree to 1e-6 Ha rather than 1e-9 and the step
+    counts to within 2."""
+    import torch
+    from oracle import systems, scf as oscf, emin_pcg
+    from pwb200 import scf
+
+    Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    start = oscf.rand_BlochWavefunc(Ho, seed=3)
+
+    def diag(Ham, psiks, tol, nconv):
+        ev = []
+        for ik in range(len(psiks)):
+            e, _, _ = emin_pcg.diag_Emin_PCG(Ham, psiks[ik], ik, tol=tol, NiterMax=100, Nstates_conv=nconv)
+            ev.append(e)
+        return np.stack(ev, axis=1)
+
+    log_o = []
+    E_o, _, _ = oscf.KS_solve_SCF(Ho, psiks=[p.copy() for p in start], betamix=0.2, mix_method="pulay",
+                                  etot_conv_thr=1e-7, diag=diag, log=log_o)
+    Hd = HostHam(systems.Ham_Si_fcc(meshk=(2, 2, 2)), (2, 2, 2))
+    ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
+    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-7, precision="fp64", psiks=ps,
+                           update_psi="PCG")
+    assert abs(len(res["log"]) - len(log_o)) <= 2
+    for row_o, row_d in zip(log_o, res["log"]):
+        assert abs(row_o[1] - row_d[1]) < 1e-6, (row_o, row_d)
+    assert abs(res["energies"]["Total"] - E_o["Total"]) < 1e-6
+    Ho2 = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    E_l, _, _ = oscf.KS_solve_SCF(Ho2, psiks=[p.copy() for p in start], betamix=0.2, mix_method="pulay",
+                                  etot_conv_thr=1e-7)
+    assert abs(res["energies"]["Total"] - E_l["Total"]) < 1e-6
