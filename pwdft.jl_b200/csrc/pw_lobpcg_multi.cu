@@ -314,7 +314,7 @@ __device__ void jacobi(double2 *A, double2 *V, int n, double2 *rot /* [NMAX/2+1]
         if (!(red[64] > 1e-26 * red[65]) || n < 2) break;   // relative off-diagonal norm 1e-13
         __syncthreads();
         for (int step = 0; step < ne - 1; ++step) {
-            // pairs of this round: position 0 fixed, the others rotate
+            // pairs of this step of the round-robin ordering: position 0 fixed, the others rotate
             const int np = ne / 2;
             for (int t = threadIdx.x; t < np; t += blockDim.x) {
                 auto at = [&](int pos) { return pos == 0 ? 0 : 1 + (pos - 1 + step) % (ne - 1); };
