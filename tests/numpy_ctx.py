@@ -2,8 +2,10 @@
 methods apply, kprec, gram, rotate, eigh, calc_grad, ortho_sqrt), with the
 layouts of the C ABI: band-major (nb, Ngw) blocks, pw_gram writing A^H B
 column-major, pw_rotate taking U column-major, pw_eigh returning
-eigenvectors as rows.  Used by the CPU tests of the host compositions
-(pwb200.davidson, pwb200.emin_pcg); test infrastructure only."""
+eigenvectors as rows; SCFCtx adds pw_update's sums, calc_rhoe, band
+energies and LOBPCG through the oracle, and HostHam the host attributes of
+pwb200.Hamiltonian, so the SCF drivers run on the CPU.  Used by the CPU
+tests of the host compositions and drivers; test infrastructure only."""
 import numpy as np
 import scipy.linalg as sla
 
@@ -53,3 +55,72 @@ class NumpyCtx:
         import torch
         from oracle.lobpcg import ortho_sqrt
         X.copy_(torch.from_numpy(np.ascontiguousarray(ortho_sqrt(X.numpy().T).T)))
+
+
+class SCFCtx(NumpyCtx):
+    """NumpyCtx plus the density, update! and band-energy entry points."""
+    torch_device = "cpu"
+    device = 0
+
+    def update(self, rho, Vps):
+        from oracle import energies
+        r = rho.numpy().copy()
+        self.H.update(r)
+        Eps, EH, Exc = energies.calc_E_local(self.H, r)
+        dVol = self.H.pw.CellVolume / self.H.pw.Npoints
+        return np.array([2.0 * EH / dVol, Eps / dVol, Exc / dVol])
+
+    def lobpcg(self, ik, ispin, X, tol=1e-5, nitermax=100, nconv=0):
+        import torch
+        from oracle.lobpcg import diag_LOBPCG_k
+        Xh = X.numpy().T.copy()
+        ev = diag_LOBPCG_k(self.H, Xh, ik, tol=tol, NiterMax=nitermax, Nstates_conv=nconv)
+        X.copy_(torch.from_numpy(np.ascontiguousarray(Xh.T)))
+        return ev, 0
+
+    def calc_rhoe(self, ik, psi, w, rho, accumulate=False):
+        import torch
+        from oracle import ops
+        pw = self.H.pw
+        psiks = [np.zeros((pw.gvecw.Ngw[k], psi.shape[0]), dtype=np.complex128) for k in range(pw.kpoints.Nkpt)]
+        psiks[ik] = psi.numpy().T
+        Focc = np.zeros((psi.shape[0], pw.kpoints.Nkpt))
+        Focc[:, ik] = np.asarray(w) / pw.kpoints.wk[ik]
+        r = torch.from_numpy(ops.calc_rhoe(self.H, psiks, Focc=Focc))
+        if accumulate:
+            rho.add_(r)
+        else:
+            rho.copy_(r)
+
+    def band_energies(self, ik, psi, w):
+        from oracle import ops
+        p = psi.numpy().T
+        Kp = np.zeros_like(p)
+        ops.op_K(self.H, p, Kp, ik)
+        Vp = np.zeros_like(p)
+        ops.op_V_Ps_nloc(self.H, p, Vp, ik)
+        w = np.asarray(w)
+        return np.array([float(np.sum(w * np.real(np.sum(p.conj() * Kp, axis=0)))),
+                         float(np.sum(w * np.real(np.sum(p.conj() * Vp, axis=0))))])
+
+
+class HostHam:
+    """The attributes of pwb200.Hamiltonian the driver reads, host-only."""
+
+    def __init__(self, Ho, meshk):
+        import pwb200
+        from pwb200.system import kpoint_grid
+        k, w = kpoint_grid(Ho.atoms.LatVecs, meshk)
+        self.system = pwb200.System(["Si", "Si"], Ho.atoms.positions, Ho.atoms.LatVecs)
+        self.basis = pwb200.Basis(Ho.atoms.LatVecs, 15.0, kpts=k)
+        self.wk = w
+        from oracle import systems
+        self.pspots = [pwb200.GTH(systems.psp("Si-q4.gth"))]
+        self.Zvals = np.array([4.0])
+        self.Nelectrons = 8.0
+        self.V_Ps_loc = Ho.V_Ps_loc
+        self.sym = None
+        self.ctx = SCFCtx(Ho)
+
+    def setup_density(self):
+        pass

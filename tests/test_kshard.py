@@ -1,7 +1,8 @@
 """k-point sharding (pwb200.kshard): the partition, and the density of a
 2-rank gloo group (each rank sums calc_rhoe over its own k-points, then
 all-reduce) against the single-process sum, on CPU with the oracle's
-calc_rhoe; and on one GPU, the device SCF sharded over 2 gloo ranks
+calc_rhoe; the whole SCF driver on 2 gloo ranks with the NumPy stand-in
+against the single-process driver, on CPU; and on one GPU, the device SCF sharded over 2 gloo ranks
 against the unsharded SCF (the kernels of the two ranks do not wait on
 each other: the exchange is host-side)."""
 import os
@@ -59,6 +60,54 @@ def test_two_rank_density_matches_single(tmp_path):
     mp.start_processes(_rank_density, args=(2, port, out), nprocs=2, start_method="spawn")
     a, b = np.load(out)
     assert np.abs(a - b).max() < 1e-12 * np.abs(b).max()
+
+
+def _rank_scf(rank, world, port, out):
+    """One rank of the SCF driver on the NumPy stand-in, k-points sharded
+    over a gloo group."""
+    import json
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from numpy_ctx import HostHam
+    from oracle import systems, scf as oscf
+    from pwb200 import scf
+    Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    start = oscf.rand_BlochWavefunc(Ho, seed=21)
+    Hd = HostHam(Ho, (2, 2, 2))
+    ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
+    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-8, precision="fp64", psiks=ps)
+    with open(out + ".%d" % rank, "w") as f:
+        json.dump({"E": [r[1] for r in res["log"]], "k": res["kpoints_local"], "evals": res["evals"].tolist()}, f)
+    dist.destroy_process_group()
+
+
+def test_two_rank_scf_matches_single(tmp_path):
+    """The SCF driver's exchange steps (density, band energies, eigenvalues
+    all-reduced over the group; KS_solve_SCF's k loop over this rank's
+    k-points) on 2 gloo ranks reproduce the single-process SCF step by step."""
+    import json
+    import torch
+    import torch.multiprocessing as mp
+    from numpy_ctx import HostHam
+    from oracle import systems, scf as oscf
+    from pwb200 import scf
+    Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    start = oscf.rand_BlochWavefunc(Ho, seed=21)
+    ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
+    ref = scf.KS_solve_SCF(HostHam(Ho, (2, 2, 2)), betamix=0.2, mix_method="pulay", etot_conv_thr=1e-8,
+                           precision="fp64", psiks=ps)
+    out = str(tmp_path / "scf")
+    port = 29700 + os.getpid() % 1000
+    mp.start_processes(_rank_scf, args=(2, port, out), nprocs=2, start_method="spawn")
+    r0, r1 = [json.load(open(out + ".%d" % r)) for r in (0, 1)]
+    assert sorted(r0["k"] + r1["k"]) == list(range(Ho.pw.kpoints.Nkpt)) and r0["k"] and r1["k"]
+    E = [row[1] for row in ref["log"]]
+    for r in (r0, r1):
+        assert len(r["E"]) == len(E)
+        assert np.abs(np.array(r["E"]) - np.array(E)).max() < 1e-10
+        assert np.abs(np.array(r["evals"]) - ref["evals"]).max() < 1e-9
 
 
 SCF_SCRIPT = r'''
