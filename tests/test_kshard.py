@@ -77,7 +77,7 @@ def _rank_scf(rank, world, port, out):
     start = oscf.rand_BlochWavefunc(Ho, seed=21)
     Hd = HostHam(Ho, (2, 2, 2))
     ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
-    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-8, precision="fp64", psiks=ps)
+    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-6, precision="fp64", psiks=ps)
     with open(out + ".%d" % rank, "w") as f:
         json.dump({"E": [r[1] for r in res["log"]], "k": res["kpoints_local"], "evals": res["evals"].tolist()}, f)
     dist.destroy_process_group()
@@ -96,7 +96,7 @@ def test_two_rank_scf_matches_single(tmp_path):
     Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
     start = oscf.rand_BlochWavefunc(Ho, seed=21)
     ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
-    ref = scf.KS_solve_SCF(HostHam(Ho, (2, 2, 2)), betamix=0.2, mix_method="pulay", etot_conv_thr=1e-8,
+    ref = scf.KS_solve_SCF(HostHam(Ho, (2, 2, 2)), betamix=0.2, mix_method="pulay", etot_conv_thr=1e-6,
                            precision="fp64", psiks=ps)
     out = str(tmp_path / "scf")
     port = 29700 + os.getpid() % 1000
