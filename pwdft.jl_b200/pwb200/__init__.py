@@ -174,3 +174,21 @@ def diag_Emin_PCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0, tol_eband
 
 
 __all__ += ["diag_Emin_PCG_"]
+
+
+def KS_solve_SCF_(Ham, **kwargs):
+    """KS_solve_SCF!(Ham; ...) (KS_solve_SCF.jl:24-373): pwb200.scf.KS_solve_SCF
+    (update_psi "LOBPCG" | "davidson" | "CheFSI" | "PCG", precision "fp64" |
+    "mixed", smearing, symmetry, k-point sharding over a process group)."""
+    from .scf import KS_solve_SCF
+    return KS_solve_SCF(Ham, **kwargs)
+
+
+def KS_solve_Emin_PCG_(Ham, psiks=None, **kwargs):
+    """KS_solve_Emin_PCG!(Ham, psiks; ...) (KS_solve_Emin_PCG.jl:27-270):
+    pwb200.emin_scf.KS_solve_Emin_PCG."""
+    from .emin_scf import KS_solve_Emin_PCG
+    return KS_solve_Emin_PCG(Ham, psiks, **kwargs)
+
+
+__all__ += ["KS_solve_SCF_", "KS_solve_Emin_PCG_"]

@@ -108,3 +108,15 @@ def test_lanczos_and_filter_wrappers():
     v0 = torch.ones(16, dtype=torch.complex128)
     assert pwb200.get_ub_lb_lanczos(H, 8, v0=v0) == (5.0, -1.0)
     assert ctx.calls[-1] == ("lanczos", 0, 0, 8, (16,))
+
+
+def test_driver_aliases_forward_arguments(monkeypatch):
+    import pwb200
+    from pwb200 import scf, emin_scf
+    seen = {}
+    monkeypatch.setattr(scf, "KS_solve_SCF", lambda Ham, **kw: seen.setdefault("scf", (Ham, kw)))
+    monkeypatch.setattr(emin_scf, "KS_solve_Emin_PCG", lambda Ham, psiks, **kw: seen.setdefault("emin", (Ham, psiks, kw)))
+    pwb200.KS_solve_SCF_("H", update_psi="PCG", etot_conv_thr=1e-7)
+    pwb200.KS_solve_Emin_PCG_("H", None, i_cg_beta=3)
+    assert seen["scf"] == ("H", {"update_psi": "PCG", "etot_conv_thr": 1e-7})
+    assert seen["emin"] == ("H", None, {"i_cg_beta": 3})
