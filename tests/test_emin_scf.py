@@ -169,3 +169,13 @@ def test_pcg_scf_driver_matches_oracle():
     E_l, _, _ = oscf.KS_solve_SCF(Ho2, psiks=[p.copy() for p in start], betamix=0.2, mix_method="pulay",
                                   etot_conv_thr=1e-7)
     assert abs(res["energies"]["Total"] - E_l["Total"]) < 1e-6
+
+
+def test_scf_rejects_unsupported_choices():
+    from oracle import systems
+    from pwb200 import scf
+    Hd = HostHam(systems.Ham_Si_fcc(meshk=(1, 1, 1)), (1, 1, 1))
+    with pytest.raises(ValueError):
+        scf.KS_solve_SCF(Hd, update_psi="PCG", precision="mixed")
+    with pytest.raises(ValueError):
+        scf.KS_solve_SCF(Hd, update_psi="nonexistent")
