@@ -80,11 +80,16 @@ def scf_comparison(device, seed):
     H = pwb200.Hamiltonian(pwb200.System(["Si"] * pos.shape[1], pos, LL), [PSP], 15.0, device=device)
     nat = pos.shape[1]
     runs = {}
-    # untimed warm-up of both paths (first-use allocations and kernel loads),
-    # so that neither timed run carries the other's one-time costs
+    # launch parameters tuned per precision by the library's autotuner, then
+    # an untimed warm-up of both paths (first-use allocations and kernel
+    # loads), so that neither timed run carries the other's one-time costs
+    tunes = {prec: H.ctx.autotune(0, 480, pwb200.PW_C64 if prec == "mixed" else pwb200.PW_C128)
+             for prec in ("mixed", "fp64")}
     for prec in ("mixed", "fp64"):
+        H.ctx.set_tuning(**tunes[prec][0])
         scf.KS_solve_SCF(H, Nstates=480, betamix=0.2, mix_method="pulay", NiterMax=2, precision=prec, seed=seed)
     for prec in ("mixed", "fp64"):
+        H.ctx.set_tuning(**tunes[prec][0])
         torch.cuda.synchronize()
         res = scf.KS_solve_SCF(H, Nstates=480, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-6 * nat,
                                fp64_switch=1e-5 * nat, precision=prec, seed=seed)
@@ -102,7 +107,8 @@ def scf_comparison(device, seed):
            "dEtot_per_atom": abs(rm["energies"]["Total"] - rd["energies"]["Total"]) / nat,
            "max_devals_occupied": float(np.abs(rm["evals"][:nocc] - rd["evals"][:nocc]).max()),
            "lobpcg_iterations_per_step": {"mixed": [r[4] for r in rm["log"]], "fp64": [r[4] for r in rd["log"]]},
-           "warmup": "2 untimed SCF iterations per precision first"}
+           "warmup": "2 untimed SCF iterations per precision first",
+           "autotune": {p: {"chosen": t[0], **t[1]} for p, t in tunes.items()}}
     del H, runs, rm, rd
     torch.cuda.empty_cache()
     return out
@@ -240,6 +246,11 @@ class ClockSampler:
 
 
 WORKLOADS = {"si64": 160, "si216": 480}   # bands of the op_H microbenchmark per system
+
+
+def workload_name(workload, nbands, ns, ngw, nbeta):
+    return "%s Gamma op_H (K+V_loc+V_Ps_nloc), %d bands, %d^3 grid, Ngw %d, NbetaNL %d" % (
+        "Si64" if workload == "si64" else "Si216", nbands, ns, ngw, nbeta)
 
 
 def build_workload(device, workload="si64"):
@@ -388,28 +399,35 @@ def multik_comparison(device, steps, flush):
             "bytes_per_op_H": nbytes, **res}
 
 
-def cpu_reference(psi, steps, warmup, budget_s):
-    """The FP64 oracle op_H on the host cores: bounded band sample per step."""
-    from oracle import systems, ops
+def reference_workload():
+    """The op_H workload of the GPU arm rebuilt in the FP64 oracle: the same
+    Si64 basis, the same V_loc (V_Ps_loc + the seeded smooth field drawn from
+    the same generator) and the same orthonormal 160-band psi."""
+    from oracle import systems
     H = systems.Ham_Si64(Nstates=NBANDS)
     rng = np.random.default_rng(SEED)
-    # same V_loc as the device arm: V_Ps_loc + the same seeded smooth field
     g = H.pw.gvec
     H.V_Total = H.V_Ps_loc + 0.01 * smooth_field(H.pw.Ns, g.G2, g.idx_g2r, rng)
-    nsamp = 16
-    x = psi[:, :nsamp].copy()
-    ops.op_H(H, x, 0)  # warm FFT plans
+    psi = orthonormal_psi(H.pw.gvecw.Ngw[0], NBANDS, rng)
+    return H, psi
+
+
+def cpu_reference(H, psi, steps, warmup, budget_s=None):
+    """The FP64 oracle op_H (the reference's per-band FFT loop restated in
+    NumPy/SciPy) on the host cores, all 160 bands per step: `warmup` untimed
+    steps, then `steps` timed ones (fewer if budget_s seconds run out).
+    Returns (seconds per step, steps timed)."""
+    from oracle import ops
+    for _ in range(max(1, warmup)):
+        ops.op_H(H, psi, 0)
+    n = 0
     t0 = time.perf_counter()
-    ops.op_H(H, x, 0)
-    t_one = time.perf_counter() - t0
-    reps = max(1, min(steps, int(budget_s / max(t_one, 1e-3))))
-    for _ in range(min(warmup, 1)):
-        ops.op_H(H, x, 0)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        ops.op_H(H, x, 0)
-    dt = (time.perf_counter() - t0) / reps
-    return dt, nsamp, reps
+    while n < steps:
+        ops.op_H(H, psi, 0)
+        n += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
+    return (time.perf_counter() - t0) / n, n
 
 
 def main():
@@ -432,22 +450,20 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        rng = np.random.default_rng(SEED)
-        from oracle import pwgrid
-        LL, _ = si64_geometry()
-        pw = pwgrid.PWGrid(15.0, LL)
-        psi = orthonormal_psi(pw.gvecw.Ngw[0], NBANDS, np.random.default_rng(SEED + 1))
-        dt, nsamp, reps = cpu_reference(psi, args.steps, args.warmup, args.cpu_budget)
+        H, psi = reference_workload()
+        pw = H.pw
         bpb, _ = byte_model(pw.Ns, pw.gvecw.idx_gw2r[0], NBANDS)
-        val = nsamp * bpb / dt / 1e9
+        dt, reps = cpu_reference(H, psi, args.steps, args.warmup)
+        val = NBANDS * bpb / dt / 1e9
         out = {"impl": "reference", "metric": METRIC, "value": val, "unit": "GB/s", "n_gpus": args.gpus,
-               "steps": reps, "warmup": args.warmup, "ms_per_step": dt * 1e3 * NBANDS / nsamp,
+               "steps": reps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
                "data": "synthetic",
-               "config": {"workload": "Si64 Gamma op_H, 160 bands, 75^3 grid (CPU sample of %d bands)" % nsamp,
+               "config": {"workload": workload_name("si64", NBANDS, pw.Ns[0], pw.gvecw.Ngw[0], H.NbetaNL),
                           "global_batch": NBANDS, "seq_len": 0, "parallelism": "cpu"},
                "cpu_baseline": {"value": val, "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
-                                "sample": "%d of 160 bands per step, %d steps" % (nsamp, reps)},
+                                "sample": "all 160 bands per step, %d timed steps after %d warm-up steps, "
+                                          "FP64 NumPy/SciPy, all host threads" % (reps, args.warmup)},
                "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
         return
@@ -476,6 +492,10 @@ def main():
     y32, y64 = torch.empty_like(x32), torch.empty_like(x64)
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
     OPS = pwb200.PW_OP_H
+    # launch parameters from the library's autotuner (timed candidates, no
+    # cache file): the mixed-precision path is tuned before its timing, the
+    # FP64 path before its own
+    tune_mixed = ctx.autotune(0, nbands, pwb200.PW_C64)
 
     if dist:
         dist.barrier()
@@ -486,6 +506,7 @@ def main():
     n1 = ctx._L.pw_launch_count(ctx.h)
     launches = (n1 - n0) * args.steps // (args.steps + args.warmup)
     t_fft = time_device(ctx, x32, y32, pwb200.PW_OP_VLOC, args.steps, args.warmup, flush)
+    tune_fp64 = ctx.autotune(0, nbands, pwb200.PW_C128)
     t_fp64 = time_device(ctx, x64, y64, OPS, max(10, args.steps // 4), args.warmup, flush)
     torch.cuda.synchronize()
     ms = sum(t_mixed) / len(t_mixed)
@@ -496,6 +517,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms, ms_fft, ms64 = [float(v) for v in t.tolist()]
 
+    ctx.set_tuning(**tune_mixed[0])
     rr = time_rayleigh_ritz(ctx, x32, nbands, max(5, args.steps // 20), flush)
     rr["eigh"] = time_eigh(ctx, nbands, max(3, args.steps // 40))
 
@@ -517,10 +539,19 @@ def main():
     for _ in range(e2e_steps):
         ctx.op_H_host(0, 0, a_in, a_out, OPS, pwb200.PW_C64)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
+    # the same host call on the reference's precision (FP64 end to end)
+    ctx.set_tuning(**tune_fp64[0])
+    for _ in range(args.warmup):
+        ctx.op_H_host(0, 0, a_in, a_out, OPS, pwb200.PW_C128)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.op_H_host(0, 0, a_in, a_out, OPS, pwb200.PW_C128)
+    e2e64_s = (time.perf_counter() - t0) / e2e_steps
+    ctx.set_tuning(**tune_mixed[0])
     if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        t = torch.tensor([e2e_s, e2e64_s], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s, e2e64_s = [float(v) for v in t.tolist()]
 
     hbm, peak_kind = peaks()
     fft_gbs = step_bytes / (ms_fft * 1e-3) / 1e9
@@ -537,9 +568,8 @@ def main():
         "vs_baseline": None,
         "dtype": "c64",
         "data": "synthetic",
-        "config": {"workload": "%s Gamma op_H (K+V_loc+V_Ps_nloc), %d bands, %d^3 grid, Ngw %d, NbetaNL %d" % (
-                               "Si64" if args.workload == "si64" else "Si216", nbands, H.basis.Ns[0],
-                               H.basis.Ngw[0], H.NbetaNL), "global_batch": nbands * world, "seq_len": 0,
+        "config": {"workload": workload_name(args.workload, nbands, H.basis.Ns[0], H.basis.Ngw[0], H.NbetaNL),
+                   "global_batch": nbands * world, "seq_len": 0,
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed between steps (256 MB write)", "bytes_per_band": bpb, "nx_active": nxa},
         "fp64_ms_per_step": ms64,
@@ -548,6 +578,14 @@ def main():
         "e2e": {"value": world * step_bytes / e2e_s / 1e9, "unit": "GB/s",
                 "h2d_bytes_per_step": int(psi.size * 16), "d2h_bytes_per_step": int(psi.size * 16),
                 "ms_per_step": e2e_s * 1e3},
+        "e2e_fp64": {"value": world * step_bytes / e2e64_s / 1e9, "unit": "GB/s",
+                     "h2d_bytes_per_step": int(psi.size * 16), "d2h_bytes_per_step": int(psi.size * 16),
+                     "ms_per_step": e2e64_s * 1e3, "dtype": "c128",
+                     "note": "pw_op_H_host computing in FP64, the reference's precision"},
+        "autotune": {"mixed": {"chosen": tune_mixed[0], **tune_mixed[1]},
+                     "fp64": {"chosen": tune_fp64[0], **tune_fp64[1]},
+                     "note": "pw_autotune on this workload before the timed arms; ms of op_H and of the "
+                             "Rayleigh-Ritz Gram + rotation with the default and the chosen parameters"},
         "roofline": {"bound": "hbm", "achieved": fft_gbs, "peak": hbm, "unit": "GB/s", "frac": fft_gbs / hbm,
                      "traffic": FFT_TRAFFIC_BYTES.get(args.workload), "peak_kind": peak_kind,
                      "kernel": "op_V_loc pruned-FFT round trip (K-zinv+K-plane+K-zfwd), %.4f ms" % ms_fft},
@@ -563,10 +601,12 @@ def main():
     if os.environ.get("PW_BENCH_NO_MULTIK") != "1" and world == 1:
         out["multik"] = multik_comparison(local, max(5, args.steps // 20), flush)
     if rank == 0 and world == 1 and args.workload == "si64" and os.environ.get("PW_BENCH_NO_CPU") != "1":
-        dt, nsamp, reps = cpu_reference(psi, 1000, 1, args.cpu_budget)
-        v = nsamp * bpb / dt / 1e9
+        Hc, psic = reference_workload()
+        dt, reps = cpu_reference(Hc, psic, 1000, 1, args.cpu_budget)
+        v = NBANDS * bpb / dt / 1e9
         out["cpu_baseline"] = {"value": v, "unit": "GB/s", "cores": os.cpu_count(), "kind": "port",
-                               "sample": "%d of 160 bands per op_H, %d repetitions, FP64 NumPy/SciPy" % (nsamp, reps)}
+                               "sample": "all 160 bands per op_H, %d repetitions (about %.0f s), FP64 NumPy/SciPy, "
+                                         "all host threads" % (reps, args.cpu_budget)}
     if rank == 0:
         print(json.dumps(out))
     ctx.close()

@@ -87,6 +87,40 @@ int64_t     pw_launch_count(const pw_ctx *ctx);
  * reference, whose BLAS calls cannot time out). */
 int         pw_check_device(pw_ctx *ctx);
 
+/* Launch parameters of a context's kernels.  No counterpart in the
+ * reference: there FFTW's planner and the BLAS pick their own blockings.
+ * A zero field means "the built-in default"; pw_set_tuning replaces all
+ * fields at once (read them with pw_get_tuning first to change one);
+ * pw_get_tuning reports the band batch in effect (48 MiB by default). */
+typedef struct pw_tuning {
+    int64_t band_chunk_bytes; /* FFT intermediate of one band batch (default 48 MiB)             */
+    int32_t plane_bands;      /* bands of one z-plane per CTA, FP32 plane pass: 1..3
+                                 (default 3 on 75-point grids, else 1)                           */
+    int32_t z_columns;        /* grid columns per CTA of the z passes, 1..256 (default: 64 for
+                                 FP32, about 48 KB of shared memory for FP64)                    */
+    int32_t gemm_splits;      /* split-K count of the tensor-core Gram and rotation, 0..64
+                                 (0: enough CTAs to fill the GPU twice)                          */
+    int32_t reserved[5];      /* must be zero                                                    */
+} pw_tuning;
+int pw_get_tuning(const pw_ctx *ctx, pw_tuning *t);
+int pw_set_tuning(pw_ctx *ctx, const pw_tuning *t);
+
+/* Autotuner of the launch parameters above for op_H (PW_OP_H) of k-point
+ * ik on nb bands of dtype and, for PW_C64 with nb > 0, the Rayleigh-Ritz
+ * Gram (3 nb x 3 nb over Ngw[ik]) and rotation (Ngw x 3nb -> nb).  Every
+ * candidate is timed with CUDA events on the context stream on seeded
+ * blocks the call allocates and frees; the fastest set is applied to the
+ * context and written to *chosen.  cache_path (NULL: the environment
+ * variable PW_AUTOTUNE_CACHE, or no cache if unset) names a text file of
+ * earlier choices keyed by GPU name, grid, Ngw, active columns and x
+ * planes, nb, dtype and projector count: a hit applies the stored choice
+ * without timing, a miss appends the new one.  ms (host, 4 doubles, may be
+ * NULL) receives {op_H default, op_H tuned, Gram+rotation default,
+ * Gram+rotation tuned} in milliseconds (negative when not timed, e.g. on a
+ * cache hit).  No counterpart in the reference. */
+int pw_autotune(pw_ctx *ctx, int ik, int nb, int dtype, const char *cache_path,
+                pw_tuning *chosen, double *ms);
+
 /* V_loc(r) = Ham.potentials.Total[:, ispin] (Hamiltonian.jl:542), host
  * FP64, N x nspin column-major.  Replaces the potential read by
  * op_V_loc.jl:127. */
@@ -166,12 +200,14 @@ int pw_rotate(pw_ctx *ctx, int dtype, int64_t M, int n, int k, const void *A,
  * device synchronisation of cudaMalloc/cudaFree.  pw_apply may grow its
  * intermediate buffer on first use or when nb grows; this call never does.
  * Its intermediate is one file-scope device array of
- * pw_noalloc_scratch_bytes() (32 MiB) that every GPU loading the library
- * holds until exit; bands are processed in batches that fit, and a grid
- * whose single band needs more returns PW_ERR_UNSUPPORTED.  The first call
- * on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the array, so calls whose
- * work overlaps on the GPU (other streams, other contexts) race. */
+ * pw_noalloc_scratch_bytes() (32 MiB).  pw_create looks up the array's
+ * device address on its device, which loads it there: from the first
+ * pw_create on a GPU the 32 MiB stay reserved until the process exits (so
+ * create the context before a pooling allocator takes the GPU's memory),
+ * and this call itself reserves nothing.  Bands are processed in batches
+ * that fit, and a grid whose single band needs more returns
+ * PW_ERR_UNSUPPORTED.  All calls share the array, so calls whose work
+ * overlaps on the GPU (other streams, other contexts) race. */
 int      pw_apply_vloc_noalloc(pw_ctx *ctx, int ik, int ispin, int dtype,
                                const void *psi, void *Hpsi, int64_t ld,
                                int nb, unsigned ops);

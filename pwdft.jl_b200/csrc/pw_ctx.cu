@@ -18,6 +18,8 @@
 
 using namespace pwk;
 
+void pwk_noalloc_prepare(int dev);   // pw_noalloc.cu
+
 namespace {
 
 thread_local std::string g_create_error;
@@ -85,6 +87,9 @@ struct pw_ctx {
     DevBuf A, P, P2, gemm_ws, rho_part, w, st_in, st_out, st_in32, st_out32, st_rho;
     std::vector<void *> allocs;
     size_t a_chunk_bytes = 48ull << 20;
+    int plane_bpc = 0;        // bands per CTA of the FP32 plane kernels (0: per-grid default)
+    int z_cols = 0;           // columns per CTA of the z passes (0: the 48 KB default)
+    int gemm_splits = 0;      // split-K of the tensor-core GEMMs (0: automatic)
     bool use_umma = true;     // mixed-precision contractions on tcgen05 (PW_GEMM=cuda: CUDA cores)
     int *d_err = nullptr;     // device error word of the bounded waits in the tensor-core kernels
     DevBuf um_a_hi, um_a_lo, um_b_hi, um_b_lo, um_b_lo2, um_ws;
@@ -302,6 +307,12 @@ FftLaunch make_launch_kd(const pw_ctx *c, const KData &kd) {
     // z passes: ~48 KB of shared memory per CTA
     int Cg = (int)((48 * 1024 / es - c->N3) / c->N3);
     L.Cg = std::max(1, std::min(64, Cg));
+    if (c->z_cols > 0) {
+        // at most ~190 KB of shared memory per z-pass CTA
+        const int cmax = std::max(1, (int)((190 * 1024 / es - c->N3) / c->N3) - 16);
+        L.Cg = std::min(c->z_cols, cmax);
+    }
+    L.bpc = c->plane_bpc > 0 ? c->plane_bpc : (c->N1 == 75 ? 3 : 1);
     // plane passes: a 100 KB budget (two CTAs per SM) when it holds at
     // least 16 full x lines, otherwise up to 220 KB
     const size_t fixed = (size_t)c->N1 + c->N2 + (size_t)kd.Nxa * c->N2;
@@ -325,6 +336,7 @@ int band_chunk(const pw_ctx *c, int ik, size_t es, int nb) {
     const size_t per_band = (size_t)c->N3 * c->k[ik].Ncol * es;
     size_t ch = c->a_chunk_bytes / std::max<size_t>(per_band, 1);
     if (ch < 1) ch = 1;
+    if (ch > 65535) ch = 65535;   // bands are blockIdx.y of the z passes
     return (int)std::min<size_t>(ch, (size_t)nb);
 }
 
@@ -355,9 +367,9 @@ int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, cons
         return s;
     CK(c, umma_prep_tn_a<float2>(Z, ldz, K, m, A, c->stream));
     CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
-    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp)))) return s;
+    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp, c->gemm_splits)))) return s;
     const int same = (Z == Wm && ldz == ldw && m == n);   // Z^H Z: add the lo*lo product
-    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper, same));
+    CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper, same, c->gemm_splits));
     c->launches += 4;
     return PW_OK;
 }
@@ -376,8 +388,9 @@ int umma_nn(pw_ctx *c, int64_t M, int n, int k, const void *A, int64_t lda, cons
     }
     if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, n, k, B))) return s;
     CK(c, umma_prep_tn_b<double2>(U, ldu, k, n, B, c->stream));
-    if ((s = ensure(c, c->um_ws, umma_ws_bytes(Ao.rows, n, Ao.Kp)))) return s;
-    CK(c, umma_gemm<float2>(Ao, B, (int)M, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream));
+    if ((s = ensure(c, c->um_ws, umma_ws_bytes(Ao.rows, n, Ao.Kp, c->gemm_splits)))) return s;
+    CK(c, umma_gemm<float2>(Ao, B, (int)M, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, 0, 0,
+                            c->gemm_splits));
     c->launches += 3;
     return PW_OK;
 }
@@ -528,6 +541,7 @@ extern "C" int pw_create(int device, const pw_grid_desc *d, pw_ctx **out) {
         st = fail(nullptr, PW_ERR_UNSUPPORTED, "grid %dx%dx%d: every dimension must factor into 2,3,5 and fit one warp per line (<= 160 with a factor 5)",
                   c->N1, c->N2, c->N3);
     }
+    if (!st) pwk_noalloc_prepare(device);
     if (!st) {
         e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) st = fail(nullptr, PW_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
@@ -586,6 +600,32 @@ extern "C" int pw_set_stream(pw_ctx *c, void *stream) {
 }
 
 extern "C" int64_t pw_launch_count(const pw_ctx *c) { return c ? c->launches : -1; }
+
+extern "C" int pw_get_tuning(const pw_ctx *c, pw_tuning *t) {
+    if (!c || !t) return PW_ERR_ARG;
+    std::memset(t, 0, sizeof(*t));
+    t->band_chunk_bytes = (int64_t)c->a_chunk_bytes;
+    t->plane_bands = c->plane_bpc;
+    t->z_columns = c->z_cols;
+    t->gemm_splits = c->gemm_splits;
+    return PW_OK;
+}
+
+extern "C" int pw_set_tuning(pw_ctx *c, const pw_tuning *t) {
+    if (!c) return PW_ERR_ARG;
+    if (!t) return fail(c, PW_ERR_ARG, "tuning is NULL");
+    for (int i = 0; i < 5; ++i)
+        if (t->reserved[i]) return fail(c, PW_ERR_ARG, "pw_tuning.reserved[%d] must be zero", i);
+    if (t->band_chunk_bytes < 0 || t->plane_bands < 0 || t->plane_bands > 3 || t->z_columns < 0 ||
+        t->z_columns > 256 || t->gemm_splits < 0 || t->gemm_splits > 64)
+        return fail(c, PW_ERR_ARG, "tuning out of range: chunk %lld, plane_bands %d, z_columns %d, gemm_splits %d",
+                    (long long)t->band_chunk_bytes, t->plane_bands, t->z_columns, t->gemm_splits);
+    c->a_chunk_bytes = t->band_chunk_bytes > 0 ? (size_t)t->band_chunk_bytes : (48ull << 20);
+    c->plane_bpc = t->plane_bands;
+    c->z_cols = t->z_columns;
+    c->gemm_splits = t->gemm_splits;
+    return PW_OK;
+}
 
 extern "C" int pw_check_device(pw_ctx *c) {
     if (!c) return PW_ERR_ARG;
@@ -1074,6 +1114,19 @@ int pwk_vloc_view(pw_ctx *c, int ik, int ispin, int dtype, pwk::FftLaunch *L, co
 }
 
 int pwk_ngw(const pw_ctx *c, int ik) { return c->k[ik].Ngw; }
+
+// Shape of k-point ik for the autotuner's cache key.
+int pwk_tune_shape(const pw_ctx *c, int ik, int *Ns, int *Ncol, int *Nxa, int *nbeta) {
+    if (ik < 0 || ik >= c->Nkpt) return PW_ERR_ARG;
+    Ns[0] = c->N1;
+    Ns[1] = c->N2;
+    Ns[2] = c->N3;
+    *Ncol = c->k[ik].Ncol;
+    *Nxa = c->k[ik].Nxa;
+    *nbeta = (c->nbeta > 0 && c->have_D) ? c->nbeta : 0;
+    return PW_OK;
+}
+int pwk_fail_msg(pw_ctx *c, int code, const char *msg) { return fail(c, code, "%s", msg); }
 
 int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out) {
     if (slot < 0 || slot >= 32) return fail(c, PW_ERR_ARG, "scratch slot %d", slot);

@@ -54,16 +54,24 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+// Failure-detection test hooks, written only through pwk_test_gsync (a
+// test-only export): the poll limit of every wait, and one CTA that withholds
+// its arrivals so that the others' waits run out.  The library itself never
+// changes them.
+__device__ long long g_gsync_limit = GSYNC_LIMIT;
+__device__ int g_gsync_withhold = -1;
+
 __device__ __forceinline__ void gsync(unsigned *ctr, unsigned &tgt, int *err) {
     __syncthreads();
     tgt += gridDim.x;
     if (threadIdx.x == 0) {
         __threadfence();
-        atomicAdd(ctr, 1u);
+        if ((int)blockIdx.x != g_gsync_withhold) atomicAdd(ctr, 1u);
         if (!*(volatile int *)err) {
+            const long long lim = g_gsync_limit;
             long long it = 0;
             while (ld_acquire_u32(ctr) < tgt) {
-                if (++it > GSYNC_LIMIT) {
+                if (++it > lim) {
                     atomicExch(err, 1);
                     break;
                 }
@@ -905,3 +913,15 @@ cudaError_t chol_inverse_upper(double2 *C, int n, double2 *Rinv, void *work, int
 }
 
 }  // namespace pwk
+
+// Test-only export (not in pwb200.h): sets the grid-barrier poll limit
+// (limit <= 0 restores the default) and the CTA that withholds its arrivals
+// (-1: none) on `device`, for the tests that make a bounded wait expire
+// without faulting or hanging the GPU.
+extern "C" int pwk_test_gsync(int device, long long limit, int withhold_cta) {
+    if (cudaSetDevice(device) != cudaSuccess) return 2;
+    const long long lim = limit > 0 ? limit : pwk::eig::GSYNC_LIMIT;
+    if (cudaMemcpyToSymbol(pwk::eig::g_gsync_limit, &lim, sizeof(lim)) != cudaSuccess) return 2;
+    if (cudaMemcpyToSymbol(pwk::eig::g_gsync_withhold, &withhold_cta, sizeof(withhold_cta)) != cudaSuccess) return 2;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
+}

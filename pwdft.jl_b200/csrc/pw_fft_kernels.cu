@@ -958,26 +958,35 @@ cudaError_t launch_zfwd(const FftLaunch &L, const void *A, const void *psi, void
 }
 
 // FP32 fixed sizes: the x-fused kernel (V(r) kept in shared memory when
-// the plane takes at most 32 KB)
-template <int NN>
-static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
+// the plane takes at most 32 KB), BPC sub-planes per CTA
+template <int NN, int BPC>
+static cudaError_t launch_plane_vloc_xb(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
     const KPlan &kp = L.kp;
     constexpr bool VS = NN * NN * 4 <= 32 * 1024;
-    // sub-planes per CTA, measured: 3 on the 75-point grid (Si64 round trip
-    // 0.996 -> 0.843 ms); 1 on the 120-point grid, where two CTAs per SM
-    // (103 KB each) beat two sub-planes in one CTA once the padded layout
-    // removed the bank conflicts (Si216 10.0 -> 8.7 ms)
-    constexpr int BPC = NN == 75 ? 3 : 1;
     PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
     ps.bands = BPC;
     ps.xs = pwf::fp_xs<NN>();
     const size_t smem = ps.elems() * sizeof(float2);
+    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS, BPC>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid(kp.N3, (nb + BPC - 1) / BPC);
     kx_plane_vloc<NN, NN, VS, BPC><<<grid, FFT_THREADS, smem, st>>>(kp, (const float2 *)L.twx, (const float2 *)L.twy,
                                                                    (const float *)Vr, (float2 *)A, nb);
     return cudaGetLastError();
+}
+// sub-planes per CTA (L.bpc), measured defaults: 3 on the 75-point grid
+// (Si64 round trip 0.996 -> 0.843 ms); 1 on the 120-point grid, where two
+// CTAs per SM (103 KB each) beat two sub-planes in one CTA once the padded
+// layout removed the bank conflicts (Si216 10.0 -> 8.7 ms)
+template <int NN>
+static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
+    switch (L.bpc) {
+        case 1: return launch_plane_vloc_xb<NN, 1>(L, Vr, A, nb, st);
+        case 2: return launch_plane_vloc_xb<NN, 2>(L, Vr, A, nb, st);
+        case 3: return launch_plane_vloc_xb<NN, 3>(L, Vr, A, nb, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 template <int NN>
 static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb, int G, int Bg, const double *w,

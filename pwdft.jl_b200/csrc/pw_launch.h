@@ -33,6 +33,7 @@ struct FftLaunch {
     const void *twx, *twy, *twz;  // twiddle tables of the launch precision
     int Cg;                       // columns per CTA in the z passes
     int Jc;                       // y lines per x chunk in the plane passes
+    int bpc = 1;                  // bands of one z-plane per CTA in the FP32 plane pass (1..3)
 };
 
 template <typename T> cudaError_t launch_zinv(const FftLaunch &, const void *psi, int64_t ld, int nb, void *A, cudaStream_t);

@@ -2,6 +2,7 @@
 // its band-batch intermediate held in a fixed, file-scope device array
 // instead of memory the context allocates.  For callers that must not call
 // cudaMalloc/cudaFree on this path (see include/pwb200.h).
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/pwb200.h"
@@ -28,25 +29,53 @@ void *g_scratch_addr[kMaxDevices] = {};
 
 // The device address of g_noalloc_scratch on `dev` (which must be the current
 // device).  Host code cannot use the symbol itself: it names a host-side
-// stand-in, not device memory.  Looked up once per device.
-int scratch_address(pw_ctx *c, int dev, void **out) {
-    if (dev < 0 || dev >= kMaxDevices) return pwk_fail(c, PW_ERR_ARG, "device index beyond the no-alloc table");
+// stand-in, not device memory.  The lookup also loads the array's module on
+// that device (under CUDA's lazy module loading this is the moment its bytes
+// are reserved), so pw_create calls it with refresh = true for its device:
+// the reservation happens when a context is built, not on the first
+// allocation-free call, and a context built after a device reset records the
+// new address.
+int lookup_scratch(int dev, bool refresh, void **out) {
+    if (dev < 0 || dev >= kMaxDevices) return PW_ERR_ARG;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_addr[dev]) {
+    if (refresh || !g_scratch_addr[dev]) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return pwk_fail(c, PW_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch) failed");
+        if (e != cudaSuccess || !p) {
+            g_scratch_addr[dev] = nullptr;
+            return PW_ERR_CUDA;
+        }
         g_scratch_addr[dev] = p;
     }
     *out = g_scratch_addr[dev];
     return PW_OK;
 }
 
+int scratch_address(pw_ctx *c, int dev, void **out) {
+    if (dev < 0 || dev >= kMaxDevices) return pwk_fail(c, PW_ERR_ARG, "device index beyond the no-alloc table");
+    if (lookup_scratch(dev, false, out) != PW_OK)
+        return pwk_fail(c, PW_ERR_CUDA, "cudaGetSymbolAddress(no-alloc scratch) failed");
+    return PW_OK;
+}
+
+}  // namespace
+
+// Called by pw_create with `dev` current: reserves the array on that device
+// now.  A failure here is not fatal to the context; the allocation-free
+// entry point then reports it when it is called.
+void pwk_noalloc_prepare(int dev) {
+    void *p = nullptr;
+    (void)lookup_scratch(dev, true, &p);
+}
+
+namespace {
+
 template <typename T>
 int run(pw_ctx *c, const pwk::FftLaunch &L, const void *V, cudaStream_t st, void *A, size_t per_band, const void *psi,
         void *Hpsi, int64_t ld, int nb, int flags) {
     const size_t es = 2 * sizeof(T);
-    const int nbc = (int)(PW_NOALLOC_SCRATCH_BYTES / per_band);
+    // bands are blockIdx.y of the z passes: at most 65535 per batch
+    const int nbc = (int)std::min<size_t>(PW_NOALLOC_SCRATCH_BYTES / per_band, 65535);
     for (int b0 = 0; b0 < nb; b0 += nbc) {
         const int cnt = nb - b0 < nbc ? nb - b0 : nbc;
         const char *pin = (const char *)psi + (size_t)b0 * ld * es;

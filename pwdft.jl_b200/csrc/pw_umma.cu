@@ -513,14 +513,17 @@ cudaError_t umma_prep_nn_a(const void *A, int64_t lda, int64_t M, int k, UmmaOpe
 
 // Split-K count: enough CTAs to fill the GPU.  (Accuracy does not depend
 // on it: each k-block is its own accumulation chain in TMEM.)
-int umma_splits(int64_t Mp, int Np, int Kp) {
-    const int tiles = (int)((Mp + BM - 1) / BM) * ((Np + BN - 1) / BN);
+int umma_splits(int64_t Mp, int Np, int Kp, int splits = 0) {
     const int KB = Kp / BK;
+    if (splits > 0) return std::max(1, std::min(splits, KB));
+    const int tiles = (int)((Mp + BM - 1) / BM) * ((Np + BN - 1) / BN);
     int S = (2 * 148 + tiles - 1) / tiles;
     return std::max(1, std::min(S, KB / 4 > 0 ? KB / 4 : 1));
 }
 
-size_t umma_ws_bytes(int64_t Mp, int Np, int Kp) { return (size_t)umma_splits(Mp, Np, Kp) * Mp * Np * sizeof(float); }
+size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits) {
+    return (size_t)umma_splits(Mp, Np, Kp, splits) * Mp * Np * sizeof(float);
+}
 
 template <int NS>
 static cudaError_t launch_umma(const CUtensorMap *mA, const CUtensorMap *mB, dim3 grid, int Mp, int n, int KB, int kb_per,
@@ -538,7 +541,7 @@ static cudaError_t launch_umma(const CUtensorMap *mA, const CUtensorMap *mB, dim
 
 template <typename CT>
 cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
-                      float *ws, int *err, cudaStream_t st, int upper, int lolo) {
+                      float *ws, int *err, cudaStream_t st, int upper, int lolo, int splits) {
     cudaError_t e = get_encoder();
     if (e != cudaSuccess) return e;
     if (A.Kp != B.Kp || A.rows != 2 * (int64_t)m || B.rows != n) return cudaErrorInvalidValue;
@@ -552,7 +555,7 @@ cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, 
         if ((e = make_map(&mB[q], pb[q], B.rows, B.Kp, BN)) != cudaSuccess) return e;
     }
     const int KB = A.Kp / BK;
-    const int S = umma_splits(A.rows, n, A.Kp);
+    const int S = umma_splits(A.rows, n, A.Kp, splits);
     const int kb_per = (KB + S - 1) / S;
     dim3 grid((unsigned)((A.rows + BM - 1) / BM), (n + BN - 1) / BN, S);
     e = ns == 3 ? launch_umma<3>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, 0, st)
@@ -567,8 +570,8 @@ template cudaError_t umma_prep_tn_b<float2>(const void *, int64_t, int64_t, int,
 template cudaError_t umma_prep_tn_b<double2>(const void *, int64_t, int64_t, int, UmmaOperand &, cudaStream_t);
 template cudaError_t umma_prep_nn_a<float2>(const void *, int64_t, int64_t, int, UmmaOperand &, cudaStream_t);
 template cudaError_t umma_gemm<float2>(const UmmaOperand &, const UmmaOperand &, int, int, void *, int64_t, int, float *,
-                                       int *, cudaStream_t, int, int);
+                                       int *, cudaStream_t, int, int, int);
 template cudaError_t umma_gemm<double2>(const UmmaOperand &, const UmmaOperand &, int, int, void *, int64_t, int, float *,
-                                        int *, cudaStream_t, int, int);
+                                        int *, cudaStream_t, int, int, int);
 
 }  // namespace pwk

@@ -20,7 +20,8 @@ struct UmmaOperand {
 
 int umma_kpad(int64_t K);                          // padded 2K (multiple of 64)
 size_t umma_operand_bytes(int64_t rows, int64_t K);  // hi + lo bytes for `rows` rows (one piece: half)
-size_t umma_ws_bytes(int64_t Mp, int Np, int Kp);    // split-K workspace
+// split-K workspace; splits > 0 overrides the automatic split count
+size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits = 0);
 
 // Operand builders (CT = float2 or double2 input element).
 //   tn_a: A' (2m rows) from Z (K x m)          for C = Z^H W
@@ -37,6 +38,6 @@ template <typename CT>
 // lolo != 0 (two-piece operands from the same block, C = Z^H Z): add the
 // lo*lo product, whose omission biases the diagonal |z|^2 low.
 cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, void *C, int64_t ldc, int accumulate,
-                      float *ws, int *err, cudaStream_t, int upper = 0, int lolo = 0);
+                      float *ws, int *err, cudaStream_t, int upper = 0, int lolo = 0, int splits = 0);
 
 }  // namespace pwk

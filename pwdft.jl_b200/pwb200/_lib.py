@@ -37,6 +37,11 @@ class pw_grid_desc(C.Structure):
                 ("idx_gw2r", C.POINTER(C.POINTER(C.c_int64))), ("Gk2", C.POINTER(C.POINTER(C.c_double)))]
 
 
+class pw_tuning(C.Structure):
+    _fields_ = [("band_chunk_bytes", C.c_int64), ("plane_bands", C.c_int32), ("z_columns", C.c_int32),
+                ("gemm_splits", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
 _vp, _i, _i64, _d, _u = C.c_void_p, C.c_int, C.c_int64, C.c_double, C.c_uint
 _dp = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
@@ -52,6 +57,9 @@ SIGNATURES = {
     "pw_synchronize": (_i, [_vp]),
     "pw_launch_count": (_i64, [_vp]),
     "pw_check_device": (_i, [_vp]),
+    "pw_get_tuning": (_i, [_vp, C.POINTER(pw_tuning)]),
+    "pw_set_tuning": (_i, [_vp, C.POINTER(pw_tuning)]),
+    "pw_autotune": (_i, [_vp, _i, _i, _i, C.c_char_p, C.POINTER(pw_tuning), _dp]),
     "pw_set_vloc": (_i, [_vp, _dp, _i]),
     "pw_set_vloc_device": (_i, [_vp, _vp, _i]),
     "pw_set_nonlocal": (_i, [_vp, _i, _dp, _i]),

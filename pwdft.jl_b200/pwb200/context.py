@@ -9,7 +9,9 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (lib, check, pw_grid_desc, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE, PW_GRAPH)
+from ._lib import (lib, check, pw_grid_desc, pw_tuning, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE, PW_GRAPH)
+
+TUNING_FIELDS = ("band_chunk_bytes", "plane_bands", "z_columns", "gemm_splits")
 
 _dp = C.POINTER(C.c_double)
 
@@ -89,6 +91,38 @@ class Context:
 
     def launch_count(self):
         return int(self._L.pw_launch_count(self.h))
+
+    # ------------------------------------------------------------- tuning
+    def get_tuning(self):
+        """The context's launch parameters (pw_tuning) as a dict; 0 = default."""
+        t = pw_tuning()
+        self._chk(self._L.pw_get_tuning(self.h, C.byref(t)))
+        return {f: int(getattr(t, f)) for f in TUNING_FIELDS}
+
+    def set_tuning(self, **kw):
+        """Change some launch parameters (the others keep their values)."""
+        cur = self.get_tuning()
+        for k, v in kw.items():
+            if k not in cur:
+                raise KeyError("unknown tuning field %r" % k)
+            cur[k] = int(v)
+        t = pw_tuning()
+        for f in TUNING_FIELDS:
+            setattr(t, f, cur[f])
+        self._chk(self._L.pw_set_tuning(self.h, C.byref(t)))
+
+    def autotune(self, ik, nb, dtype=PW_C64, cache_path=None):
+        """pw_autotune: time candidate launch parameters for op_H on nb bands of
+        k-point ik (and the Rayleigh-Ritz products for PW_C64), apply the
+        fastest.  Returns (tuning dict, {op_H_default_ms, op_H_tuned_ms,
+        rr_default_ms, rr_tuned_ms}); a cache hit reports -1 timings."""
+        t = pw_tuning()
+        ms = np.zeros(4)
+        self.use_torch_stream()
+        self._chk(self._L.pw_autotune(self.h, int(ik), int(nb), int(dtype),
+                                      None if cache_path is None else str(cache_path).encode(), C.byref(t), _dptr(ms)))
+        names = ("op_H_default_ms", "op_H_tuned_ms", "rr_default_ms", "rr_tuned_ms")
+        return {f: int(getattr(t, f)) for f in TUNING_FIELDS}, dict(zip(names, ms.tolist()))
 
     # ------------------------------------------------------------ set-up
     def set_vloc(self, V):

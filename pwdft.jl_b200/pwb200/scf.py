@@ -5,11 +5,10 @@ density mixing):
   ethr schedule            KS_solve_SCF.jl:177-185
   diag_LOBPCG!             pw_lobpcg per k-point          (device, update_psi="LOBPCG"), or
                            pw_lobpcg_multi for all k-points together (batched=True, nb <= 16)
-  diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson";
-                           the call of electrons_scf.jl:150; the reference's
-                           KS_solve_SCF.jl:194-198 calls the 2-block diag_davidson!
-                           there, which is not built: same eigenpairs, other
-                           iteration counts)
+  diag_davidson!           pwb200.davidson per k-point    (device, update_psi="davidson", FP64;
+                           the 2-block solver KS_solve_SCF.jl:194-198 calls)
+  diag_davidson_qe!        pw_davidson per k-point        (device, update_psi="davidson_qe";
+                           the QE-style solver of electrons_scf.jl:150, FP64 or mixed)
   diag_CheFSI!             pwb200.chefsi per k-point      (device, update_psi="CheFSI",
                            cheby_degree; KS_solve_SCF.jl:205-208)
   diag_Emin_PCG!           pwb200.emin_pcg per k-point    (device, update_psi="PCG", FP64;
@@ -181,10 +180,13 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     Focc, Nocc = occupations(Nel, Nstates, b.Nkpt)
     wk = Ham.wk
     Ham.setup_density()
-    if update_psi not in ("LOBPCG", "davidson", "CheFSI", "PCG"):
-        raise ValueError("update_psi must be 'LOBPCG', 'davidson', 'CheFSI' or 'PCG'")
+    if update_psi not in ("LOBPCG", "davidson", "davidson_qe", "CheFSI", "PCG"):
+        raise ValueError("update_psi must be 'LOBPCG', 'davidson', 'davidson_qe', 'CheFSI' or 'PCG'")
     if update_psi == "PCG" and precision != "fp64":
         raise ValueError("update_psi='PCG' (diag_Emin_PCG!) runs on FP64 blocks only")
+    if update_psi == "davidson" and precision != "fp64":
+        raise ValueError("update_psi='davidson' (the 2-block diag_davidson!) runs on FP64 blocks only; "
+                         "update_psi='davidson_qe' has a mixed-precision path")
     crng = np.random.default_rng(seed + 1)   # Lanczos start vectors of CheFSI
     mixed = precision == "mixed"
     dt = torch.complex64 if mixed else torch.complex128
@@ -227,6 +229,9 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             if update_psi == "LOBPCG":
                 ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
             elif update_psi == "davidson":
+                from .davidson import diag_davidson_k
+                ev, n = diag_davidson_k(ctx, ik, 0, psiks[ik], tol=ethr, NiterMax=lobpcg_maxiter, Nstates_conv=Nocc)
+            elif update_psi == "davidson_qe":
                 ev, n = ctx.davidson(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter)
             elif update_psi == "PCG":
                 from .emin_pcg import diag_Emin_PCG_k

@@ -171,6 +171,38 @@ def test_pcg_scf_driver_matches_oracle():
     assert abs(res["energies"]["Total"] - E_l["Total"]) < 1e-6
 
 
+def test_davidson_scf_driver_matches_oracle():
+    """KS_solve_SCF(update_psi="davidson") runs the 2-block diag_davidson! per
+    k-point, as KS_solve_SCF.jl:194-198 does: on the NumPy stand-in it follows
+    the oracle's SCF driven by the oracle's diag_davidson step by step (same
+    energies to 1e-9 Ha, same number of SCF steps)."""
+    import torch
+    from oracle import systems, scf as oscf, davidson
+    from pwb200 import scf
+
+    Ho = systems.Ham_Si_fcc(meshk=(2, 2, 2))
+    start = oscf.rand_BlochWavefunc(Ho, seed=5)
+
+    def diag(Ham, psiks, tol, nconv):
+        ev = []
+        for ik in range(len(psiks)):
+            e, _, _ = davidson.diag_davidson(Ham, psiks[ik], ik, tol=tol, NiterMax=100, Nstates_conv=nconv)
+            ev.append(e)
+        return np.stack(ev, axis=1)
+
+    log_o = []
+    E_o, _, _ = oscf.KS_solve_SCF(Ho, psiks=[p.copy() for p in start], betamix=0.2, mix_method="pulay",
+                                  etot_conv_thr=1e-8, diag=diag, log=log_o)
+    Hd = HostHam(systems.Ham_Si_fcc(meshk=(2, 2, 2)), (2, 2, 2))
+    ps = [torch.from_numpy(np.ascontiguousarray(p.T)) for p in start]
+    res = scf.KS_solve_SCF(Hd, betamix=0.2, mix_method="pulay", etot_conv_thr=1e-8, precision="fp64", psiks=ps,
+                           update_psi="davidson")
+    assert len(res["log"]) == len(log_o)
+    for row_o, row_d in zip(log_o, res["log"]):
+        assert abs(row_o[1] - row_d[1]) < 1e-9, (row_o, row_d)
+    assert abs(res["energies"]["Total"] - E_o["Total"]) < 1e-9
+
+
 def test_scf_rejects_unsupported_choices():
     from oracle import systems
     from pwb200 import scf
@@ -179,3 +211,5 @@ def test_scf_rejects_unsupported_choices():
         scf.KS_solve_SCF(Hd, update_psi="PCG", precision="mixed")
     with pytest.raises(ValueError):
         scf.KS_solve_SCF(Hd, update_psi="nonexistent")
+    with pytest.raises(ValueError):
+        scf.KS_solve_SCF(Hd, update_psi="davidson", precision="mixed")

@@ -119,6 +119,59 @@ def test_op_H_120_grid(si216, prec):
 
 
 @pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_op_H_120_grid_band_batch_boundary(si216, prec):
+    """Band batches of 5 MiB on the 120-point grid (2 FP32 bands or 1 FP64
+    band per batch), so that 5 bands cross 2-4 batch boundaries, with 1 and 2
+    sub-planes per plane-kernel CTA."""
+    import torch
+    import pwb200
+    from oracle import ops
+    H, ctx, psi = si216
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    ref = ops.op_H(H, psi, 0)
+    w = np.array([2.0, 2.0, 1.5, 0.5, 0.25])
+    ref_rho = ops.calc_rhoe(H, [psi], Focc=w[:, None])
+    saved = ctx.get_tuning()
+    try:
+        for pb in (1, 2):
+            ctx.set_tuning(band_chunk_bytes=5 << 20, plane_bands=pb)
+            x = to_dev(psi, dt)
+            y = torch.empty_like(x)
+            ctx.apply(0, 0, x, y, pwb200.PW_OP_H)
+            assert rel_err(to_host(y), ref) < TOL[prec], pb
+            rho = torch.zeros(H.pw.Npoints, dtype=torch.float64, device="cuda")
+            ctx.calc_rhoe(0, x, w, rho)
+            assert rel_err(rho.cpu().numpy(), ref_rho) < TOL[prec], pb
+    finally:
+        ctx.set_tuning(**saved)
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_tuning_candidates(system, prec):
+    """Every launch-parameter set the autotuner tries (plane bands per CTA,
+    band batch, z-pass columns) gives the oracle's op_H."""
+    import torch
+    import pwb200
+    from oracle import ops
+    H, ctx, psis = system
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    ik = len(psis) - 1
+    ref = ops.op_H(H, psis[ik], ik)
+    x = to_dev(psis[ik], dt)
+    y = torch.empty_like(x)
+    saved = ctx.get_tuning()
+    try:
+        for pb in (1, 2, 3):
+            for ch in (1, 16, 96):
+                for zc in (16, 32, 48, 64, 96, 128):
+                    ctx.set_tuning(plane_bands=pb, band_chunk_bytes=ch << 20, z_columns=zc)
+                    ctx.apply(ik, 0, x, y, pwb200.PW_OP_H)
+                    assert rel_err(to_host(y), ref) < TOL[prec], (pb, ch, zc)
+    finally:
+        ctx.set_tuning(**saved)
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
 @pytest.mark.parametrize("term", ["K", "VLOC", "VNL"])
 def test_op_terms_accumulate(system, prec, term):
     """op_K!/op_V_loc!/op_V_Ps_nloc! accumulate into Hpsi."""
@@ -139,14 +192,19 @@ def test_op_terms_accumulate(system, prec, term):
     assert rel_err(to_host(y), ref) < TOL[prec]
 
 
-def test_kprec(system):
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_kprec(system, prec):
+    """Kprec in FP64 and in the FP32 form the mixed-precision eigensolvers use
+    (FP32 result: one rounding of the scaled value)."""
     import torch
     from oracle import ops
     H, ctx, psis = system
-    x = to_dev(psis[0], torch.complex128)
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    x = to_dev(psis[0], dt)
     y = torch.empty_like(x)
     ctx.kprec(0, x, y)
-    assert rel_err(to_host(y), ops.Kprec(H, psis[0], 0)) < 1e-14
+    ref = ops.Kprec(H, to_host(x), 0)
+    assert rel_err(to_host(y), ref) < (1e-14 if prec == "c128" else 2e-7)
 
 
 @pytest.mark.parametrize("prec", ["c128", "c64"])

@@ -6,9 +6,11 @@ total energy and the FP64 oracle's converged SCF.
     FP64 path:  |Etot - ABINIT| < 1e-5 (test/validations_old/Si_fcc.jl:15)
                 |Etot - oracle| < 2e-7, components within 2e-6
     mixed path (FP64 switch at |dE| < 1e-5): |Etot - ABINIT| < 1e-5
-  The same with update_psi = "davidson" (diag_davidson_qe!, Pulay beta 0.5 as
-  test/validations_old/Si_fcc.jl:94-101): |Etot - ABINIT| < 1e-5 and the
-  FP64 result within 2e-7 of the LOBPCG-driven oracle SCF.
+  The same with the Davidson solvers (Pulay beta 0.5 as
+  test/validations_old/Si_fcc.jl:94-101): update_psi = "davidson" (the 2-block
+  diag_davidson! of KS_solve_SCF.jl:194-198, FP64) and "davidson_qe"
+  (diag_davidson_qe!, FP64 and mixed): |Etot - ABINIT| < 1e-5 and the FP64
+  results within 2e-7 of the LOBPCG-driven oracle SCF.
 """
 import numpy as np
 import pytest
@@ -49,11 +51,12 @@ def test_scf_si_fcc(si_fcc_gpu, si_fcc_scf, precision):
         assert res["switched_to_fp64_at"] is not None
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_scf_si_fcc_davidson(si_fcc_gpu, si_fcc_scf, precision):
+@pytest.mark.parametrize("solver,precision", [("davidson", "fp64"), ("davidson_qe", "fp64"),
+                                              ("davidson_qe", "mixed")])
+def test_scf_si_fcc_davidson(si_fcc_gpu, si_fcc_scf, solver, precision):
     from pwb200 import scf
     res = scf.KS_solve_SCF(si_fcc_gpu, betamix=0.5, mix_method="pulay", etot_conv_thr=1e-8, precision=precision,
-                           update_psi="davidson")
+                           update_psi=solver)
     E = res["energies"]
     assert abs(E["Total"] - ABINIT) < 1e-5, res["log"][-3:]
     if precision == "fp64":

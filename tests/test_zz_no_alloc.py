@@ -80,3 +80,37 @@ def test_noalloc_rejects_oversized_grid_and_ops(si64):
     assert e.value.status == pwb200._lib.PW_ERR_UNSUPPORTED
     assert int(pwb200.lib().pw_noalloc_scratch_bytes()) == 32 << 20
     big.close()
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_noalloc_leaves_free_memory_unchanged(prec):
+    """The property the entry point exists for: after one warm-up call (which
+    loads its kernels), calls with growing band counts take no device
+    memory.  A fresh context that never ran pw_apply; every tensor is
+    allocated before the free memory is read."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    import pwb200
+    from oracle import systems
+    H = systems.Ham_Si_fcc(meshk=(1, 1, 1), extra_states=4)
+    pw = H.pw
+    rng = np.random.default_rng(7)
+    ctx = pwb200.Context(pw.Ns, pw.CellVolume, pw.gvecw.idx_gw2r, [pw.Gk2(0)])
+    ctx.set_vloc(H.V_Ps_loc + 0.01 * rng.standard_normal(pw.Npoints))
+    ngw = pw.gvecw.Ngw[0]
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    nmax = 96
+    psi = (rng.standard_normal((ngw, nmax)) + 1j * rng.standard_normal((ngw, nmax))) / np.sqrt(ngw)
+    x = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda().to(dt)
+    y = torch.zeros_like(x)
+    ops = pwb200.PW_OP_VLOC | pwb200.PW_OP_K
+    ctx.apply_vloc_noalloc(0, 0, x[:1], y[:1], ops)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for nb in (1, 2, 8, 33, nmax):
+        ctx.apply_vloc_noalloc(0, 0, x[:nb], y[:nb], ops)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    ctx.close()
