@@ -87,6 +87,16 @@ int64_t     pw_launch_count(const pw_ctx *ctx);
  * reference, whose BLAS calls cannot time out). */
 int         pw_check_device(pw_ctx *ctx);
 
+/* Device buffers and copies for hosts that have no GPU array type of their
+ * own (the Julia binding without CUDA.jl; no counterpart in the reference,
+ * whose arrays all live on the host).  A buffer belongs to the context and
+ * is freed by pw_device_free or pw_destroy; the copies are ordered on the
+ * context stream and complete before the call returns. */
+int pw_device_alloc(pw_ctx *ctx, uint64_t bytes, void **dptr);
+int pw_device_free(pw_ctx *ctx, void *dptr);
+int pw_copy_to_device(pw_ctx *ctx, void *dst, const void *src, uint64_t bytes);
+int pw_copy_to_host(pw_ctx *ctx, void *dst, const void *src, uint64_t bytes);
+
 /* Launch parameters of a context's kernels.  No counterpart in the
  * reference: there FFTW's planner and the BLAS pick their own blockings.
  * A zero field means "the built-in default"; pw_set_tuning replaces all
@@ -109,8 +119,9 @@ int pw_set_tuning(pw_ctx *ctx, const pw_tuning *t);
  * ik on nb bands of dtype and, for PW_C64 with nb > 0, the Rayleigh-Ritz
  * Gram (3 nb x 3 nb over Ngw[ik]) and rotation (Ngw x 3nb -> nb).  Every
  * candidate is timed with CUDA events on the context stream on seeded
- * blocks the call allocates and frees; the fastest set is applied to the
- * context and written to *chosen.  cache_path (NULL: the environment
+ * blocks the call allocates and frees, starting from the built-in defaults
+ * (the context's current setting is not a candidate); the fastest set is
+ * applied to the context and written to *chosen.  cache_path (NULL: the environment
  * variable PW_AUTOTUNE_CACHE, or no cache if unset) names a text file of
  * earlier choices keyed by GPU name, grid, Ngw, active columns and x
  * planes, nb, dtype and projector count: a hit applies the stored choice
@@ -179,6 +190,19 @@ int pw_kprec(pw_ctx *ctx, int ik, int dtype, const void *in, void *out,
  * overwrites. */
 int pw_calc_rhoe(pw_ctx *ctx, int ik, int dtype, const void *psi, int64_t ld,
                  int nb, const double *w, double *rhoe, int accumulate);
+
+/* Adjoint of op_V_loc! (op_V_loc.jl:33-92) with respect to the potential:
+ *   dV[r] (+)= sum_b w[b] N Re( conj(G_to_R(lam_b))[r] G_to_R(psi_b)[r] ),
+ * the gradient of L = sum_b w_b Re<lam_b| V_loc psi_b> with respect to the
+ * V_loc(r) of pw_set_vloc.  lam == psi (or NULL) gives dE/dV_loc(r) of the
+ * band energy E = sum_b w_b <psi_b|H|psi_b> (w = wk * Focc): the density of
+ * calc_rhoe.jl:51-78 times dVol = Omega/N, the quantity that
+ * calc_forces_Ps_loc.jl:13-72 contracts with dV_ps/dtau and, at self
+ * consistency, the derivative of the total energy with respect to an
+ * external potential.  psi, lam: device Ngw x nb (ld) of dtype; w: host nb;
+ * dV: device FP64, N points; accumulate = 0 overwrites. */
+int pw_vloc_vjp(pw_ctx *ctx, int ik, int dtype, const void *psi, const void *lam,
+                int64_t ld, int nb, const double *w, double *dV, int accumulate);
 
 /* Rayleigh-Ritz contractions (diag_LOBPCG.jl:85,144,152-153,183-184):
  * C (m x n, device ComplexF64, ldc) (+)= A^H B, A is K x m, B is K x n,

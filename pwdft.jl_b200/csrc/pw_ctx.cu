@@ -636,6 +636,46 @@ extern "C" int pw_check_device(pw_ctx *c) {
     return PW_OK;
 }
 
+extern "C" int pw_device_alloc(pw_ctx *c, uint64_t bytes, void **dptr) {
+    if (!c) return PW_ERR_ARG;
+    if (!dptr || bytes == 0) return fail(c, PW_ERR_ARG, "pw_device_alloc: NULL out pointer or zero size");
+    CK(c, cudaSetDevice(c->device));
+    unsigned char *p = nullptr;
+    int s = dalloc(c, &p, (size_t)bytes);
+    if (s) return s;
+    *dptr = p;
+    return PW_OK;
+}
+
+extern "C" int pw_device_free(pw_ctx *c, void *dptr) {
+    if (!c) return PW_ERR_ARG;
+    if (!dptr) return PW_OK;
+    if (std::find(c->allocs.begin(), c->allocs.end(), dptr) == c->allocs.end())
+        return fail(c, PW_ERR_ARG, "pw_device_free: pointer not from pw_device_alloc of this context");
+    CK(c, cudaSetDevice(c->device));
+    CK(c, cudaStreamSynchronize(c->stream));
+    dfree(c, dptr);
+    return PW_OK;
+}
+
+extern "C" int pw_copy_to_device(pw_ctx *c, void *dst, const void *src, uint64_t bytes) {
+    if (!c) return PW_ERR_ARG;
+    if (!dst || !src) return fail(c, PW_ERR_ARG, "pw_copy_to_device: NULL pointer");
+    CK(c, cudaSetDevice(c->device));
+    CK(c, cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return PW_OK;
+}
+
+extern "C" int pw_copy_to_host(pw_ctx *c, void *dst, const void *src, uint64_t bytes) {
+    if (!c) return PW_ERR_ARG;
+    if (!dst || !src) return fail(c, PW_ERR_ARG, "pw_copy_to_host: NULL pointer");
+    CK(c, cudaSetDevice(c->device));
+    CK(c, cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return PW_OK;
+}
+
 extern "C" int pw_synchronize(pw_ctx *c) {
     if (!c) return PW_ERR_ARG;
     CK(c, cudaStreamSynchronize(c->stream));
@@ -951,6 +991,45 @@ extern "C" int pw_calc_rhoe(pw_ctx *c, int ik, int dtype, const void *psi, int64
     CK(c, cudaSetDevice(c->device));
     return dtype == PW_C128 ? rhoe_T<double>(c, ik, psi, ld, nb, w, rhoe, accumulate)
                             : rhoe_T<float>(c, ik, psi, ld, nb, w, rhoe, accumulate);
+}
+
+// Adjoint of op_V_loc with respect to V: dV (+)= sum_b w_b N Re(conj(u_lam) u_psi)
+// with u = G_to_R(.).  The density kernels give sum_b (w'_b / Omega) |N u_b|^2,
+// so w' = w Omega / N; for lam != psi the polarised block [psi + lam, psi - lam]
+// goes through them with weights +-w'/4.
+template <typename T>
+int vjp_T(pw_ctx *c, int ik, const void *psi, const void *lam, int64_t ld, int nb, const double *w, double *dV,
+          int accumulate) {
+    const double scale = c->CellVolume / (double)c->N;
+    if (!lam || lam == psi) {
+        std::vector<double> wv(w, w + nb);
+        for (auto &x : wv) x *= scale;
+        return rhoe_T<T>(c, ik, psi, ld, nb, wv.data(), dV, accumulate);
+    }
+    const KData &kd = c->k[ik];
+    const size_t es = 2 * sizeof(T);
+    int s;
+    if ((s = ensure(c, c->slots[SL_VJP], 2 * (size_t)nb * kd.Ngw * es))) return s;
+    CK(c, launch_polarize<T>(kd.Ngw, nb, psi, lam, ld, c->slots[SL_VJP].p, c->stream));
+    c->launches += 1;
+    std::vector<double> wv(2 * (size_t)nb);
+    for (int b = 0; b < nb; ++b) {
+        wv[b] = 0.25 * w[b] * scale;
+        wv[nb + b] = -0.25 * w[b] * scale;
+    }
+    return rhoe_T<T>(c, ik, c->slots[SL_VJP].p, kd.Ngw, 2 * nb, wv.data(), dV, accumulate);
+}
+
+extern "C" int pw_vloc_vjp(pw_ctx *c, int ik, int dtype, const void *psi, const void *lam, int64_t ld, int nb,
+                           const double *w, double *dV, int accumulate) {
+    if (!c) return PW_ERR_ARG;
+    int s;
+    if ((s = check_k(c, ik)) || (s = check_dtype(c, dtype))) return s;
+    if (!psi || !w || !dV || nb <= 0 || ld < c->k[ik].Ngw) return fail(c, PW_ERR_ARG, "bad pw_vloc_vjp arguments");
+    if (2 * (int64_t)nb > 65535 * 8) return fail(c, PW_ERR_ARG, "pw_vloc_vjp: nb too large");
+    CK(c, cudaSetDevice(c->device));
+    return dtype == PW_C128 ? vjp_T<double>(c, ik, psi, lam, ld, nb, w, dV, accumulate)
+                            : vjp_T<float>(c, ik, psi, lam, ld, nb, w, dV, accumulate);
 }
 
 extern "C" int pw_gram(pw_ctx *c, int dtype, int64_t K, int m, int n, const void *A, int64_t lda, const void *B,

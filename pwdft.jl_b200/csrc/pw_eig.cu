@@ -812,6 +812,14 @@ cudaError_t chol_and_inverse(double2 *G, int n, double2 *Linv, double2 *DI, unsi
     return cudaSuccess;
 }
 
+// flag[0] = 1 if any diagonal or off-diagonal entry of the tridiagonal
+// matrix is not finite
+__global__ void k_check_finite(const double *__restrict__ d, const double *__restrict__ e, int n, int *flag) {
+    bool bad = false;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) bad |= !isfinite(d[i]) || (i + 1 < n && !isfinite(e[i]));
+    if (__syncthreads_or(bad) && threadIdx.x == 0) *flag = 1;
+}
+
 cudaError_t hegv_lowest(double2 *T, double2 *G, int n, int k, double *lam_out, double2 *S, void *work, size_t work_bytes,
                         void *gemm_ws, int *d_status, cudaStream_t st) {
     if (n <= 0 || k <= 0 || k > n || work_bytes < eig_work_bytes(n, k)) return cudaErrorInvalidValue;
@@ -863,6 +871,9 @@ cudaError_t hegv_lowest(double2 *T, double2 *G, int n, int k, double *lam_out, d
         if ((e_ = cudaLaunchCooperativeKernel((const void *)k_tridiag, nblk, COOP_THREADS, args, smem, st)) != cudaSuccess)
             return e_;
     }
+    // a non-finite T or G reaches the tridiagonal matrix: report it (the
+    // Sturm counts would otherwise turn it into finite, meaningless values)
+    k_check_finite<<<1, 256, 0, st>>>(d, e, n, err + 2);
     k_bisect<<<(k + 7) / 8, 256, 0, st>>>(d, e, n, k, lam, nrm);
     if ((e_ = cudaMemcpyAsync(lam_out, lam, k * sizeof(double), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e_;
     if (S) {
@@ -889,8 +900,9 @@ cudaError_t hegv_lowest(double2 *T, double2 *G, int n, int k, double *lam_out, d
         }
     }
     if ((e_ = cudaGetLastError()) != cudaSuccess) return e_;
-    // status: [0] barrier expiry, [1] Cholesky breakdown column (1-based)
-    return cudaMemcpyAsync(d_status, err, 2 * sizeof(int), cudaMemcpyDeviceToDevice, st);
+    // status: [0] barrier expiry, [1] Cholesky breakdown column (1-based),
+    // [2] non-finite tridiagonal matrix
+    return cudaMemcpyAsync(d_status, err, 3 * sizeof(int), cudaMemcpyDeviceToDevice, st);
 }
 
 cudaError_t chol_inverse_upper(double2 *C, int n, double2 *Rinv, void *work, int *d_status, cudaStream_t st) {

@@ -236,6 +236,21 @@ __global__ void k_kprec(int Ngw, int nb, const double *__restrict__ Gk2, const C
     }
 }
 
+// out[b] = psi_b + lam_b, out[nb + b] = psi_b - lam_b (out: 2 nb columns of
+// Ngw): the polarisation Re(conj(l) p) = (|p + l|^2 - |p - l|^2) / 4 that
+// turns the density kernels into the adjoint of op_V_loc with respect to V
+template <typename T>
+__global__ void k_polarize(int Ngw, int nb, const Cx<T> *__restrict__ psi, const Cx<T> *__restrict__ lam, int64_t ld,
+                           Cx<T> *__restrict__ out) {
+    const size_t total = (size_t)Ngw * nb;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(t / Ngw), g = (int)(t - (size_t)b * Ngw);
+        const Cx<T> p = psi[(size_t)b * ld + g], l = lam[(size_t)b * ld + g];
+        out[t] = cadd(p, l);
+        out[total + t] = cmake(p.x - l.x, p.y - l.y);
+    }
+}
+
 template <typename T>
 __global__ void k_zero(Cx<T> *p, int Ngw, int nb, int64_t ld) {
     const size_t total = (size_t)Ngw * nb;
@@ -1153,6 +1168,13 @@ cudaError_t launch_kprec(int Ngw, int nb, const double *Gk2, const void *in, voi
 }
 
 template <typename T>
+cudaError_t launch_polarize(int Ngw, int nb, const void *psi, const void *lam, int64_t ld, void *out, cudaStream_t st) {
+    k_polarize<T><<<grid_stride_blocks((size_t)Ngw * nb), 256, 0, st>>>(Ngw, nb, (const Cx<T> *)psi, (const Cx<T> *)lam,
+                                                                         ld, (Cx<T> *)out);
+    return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t st) {
     k_zero<T><<<grid_stride_blocks((size_t)Ngw * nb), 256, 0, st>>>((Cx<T> *)p, Ngw, nb, ld);
     return cudaGetLastError();
@@ -1171,7 +1193,8 @@ cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t st) {
     template cudaError_t launch_rho_reduce<T>(const void *, int, size_t, double *, int, cudaStream_t);              \
     template cudaError_t launch_opK<T>(int, int, const double *, const void *, void *, int64_t, int, cudaStream_t); \
     template cudaError_t launch_kprec<T>(int, int, const double *, const void *, void *, int64_t, cudaStream_t);    \
-    template cudaError_t launch_zero<T>(void *, int, int, int64_t, cudaStream_t);
+    template cudaError_t launch_zero<T>(void *, int, int, int64_t, cudaStream_t);                                \
+    template cudaError_t launch_polarize<T>(int, int, const void *, const void *, int64_t, void *, cudaStream_t);
 PW_INST(float)
 PW_INST(double)
 

@@ -22,6 +22,8 @@ enum ScratchSlot {
     SL_HOST_C128, SL_HOST_C64,
     // forces
     SL_FRC_A, SL_FRC_B, SL_FRC_C,
+    // adjoint of op_V_loc with respect to V (polarised blocks)
+    SL_VJP,
     SL_COUNT
 };
 static_assert(SL_COUNT <= 32, "pw_ctx holds 32 scratch slots");
@@ -64,6 +66,8 @@ cudaError_t launch_opK(int Ngw, int nb, const double *Gk2, const void *psi, void
 template <typename T>
 cudaError_t launch_kprec(int Ngw, int nb, const double *Gk2, const void *in, void *out, int64_t ld, cudaStream_t);
 template <typename T> cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t);
+template <typename T>
+cudaError_t launch_polarize(int Ngw, int nb, const void *psi, const void *lam, int64_t ld, void *out, cudaStream_t);
 
 // C (m x n, double2, ldc) (+)= A^H B with A (K x m), B (K x n) of element Cx<T>.
 // ws: split-K workspace of at least gemm_tn_ws_bytes() bytes.

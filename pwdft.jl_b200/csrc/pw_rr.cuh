@@ -93,11 +93,12 @@ struct Run {
 // lowest k eigenpairs of (T, G) (G may be null) of order n; T, G overwritten
 int eig(Run &r, double2 *T, double2 *G, int n, int k, double *lam_dev, double2 *S) {
     CKR(r.c, pwk::hegv_lowest(T, G, n, k, lam_dev, S, r.eigw, r.eigw_bytes, nullptr, r.eigstat, r.st));
-    int h[2] = {0, 0};
+    int h[3] = {0, 0, 0};
     CKR(r.c, cudaMemcpyAsync(h, r.eigstat, sizeof(h), cudaMemcpyDeviceToHost, r.st));
     CKR(r.c, cudaStreamSynchronize(r.st));
     if (h[0]) return pwk_fail(r.c, PW_ERR_TIMEOUT, "a bounded grid barrier of the eigensolver expired");
     if (h[1]) return pwk_fail(r.c, PW_ERR_NOT_POSDEF, "overlap matrix not positive definite (Cholesky)");
+    if (h[2]) return pwk_fail(r.c, PW_ERR_NAN, "non-finite value in the eigenproblem");
     pwk_count_launches(r.c, 10);
     return PW_OK;
 }

@@ -141,6 +141,7 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
     if (read_cache(path, key, &t)) {
         int s = pw_set_tuning(c, &t);
         if (s) return s;
+        pw_get_tuning(c, &t);   // the values in effect (a zero field reads as its default)
         if (chosen) *chosen = t;
         return PW_OK;
     }
@@ -159,9 +160,10 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
         if (pw_set_tuning(c, &cand) != PW_OK) return -1.0;
         return time_ms(st, run_h);
     };
-    // ---- op_H: coordinate descent over plane bands, band batch, z columns
-    pw_tuning best = base;
-    best.gemm_splits = 0;
+    // ---- op_H: coordinate descent over plane bands, band batch, z columns,
+    // from the built-in defaults (whatever the context was set to before)
+    pw_tuning best;
+    std::memset(&best, 0, sizeof(best));
     double tbest = eval(best);
     if (tbest < 0) {
         pw_set_tuning(c, &base);
@@ -228,6 +230,7 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
     cudaGetLastError();
     int s = pw_set_tuning(c, &best);
     if (s) return s;
+    pw_get_tuning(c, &best);    // the values in effect (a zero field reads as its default)
     append_cache(path, key, best);
     if (chosen) *chosen = best;
     return PW_OK;

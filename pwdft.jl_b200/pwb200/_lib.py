@@ -57,6 +57,10 @@ SIGNATURES = {
     "pw_synchronize": (_i, [_vp]),
     "pw_launch_count": (_i64, [_vp]),
     "pw_check_device": (_i, [_vp]),
+    "pw_device_alloc": (_i, [_vp, C.c_uint64, C.POINTER(_vp)]),
+    "pw_device_free": (_i, [_vp, _vp]),
+    "pw_copy_to_device": (_i, [_vp, _vp, _vp, C.c_uint64]),
+    "pw_copy_to_host": (_i, [_vp, _vp, _vp, C.c_uint64]),
     "pw_get_tuning": (_i, [_vp, C.POINTER(pw_tuning)]),
     "pw_set_tuning": (_i, [_vp, C.POINTER(pw_tuning)]),
     "pw_autotune": (_i, [_vp, _i, _i, _i, C.c_char_p, C.POINTER(pw_tuning), _dp]),
@@ -71,6 +75,7 @@ SIGNATURES = {
     "pw_noalloc_scratch_bytes": (C.c_uint64, []),
     "pw_kprec": (_i, [_vp, _i, _i, _vp, _vp, _i64, _i]),
     "pw_calc_rhoe": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _vp, _i]),
+    "pw_vloc_vjp": (_i, [_vp, _i, _i, _vp, _vp, _i64, _i, _dp, _vp, _i]),
     "pw_gram": (_i, [_vp, _i, _i64, _i, _i, _vp, _i64, _vp, _i64, _vp, _i64, _i]),
     "pw_rotate": (_i, [_vp, _i, _i64, _i, _i, _vp, _i64, _vp, _i64, _vp, _i64, _i]),
     "pw_eigh": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp]),

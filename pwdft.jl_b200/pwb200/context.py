@@ -217,6 +217,18 @@ class Context:
         self._chk(self._L.pw_calc_rhoe(self.h, ik, dtype_code(psi), C.c_void_p(psi.data_ptr()), ld, nb, _dptr(w),
                                        C.c_void_p(rhoe.data_ptr()), int(accumulate)))
 
+    def vloc_vjp(self, ik, psi, w, dV, lam=None, accumulate=False):
+        """pw_vloc_vjp: dV (torch float64, N) (+)= the gradient with respect to
+        V_loc(r) of sum_b w_b Re<lam_b|V_loc psi_b> (lam None: lam = psi, i.e.
+        dE/dV_loc of the band energy with w = wk*Focc)."""
+        nb, ld = psi.shape
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        assert len(w) == nb and (lam is None or (lam.shape == psi.shape and lam.dtype == psi.dtype))
+        self.use_torch_stream()
+        self._chk(self._L.pw_vloc_vjp(self.h, ik, dtype_code(psi), C.c_void_p(psi.data_ptr()),
+                                      None if lam is None else C.c_void_p(lam.data_ptr()), ld, nb, _dptr(w),
+                                      C.c_void_p(dV.data_ptr()), int(accumulate)))
+
     def gram(self, A, B, out, accumulate=False):
         """out (torch complex128, (n, m) row-major = m x n column-major) (+)= A^H B,
         A: (m, K), B: (n, K) band-major blocks."""
