@@ -333,6 +333,17 @@ int pw_set_symmetry(pw_ctx *ctx, int nshell, int nsym, const int32_t *isg,
  * sphere are kept. */
 int pw_symmetrize_rhoe(pw_ctx *ctx, double *rhoe);
 
+/* mix_pulay! (mix_pulay.jl:1-41) on device vectors, the history kept in the
+ * context: x (device FP64, n) is the input density of SCF iteration iter
+ * (1-based; iter == 1 starts a new history), gx (device, n, distinct) the
+ * output density.  x is overwritten with x + beta f before iteration
+ * mixdim + 1 and with x + beta f - (X + beta F) inv(F'F) F'f from then on
+ * (f = gx - x; X, F the last mixdim differences), then clamped to >= eps()
+ * when clamp != 0 (KS_solve_SCF.jl:277-281).  mixdim <= 16; a singular F'F
+ * mixes simply for that iteration.  No host synchronisation. */
+int pw_mix_pulay(pw_ctx *ctx, double *x, const double *gx, int64_t n, double beta,
+                 int iter, int mixdim, int clamp);
+
 /* Poisson_solve! (Poisson_solve.jl:22-40): V_H(r) from rho(r), device FP64
  * arrays of N points. */
 int pw_poisson(pw_ctx *ctx, const double *rho, double *VH);

@@ -19,6 +19,7 @@
 using namespace pwk;
 
 void pwk_noalloc_prepare(int dev);   // pw_noalloc.cu
+void pwk_mix_free(void *state);      // pw_mix.cu
 
 namespace {
 
@@ -121,6 +122,7 @@ struct pw_ctx {
     cudaStream_t cp_in = nullptr, cp_out = nullptr;
     cudaEvent_t ev_in[8] = {}, ev_cmp[8] = {};
     int64_t launches = 0;  // kernels launched by this context (reported by pw_launch_count)
+    void *mix_state = nullptr;  // Pulay history of pw_mix_pulay (pw_mix.cu)
 };
 
 namespace {
@@ -583,6 +585,7 @@ extern "C" void pw_destroy(pw_ctx *c) {
     }
     if (c->cp_in) cudaStreamDestroy(c->cp_in);
     if (c->cp_out) cudaStreamDestroy(c->cp_out);
+    pwk_mix_free(c->mix_state);
     for (void *p : c->allocs) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1206,6 +1209,7 @@ int pwk_tune_shape(const pw_ctx *c, int ik, int *Ns, int *Ncol, int *Nxa, int *n
     return PW_OK;
 }
 int pwk_fail_msg(pw_ctx *c, int code, const char *msg) { return fail(c, code, "%s", msg); }
+void **pwk_mix_slot(pw_ctx *c) { return &c->mix_state; }
 
 int pwk_scratch(pw_ctx *c, int slot, size_t bytes, void **out) {
     if (slot < 0 || slot >= 32) return fail(c, PW_ERR_ARG, "scratch slot %d", slot);

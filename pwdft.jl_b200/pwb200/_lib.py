@@ -88,6 +88,7 @@ SIGNATURES = {
     "pw_lanczos_bounds": (_i, [_vp, _i, _i, _i, _vp, _dp, _dp]),
     "pw_set_density_sphere": (_i, [_vp, _i64, _i64p, _dp, _i]),
     "pw_poisson": (_i, [_vp, _vp, _vp]),
+    "pw_mix_pulay": (_i, [_vp, _vp, _vp, _i64, _d, _i, _i, _i]),
     "pw_update": (_i, [_vp, _vp, _vp, _vp, _vp, _dp]),
     "pw_band_energies": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _dp]),
     "pw_ortho_cholesky": (_i, [_vp, _i, _vp, _i64, _i64, _i]),

@@ -323,6 +323,15 @@ class Context:
         self._keep_dens = (idx, g2)
         self._chk(self._L.pw_set_density_sphere(self.h, len(idx), idx.ctypes.data_as(C.POINTER(C.c_int64)), _dptr(g2), 0))
 
+    def mix_pulay(self, x, gx, beta, it, mixdim, clamp=True):
+        """mix_pulay! on the device (history in the library): x (torch float64,
+        N) := the mixed density of iteration it (1 starts a new history),
+        clamped at eps() when clamp."""
+        self.use_torch_stream()
+        self._chk(self._L.pw_mix_pulay(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(gx.data_ptr()), x.numel(),
+                                       float(beta), int(it), int(mixdim), int(clamp)))
+        return x
+
     def poisson(self, rho, VH):
         self.use_torch_stream()
         self._chk(self._L.pw_poisson(self.h, C.c_void_p(rho.data_ptr()), C.c_void_p(VH.data_ptr())))

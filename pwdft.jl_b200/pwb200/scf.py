@@ -15,7 +15,7 @@ density mixing):
                            KS_solve_SCF.jl:199-203)
   calc_rhoe!               pw_calc_rhoe                   (device)
   symmetrize_rhoe!         pw_symmetrize_rhoe             (device, Hamiltonians built with symmetry)
-  mix_pulay! / simple      mix_pulay.jl:1-41              (device vectors, torch ops)
+  mix_pulay! / simple      mix_pulay.jl:1-41              (device: pw_mix_pulay, history in the library)
   smearing (use_smearing)  KS_solve_SCF.jl:218-223, occupations.jl:6-245  (host: Fermi level
                            by bisection over the Nstates x Nkpt eigenvalues, -TS)
   rho >= eps clamp         KS_solve_SCF.jl:277-281        (device)
@@ -121,43 +121,6 @@ def rand_psiks(Ham, Nstates, seed, dtype, keep=None):
     return out
 
 
-class PulayMixer:
-    """mix_pulay.jl:1-41 on device vectors."""
-
-    def __init__(self, N, beta, mixdim, device):
-        import torch
-        self.beta, self.mixdim = beta, mixdim
-        self.X = torch.zeros((mixdim, N), dtype=torch.float64, device=device)
-        self.F = torch.zeros((mixdim, N), dtype=torch.float64, device=device)
-        self.x_old = None
-        self.f_old = None
-
-    def __call__(self, x, gx, it):
-        import torch
-        f = gx - x
-        if it == 1:
-            dx, df = x.clone(), f.clone()
-        else:
-            dx, df = x - self.x_old, f - self.f_old
-        if it <= self.mixdim:
-            self.X[it - 1] = dx
-            self.F[it - 1] = df
-        else:
-            self.X = torch.roll(self.X, -1, dims=0)
-            self.F = torch.roll(self.F, -1, dims=0)
-            self.X[-1] = dx
-            self.F[-1] = df
-        self.x_old = x.clone()
-        self.f_old = f.clone()
-        if it > self.mixdim:
-            FtF = (self.F @ self.F.T).cpu().numpy()
-            Ftf = (self.F @ f).cpu().numpy()
-            c = torch.from_numpy(np.linalg.inv(FtF) @ Ftf).to(x.device)
-            addv = (self.X + self.beta * self.F).T @ c
-            return x + self.beta * f - addv
-        return x + self.beta * f
-
-
 def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
                  verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3,
@@ -203,7 +166,6 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     rho = torch.from_numpy(guess_rhoe(Ham.system, b, Ham.pspots, Nel)).to(dev)
     ctx.update(rho, Vps)
     E_NN = ewald_energy(Ham.system.LatVecs, Ham.system.positions, Ham.Zvals[Ham.system.atm2species])
-    mixer = PulayMixer(N, betamix, mixdim, dev) if mix_method == "pulay" else None
     rho_new = torch.zeros(N, dtype=torch.float64, device=dev)
     Etot_old, Nconv, ethr = 0.0, 0, 0.1
     imix = 0
@@ -258,11 +220,10 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         sync()
         t2 = time.perf_counter()
         imix += 1
-        if mixer is not None:
-            rho = mixer(rho, rho_new, imix)
+        if mix_method == "pulay":
+            rho = ctx.mix_pulay(rho, rho_new, betamix, imix, mixdim, clamp=True)
         else:
-            rho = betamix * rho_new + (1 - betamix) * rho
-        rho = torch.clamp(rho, min=EPS)
+            rho = torch.clamp(betamix * rho_new + (1 - betamix) * rho, min=EPS)
         sums = ctx.update(rho, Vps)
         Ek = En = 0.0
         for ik in mine:

@@ -70,6 +70,20 @@ class SCFCtx(NumpyCtx):
         dVol = self.H.pw.CellVolume / self.H.pw.Npoints
         return np.array([2.0 * EH / dVol, Eps / dVol, Exc / dVol])
 
+    def mix_pulay(self, x, gx, beta, it, mixdim, clamp=True):
+        """pw_mix_pulay through the oracle's mix_pulay (its history here)."""
+        import torch
+        from oracle.scf import mix_pulay
+        if it == 1:
+            n = x.numel()
+            self._mix = (np.zeros((n, mixdim)), np.zeros((n, mixdim)), {})
+        X, F, state = self._mix
+        r = mix_pulay(x.numpy().copy(), gx.numpy().copy(), beta, X, F, it, mixdim, state)
+        if clamp:
+            r = np.maximum(r, np.finfo(np.float64).eps)
+        x.copy_(torch.from_numpy(r))
+        return x
+
     def lobpcg(self, ik, ispin, X, tol=1e-5, nitermax=100, nconv=0):
         import torch
         from oracle.lobpcg import diag_LOBPCG_k

@@ -62,3 +62,34 @@ def test_scf_si_fcc_davidson(si_fcc_gpu, si_fcc_scf, solver, precision):
     if precision == "fp64":
         _, Eo, _, _ = si_fcc_scf
         assert abs(E["Total"] - Eo["Total"]) < 2e-7
+
+
+def test_device_pulay_mixing_matches_oracle():
+    """pw_mix_pulay (ring history, F'F updated by one row per iteration,
+    on-device solve) against the oracle's mix_pulay (mix_pulay.jl:1-41)
+    step by step on seeded densities: mixdim 3, 9 iterations (Pulay from
+    the 4th), clamping at eps(); then a new history (iter = 1) restarts."""
+    if not cuda_ok():
+        pytest.skip("no CUDA device")
+    import torch
+    import pwb200
+    from oracle.scf import mix_pulay
+    from oracle import systems
+    Ho = systems.Ham_Si_fcc(meshk=(1, 1, 1))
+    pw = Ho.pw
+    ctx = pwb200.Context(pw.Ns, pw.CellVolume, pw.gvecw.idx_gw2r, [pw.Gk2(0)])
+    rng = np.random.default_rng(17)
+    n, mixdim, beta = pw.Npoints, 3, 0.3
+    for rep in range(2):
+        x_o = np.abs(rng.standard_normal(n)) * 0.05
+        x_d = torch.from_numpy(x_o.copy()).cuda()
+        X, F, state = np.zeros((n, mixdim)), np.zeros((n, mixdim)), {}
+        for it in range(1, 10):
+            # a contracting "SCF map" with a little noise
+            gx = 0.6 * x_o + 0.4 * np.abs(np.sin(0.001 * np.arange(n) * it)) * 0.05 + 1e-4 * rng.standard_normal(n)
+            x_o = np.maximum(mix_pulay(x_o, gx, beta, X, F, it, mixdim, state), np.finfo(np.float64).eps)
+            ctx.mix_pulay(x_d, torch.from_numpy(gx).cuda(), beta, it, mixdim, clamp=True)
+            got = x_d.cpu().numpy()
+            assert np.abs(got - x_o).max() < 1e-10 * np.abs(x_o).max(), (rep, it)
+            x_d = torch.from_numpy(x_o.copy()).cuda()   # both continue from the oracle's x
+    ctx.close()
