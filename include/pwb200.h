@@ -394,6 +394,12 @@ int pw_forces_nonlocal(pw_ctx *ctx, int ik, int dtype, const void *psi, int64_t 
 int pw_ortho_sqrt(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw,
                   int nb);
 
+/* Rinv = inv(cholesky(Hermitian(C)).U): the upper-triangular factor that
+ * diag_LOBPCG.jl:118-125,186-194 divides W and P by (W / R).  C (device,
+ * n x n ComplexF64, upper triangle read) is overwritten; Rinv (device, n x n
+ * column-major).  PW_ERR_NOT_POSDEF when C is not positive definite. */
+int pw_chol_rinv(pw_ctx *ctx, int n, double *C, double *Rinv);
+
 /* ortho_cholesky!(Ham, psi) (ortho_sqrt.jl:80-89): O = psi'psi = U^H U,
  * psi := psi / U, psi device Ngw x nb (ld), in place. */
 int pw_ortho_cholesky(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw, int nb);

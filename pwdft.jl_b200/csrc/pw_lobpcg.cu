@@ -299,6 +299,22 @@ extern "C" int pw_ortho_sqrt(pw_ctx *c, int dtype, void *psi, int64_t ld, int64_
     return PW_OK;
 }
 
+// Rinv = inv(cholesky(Hermitian(C)).U) (the W / R and P / R of
+// diag_LOBPCG.jl:118-125,186-194), C read from its upper triangle and
+// overwritten; FP64 on the device.
+extern "C" int pw_chol_rinv(pw_ctx *c, int n, double *C, double *Rinv) {
+    if (!c) return PW_ERR_ARG;
+    if (!C || !Rinv || n <= 0 || C == Rinv) return pwk_fail(c, PW_ERR_ARG, "bad pw_chol_rinv arguments");
+    if (cudaSetDevice(pwk_device(c)) != cudaSuccess) return pwk_fail(c, PW_ERR_CUDA, "cudaSetDevice failed");
+    Run r{};
+    r.c = c;
+    r.st = pwk_stream(c);
+    r.eigw_bytes = pwk::eig_work_bytes(n, 1);
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGW, r.eigw_bytes, &r.eigw));
+    RK(pwk_scratch(c, pwk::SL_LOB_EIGSTAT, 64, (void **)&r.eigstat));
+    return chol_rinv(r, (double2 *)C, n, (double2 *)Rinv);
+}
+
 // ortho_cholesky!(psi) (ortho_sqrt.jl:80-89): O = psi'psi = U^H U (Cholesky),
 // psi := psi / U.
 extern "C" int pw_ortho_cholesky(pw_ctx *c, int dtype, void *psi, int64_t ld, int64_t ngw, int nb) {

@@ -92,6 +92,7 @@ SIGNATURES = {
     "pw_update": (_i, [_vp, _vp, _vp, _vp, _vp, _dp]),
     "pw_band_energies": (_i, [_vp, _i, _i, _vp, _i64, _i, _dp, _dp]),
     "pw_ortho_cholesky": (_i, [_vp, _i, _vp, _i64, _i64, _i]),
+    "pw_chol_rinv": (_i, [_vp, _i, _vp, _vp]),
     "pw_calc_grad": (_i, [_vp, _i, _i, _i, _vp, _vp, _i64, _i, _dp, _d]),
     "pw_set_force_tables": (_i, [_vp, _i, _dp, _dp]),
     "pw_set_xc": (_i, [_vp, _i, _dp]),

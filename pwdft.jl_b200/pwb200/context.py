@@ -20,6 +20,10 @@ def _dptr(a):
     return a.ctypes.data_as(_dp)
 
 
+def C_void(t):
+    return C.c_void_p(t.data_ptr())
+
+
 def dtype_code(t):
     """Element type code of a torch complex tensor."""
     import torch
@@ -351,6 +355,17 @@ class Context:
         nb, ld = psi.shape
         self.use_torch_stream()
         self._chk(self._L.pw_ortho_cholesky(self.h, dtype_code(psi), C.c_void_p(psi.data_ptr()), ld, ld, nb))
+
+    def chol_rinv(self, C):
+        """inv(cholesky(Hermitian(C)).U) on the device: C torch complex128 (n, n)
+        holding the column-major matrix (its transpose); returns Rinv in the
+        same convention.  C is overwritten."""
+        import torch
+        n = C.shape[0]
+        R = torch.empty_like(C)
+        self.use_torch_stream()
+        self._chk(self._L.pw_chol_rinv(self.h, n, C_void(C), C_void(R)))
+        return R
 
     def calc_grad(self, ik, ispin, psi, Focc, wk):
         """calc_grad: returns grad (same shape and dtype as psi (nb, Ngw))."""

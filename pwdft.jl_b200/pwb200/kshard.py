@@ -34,8 +34,33 @@ class KShards:
         self.owned = shard_kpoints([float(n) * Nstates for n in Ngw], self.world)
         self.mine = self.owned[self.rank]
 
+    kind = "kpoints"
+
     def sum_(self, t):
         """In-place sum over ranks of a tensor."""
         if self.dist is not None:
             self.dist.all_reduce(t)
         return t
+
+    def reduce_evals(self, evals):
+        """Each rank filled the columns of its own k-points: sum them."""
+        if self.world > 1:
+            import torch
+            t = torch.from_numpy(evals.copy())
+            if self.dist.get_backend() == "nccl":
+                t = t.cuda()
+            evals[:] = self.sum_(t).cpu().numpy()
+        return evals
+
+
+def make_shards(Ngw, Nstates):
+    """The SCF's work split over the default process group: by k-points, or
+    for a single k-point with more than one rank, inside the Gamma point
+    (pwb200.gshard: bands for op_H and the density, plane-wave rows for the
+    Rayleigh-Ritz products)."""
+    import torch.distributed as dist
+    world = dist.get_world_size() if dist.is_available() and dist.is_initialized() else 1
+    if world > 1 and len(Ngw) == 1:
+        from .gshard import GammaShards
+        return GammaShards()
+    return KShards(Ngw, Nstates)

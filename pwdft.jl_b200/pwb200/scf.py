@@ -153,9 +153,14 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     crng = np.random.default_rng(seed + 1)   # Lanczos start vectors of CheFSI
     mixed = precision == "mixed"
     dt = torch.complex64 if mixed else torch.complex128
-    from .kshard import KShards
-    shards = KShards(b.Ngw, Nstates)
+    from .kshard import make_shards
+    shards = make_shards(b.Ngw, Nstates)
+    gamma = shards.kind == "gamma"
+    if gamma and update_psi != "LOBPCG":
+        raise ValueError("Gamma-point sharding over ranks runs update_psi='LOBPCG' only")
     mine = shards.mine
+    from .gshard import split
+    ba, bb = split(Nstates, shards.world)[shards.rank] if gamma else (0, Nstates)
     if savewfc and shards.world > 1:
         raise ValueError("savewfc with k-point sharding: write each rank's blocks with pwb200.io instead")
     if psiks is None:
@@ -182,12 +187,18 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         t0 = time.perf_counter()
         nit = [0]
         evals[:] = 0.0
-        if batched and update_psi == "LOBPCG" and mine:
+        if gamma:
+            # one k-point, its work split over the ranks (pwb200.gshard)
+            from .gshard import diag_LOBPCG_gamma
+            ev, n = diag_LOBPCG_gamma(ctx, psiks[0], shards, tol=ethr, NiterMax=lobpcg_maxiter, Nstates_conv=Nocc)
+            evals[:, 0] = ev
+            nit.append(n)
+        elif batched and update_psi == "LOBPCG" and mine:
             # every k-point of this rank advanced together (pw_lobpcg_multi)
             ev, n = ctx.lobpcg_multi(mine, 0, [psiks[ik] for ik in mine], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
             evals[:, mine] = ev
             nit.append(n)
-        for ik in ([] if (batched and update_psi == "LOBPCG") else mine):
+        for ik in ([] if (gamma or (batched and update_psi == "LOBPCG")) else mine):
             if update_psi == "LOBPCG":
                 ev, n = ctx.lobpcg(ik, 0, psiks[ik], tol=ethr, nitermax=lobpcg_maxiter, nconv=Nocc)
             elif update_psi == "davidson":
@@ -204,7 +215,7 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
             evals[:, ik] = ev
             nit.append(n)
         if shards.world > 1:
-            evals[:] = shards.sum_(torch.from_numpy(evals).to(dev)).cpu().numpy()
+            shards.reduce_evals(evals)
         sync()
         mTS = 0.0
         if use_smearing:
@@ -212,7 +223,8 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         t1 = time.perf_counter()
         rho_new.zero_()
         for j, ik in enumerate(mine):
-            ctx.calc_rhoe(ik, psiks[ik], wk[ik] * Focc[:, ik], rho_new, accumulate=(j > 0))
+            if bb > ba:
+                ctx.calc_rhoe(ik, psiks[ik][ba:bb], wk[ik] * Focc[ba:bb, ik], rho_new, accumulate=(j > 0))
         shards.sum_(rho_new)
         if Ham.sym is not None:
             ctx.symmetrize_rhoe(rho_new)
@@ -227,9 +239,10 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
         sums = ctx.update(rho, Vps)
         Ek = En = 0.0
         for ik in mine:
-            e2 = ctx.band_energies(ik, psiks[ik], wk[ik] * Focc[:, ik])
-            Ek += e2[0]
-            En += e2[1]
+            if bb > ba:
+                e2 = ctx.band_energies(ik, psiks[ik][ba:bb], wk[ik] * Focc[ba:bb, ik])
+                Ek += e2[0]
+                En += e2[1]
         if shards.world > 1:
             Ek, En = [float(v) for v in shards.sum_(torch.tensor([Ek, En], dtype=torch.float64, device=dev)).tolist()]
         E = {"Kinetic": Ek, "Ps_loc": sums[1] * dVol, "Ps_nloc": En, "Hartree": 0.5 * sums[0] * dVol,

@@ -45,6 +45,12 @@ class NumpyCtx:
         Sv = torch.from_numpy(np.ascontiguousarray(S[:, :k].T)) if vectors else None
         return torch.from_numpy(lam[:k].copy()), Sv
 
+    def chol_rinv(self, C):
+        import torch
+        from oracle.lobpcg import _chol_upper
+        R = _chol_upper(C.numpy().T)
+        return torch.from_numpy(np.ascontiguousarray(np.linalg.inv(R).T))
+
     def calc_grad(self, ik, ispin, psi, Focc, wk):
         import torch
         from oracle import ops
