@@ -502,7 +502,11 @@ def main():
     # launch parameters from the library's autotuner (timed candidates, no
     # cache file): the mixed-precision path is tuned before its timing, the
     # FP64 path before its own
-    tune_mixed = ctx.autotune(0, nbands, pwb200.PW_C64)
+    # (PW_BENCH_NO_AUTOTUNE=1 keeps the built-in defaults: profiling captures
+    # of one kernel instantiation)
+    no_tune = os.environ.get("PW_BENCH_NO_AUTOTUNE") == "1"
+    notune = (ctx.get_tuning(), {})
+    tune_mixed = notune if no_tune else ctx.autotune(0, nbands, pwb200.PW_C64)
 
     if dist:
         dist.barrier()
@@ -517,7 +521,7 @@ def main():
     n1 = ctx._L.pw_launch_count(ctx.h)
     launches = (n1 - n0) * args.steps // (args.steps + args.warmup)
     t_fft = time_device(ctx, x32, y32, pwb200.PW_OP_VLOC, args.steps, args.warmup, flush)
-    tune_fp64 = ctx.autotune(0, nbands, pwb200.PW_C128)
+    tune_fp64 = notune if no_tune else ctx.autotune(0, nbands, pwb200.PW_C128)
     t_fp64 = time_device(ctx, x64, y64, OPS, max(10, args.steps // 4), args.warmup, flush)
     for _ in range(max(1, int(0.5 / max(1e-4, sum(t_fp64) / len(t_fp64) * 1e-3 * 60)))):
         # keep the GPU busy on the timed arms long enough for the clock samples

@@ -47,6 +47,8 @@ struct KPlan {
     const int *xa;         // [Nxa] active x values
     const double *Gk2;     // [Ngw] |G+k|^2
     const float *Gk2f;     // [Ngw] |G+k|^2 (FP32 copy)
+    const double *ent_g2;  // [Ngw] |G+k|^2 of entry e (entry order: coalesced in the z passes)
+    const float *ent_g2f;  // [Ngw] FP32 copy
 };
 
 // One k-point of a batched op_H (every k-point and band in one launch per

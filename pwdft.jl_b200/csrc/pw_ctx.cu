@@ -36,6 +36,8 @@ struct KData {
     int *d_col_ia = nullptr, *d_col_j = nullptr, *d_xa = nullptr;
     double *d_Gk2 = nullptr;
     float *d_Gk2f = nullptr;
+    double *d_eg2 = nullptr;   // |G+k|^2 in entry order
+    float *d_eg2f = nullptr;
     double2 *d_beta64 = nullptr;
     float2 *d_beta32 = nullptr;
     UmmaOperand beta_tn;  // split-BF16 betaNL for betaNL' psi   (tensor-core path)
@@ -268,6 +270,14 @@ int build_kdata(pw_ctx *c, KData &kd, int64_t Ngw, const int64_t *idx, int base,
     for (int64_t g = 0; g < Ngw; ++g) g2f[g] = (float)g2[g];
     if ((s = upload(c, &kd.d_Gk2, g2))) return s;
     if ((s = upload(c, &kd.d_Gk2f, g2f))) return s;
+    std::vector<double> eg2(Ngw);
+    std::vector<float> eg2f(Ngw);
+    for (int64_t e = 0; e < Ngw; ++e) {
+        eg2[e] = g2[e_igw[e]];
+        eg2f[e] = g2f[e_igw[e]];
+    }
+    if ((s = upload(c, &kd.d_eg2, eg2))) return s;
+    if ((s = upload(c, &kd.d_eg2f, eg2f))) return s;
     (void)N3;
     return PW_OK;
 }
@@ -298,6 +308,8 @@ FftLaunch make_launch_kd(const pw_ctx *c, const KData &kd) {
     L.kp.xa = kd.d_xa;
     L.kp.Gk2 = kd.d_Gk2;
     L.kp.Gk2f = kd.d_Gk2f;
+    L.kp.ent_g2 = kd.d_eg2;
+    L.kp.ent_g2f = kd.d_eg2f;
     L.dx = c->dx;
     L.dy = c->dy;
     L.dz = c->dz;

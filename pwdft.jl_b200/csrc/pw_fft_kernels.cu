@@ -92,7 +92,7 @@ k_zfwd(KPlan kp, FftDim dz, const Cx<T> *__restrict__ twz, const Cx<T> *__restri
         const int igw = kp.ent_igw[e];
         Cx<T> out = Z[kp.ent_kz[e] * Cg + cl];
         if (flags & 2) {
-            const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[igw] : (T)kp.Gk2f[igw];
+            const T g2 = sizeof(T) == 8 ? (T)kp.ent_g2[e] : (T)kp.ent_g2f[e];
             out = cadd(out, cscale(ps[igw], (T)0.5 * g2));
         }
         if (flags & 4) out = cadd(out, hs[igw]);
@@ -423,7 +423,8 @@ __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restri
             kin[u] = cmake((T)0, (T)0);
             acc[u] = cmake((T)0, (T)0);
             if (flags & 2) {
-                const T g2 = sizeof(T) == 8 ? (T)kp.Gk2[ig[u]] : (T)kp.Gk2f[ig[u]];
+                const int e = min(eb + u * (int)blockDim.x, e1 - 1);
+                const T g2 = sizeof(T) == 8 ? (T)kp.ent_g2[e] : (T)kp.ent_g2f[e];
                 kin[u] = cscale(ps[ig[u]], (T)0.5 * g2);
             }
             if (flags & 4) acc[u] = hs[ig[u]];
