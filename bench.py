@@ -50,11 +50,12 @@ DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) of one FP32 pruned-FFT round trip of the Si64
-# op_H (160 bands: kf_zinv + kx_plane_vloc + kf_zfwd over two band chunks),
-# from one capture of this bench:
-#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 PW_BENCH_NO_MULTIK=1 ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum
-#     --clock-control none -k regex:"kf_z|kx_plane" -s 12 -c 6 python bench.py --steps 3 --warmup 3
-FFT_TRAFFIC_BYTES = {"si64": 262.8e6}
+# op_H (160 bands: kf_zinv + kx_plane_vloc + kf_zfwd over two band batches),
+# from one --set full capture of each kernel of the first batch (83 bands)
+# scaled by 160/83:
+#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 PW_BENCH_NO_MULTIK=1 PW_BENCH_NO_AUTOTUNE=1 ncu --set full
+#     --clock-control none -k regex:<kernel> -s 6 -c 1 python bench.py --steps 3 --warmup 3
+FFT_TRAFFIC_BYTES = {"si64": 267.7e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -354,7 +355,8 @@ def multik_comparison(device, steps, flush):
     reduced by time reversal, 10 bands per k-point, V_loc = V_Ps_loc + a
     seeded smooth field, psi seeded and orthonormal (FP32).  Three arms on
     the same blocks: a host loop of pw_apply per k-point, one pw_apply_multi
-    (one launch per stage for all k-points), and its CUDA-graph replay;
+    (one launch per stage for all k-points), its CUDA-graph replay, and all
+    stages in one persistent cooperative launch (PW_PERSISTENT);
     device time per full op_H, L2 flushed between steps."""
     import torch
     import pwb200
@@ -380,7 +382,8 @@ def multik_comparison(device, steps, flush):
             ctx.apply(ik, 0, X[ik], Y[ik])
 
     arms = {"per_k_loop": loop, "batched": lambda: ctx.apply_multi(iks, 0, X, Y),
-            "batched_graph": lambda: ctx.apply_multi(iks, 0, X, Y, graph=True)}
+            "batched_graph": lambda: ctx.apply_multi(iks, 0, X, Y, graph=True),
+            "batched_persistent": lambda: ctx.apply_multi(iks, 0, X, Y, persistent=True)}
     res = {}
     stream = torch.cuda.current_stream()
     for name, fn in arms.items():

@@ -53,6 +53,7 @@ extern "C" {
 #define PW_OP_H        7u   /* op_H!        op_H.jl:53-63          */
 #define PW_ACCUMULATE  0x100u
 #define PW_GRAPH       0x200u   /* pw_apply_multi: replay a captured CUDA graph */
+#define PW_PERSISTENT  0x400u   /* pw_apply_multi: every stage in one cooperative launch */
 
 typedef struct pw_ctx pw_ctx;
 
@@ -175,7 +176,12 @@ int pw_apply(pw_ctx *ctx, int ik, int ispin, int dtype, const void *psi,
  * cube grids of 27, 75 or 120 points, at most 65535 bands and 2048
  * projectors.  With PW_GRAPH the launches are captured in a CUDA graph and
  * a later call with the same k-points, blocks, flags and buffers replays
- * it. */
+ * it.  With PW_PERSISTENT all stages run in one cooperative launch whose
+ * CTAs loop over the work of each stage, separated by bounded grid
+ * barriers (it falls back to the per-stage launches when one CTA per SM
+ * does not fit); the per-stage launches are the default because they
+ * measured faster (the fused kernel holds the registers of its largest
+ * stage throughout). */
 int pw_apply_multi(pw_ctx *ctx, int nk, const int *iks, int ispin, int dtype,
                    void *const *psi, void *const *Hpsi, const int64_t *ld,
                    const int *nb, unsigned ops);

@@ -119,6 +119,8 @@ struct pw_ctx {
     DevBuf mk_tab;
     uint64_t mk_key = 0;
     cudaGraphExec_t mk_exec = nullptr;
+    int mk_nlaunch = 0;
+
     cudaStream_t cap_stream = nullptr;
     // host drop-ins: copy streams and per-chunk events of the pipelined op_H
     cudaStream_t cp_in = nullptr, cp_out = nullptr;
@@ -647,7 +649,9 @@ extern "C" int pw_check_device(pw_ctx *c) {
     int h = 0;
     CK(c, cudaStreamSynchronize(c->stream));
     CK(c, cudaMemcpy(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h) return fail(c, PW_ERR_TIMEOUT, "a bounded wait in a tensor-core kernel expired (code %d)", h);
+    if (h)
+        return fail(c, PW_ERR_TIMEOUT, "a bounded device-side wait expired (code %d: 1-2 tensor-core GEMM pipeline, "
+                    "3 grid barrier of the persistent batched op_H)", h);
     return PW_OK;
 }
 
@@ -906,14 +910,15 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
     if ((s = ensure(c, c->A, aoff * es))) return s;
     const size_t tab_bytes = (size_t)nk * sizeof(MkK), bk_bytes = (size_t)nbands * sizeof(int);
     const size_t bk_off = (tab_bytes + 255) / 256 * 256;
-    if ((s = ensure(c, c->mk_tab, bk_off + bk_bytes))) return s;
+    const size_t ctr_off = (bk_off + bk_bytes + 255) / 256 * 256;   // grid-barrier counter of the persistent launch
+    if ((s = ensure(c, c->mk_tab, ctr_off + 256))) return s;
     const void *V = sizeof(T) == 8 ? (const void *)(c->d_V64 + (size_t)ispin * c->N)
                                    : (const void *)(c->d_V32 + (size_t)ispin * c->N);
     const int flags = ((o & PW_OP_K) ? 2 : 0) | ((ops & PW_ACCUMULATE) ? 4 : 0);
     const FftLaunch L = make_launch<T>(c, kx);
     const MkK *d_tab = (const MkK *)c->mk_tab.p;
     const int *d_bk = (const int *)((const char *)c->mk_tab.p + bk_off);
-    const int nlaunch = vnl ? 4 : 3;
+    unsigned *d_ctr = (unsigned *)((char *)c->mk_tab.p + ctr_off);
     // graph replay: same blocks, k-points, flags and buffers as the captured call
     uint64_t key = 1469598103934665603ull;
     key = fnv(key, tab.data(), tab_bytes);
@@ -921,15 +926,33 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
     key = fnv(key, &c->A.p, sizeof(void *));
     key = fnv(key, &c->mk_tab.p, sizeof(void *));
     key = fnv(key, &flags, sizeof(flags));
+    const unsigned pflag = ops & PW_PERSISTENT;
+    key = fnv(key, &pflag, sizeof(pflag));
     key = fnv(key, &nbands, sizeof(nbands));
     if ((ops & PW_GRAPH) && c->mk_exec && key == c->mk_key) {
         CK(c, cudaGraphLaunch(c->mk_exec, c->stream));
-        c->launches += nlaunch;
+        c->launches += c->mk_nlaunch;
         return PW_OK;
     }
     CK(c, cudaMemcpyAsync(c->mk_tab.p, tab.data(), tab_bytes, cudaMemcpyHostToDevice, c->stream));
     CK(c, cudaMemcpyAsync((char *)c->mk_tab.p + bk_off, band_k.data(), bk_bytes, cudaMemcpyHostToDevice, c->stream));
+    // one persistent cooperative launch for every stage (the per-stage
+    // launches when it does not fit or a stream capture refuses it)
+    bool persistent = (ops & PW_PERSISTENT) != 0;
+    int nlaunch = 1;
     auto run = [&](cudaStream_t st) {
+        if (persistent) {
+            const cudaError_t e = launch_multik_persistent<T>(L, d_tab, d_bk, nbands, maxcol, V, c->A.p, flags,
+                                                              c->d_Drow, c->d_Dcol, c->d_Dval, vnl ? c->nbeta : 0,
+                                                              d_ctr, c->d_err, st);
+            if (e == cudaSuccess) {
+                nlaunch = 1;
+                return e;
+            }
+            if (e != cudaErrorCooperativeLaunchTooLarge && e != cudaErrorNotSupported) return e;
+            persistent = false;
+        }
+        nlaunch = vnl ? 4 : 3;
         return launch_multik<T>(L, d_tab, d_bk, nk, nbands, maxnb, maxcol, V, c->A.p, flags, c->d_Drow, c->d_Dcol,
                                 c->d_Dval, vnl ? c->nbeta : 0, st);
     };
@@ -946,8 +969,18 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
         }
         cudaGraph_t g = nullptr;
         CK(c, cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed));
-        const cudaError_t e = run(c->cap_stream);
-        const cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
+        cudaError_t e = run(c->cap_stream);
+        cudaError_t e2 = cudaStreamEndCapture(c->cap_stream, &g);
+        if ((e != cudaSuccess || e2 != cudaSuccess) && persistent) {
+            // the capture refused the cooperative launch: capture the per-stage launches
+            if (g) cudaGraphDestroy(g);
+            g = nullptr;
+            cudaGetLastError();
+            persistent = false;
+            CK(c, cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeRelaxed));
+            e = run(c->cap_stream);
+            e2 = cudaStreamEndCapture(c->cap_stream, &g);
+        }
         if (e != cudaSuccess || e2 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             return fail(c, PW_ERR_CUDA, "capturing the batched op_H failed: %s",
@@ -960,6 +993,7 @@ int apply_multi_T(pw_ctx *c, int nk, const int *iks, int ispin, void *const *psi
             return fail(c, PW_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(e3));
         }
         c->mk_key = key;
+        c->mk_nlaunch = nlaunch;
     }
     return PW_OK;
 }
@@ -971,7 +1005,7 @@ extern "C" int pw_apply_multi(pw_ctx *c, int nk, const int *iks, int ispin, int 
     int s;
     if ((s = check_dtype(c, dtype))) return s;
     if (nk <= 0 || !iks || !psi || !Hpsi || !ld || !nb) return fail(c, PW_ERR_ARG, "bad pw_apply_multi arguments");
-    if (ops & ~(PW_OP_H | PW_ACCUMULATE | PW_GRAPH)) return fail(c, PW_ERR_ARG, "unknown op flags 0x%x", ops);
+    if (ops & ~(PW_OP_H | PW_ACCUMULATE | PW_GRAPH | PW_PERSISTENT)) return fail(c, PW_ERR_ARG, "unknown op flags 0x%x", ops);
     for (int i = 0; i < nk; ++i) {
         if ((s = check_k(c, iks[i]))) return s;
         if (!psi[i] || !Hpsi[i]) return fail(c, PW_ERR_ARG, "NULL wavefunction pointer (entry %d)", i);
@@ -1120,7 +1154,10 @@ extern "C" int pw_op_H_host(pw_ctx *c, int ik, int ispin, const double *psi, dou
     // Pipelined over band chunks: the host-to-device copy of chunk i+1 and the
     // device-to-host copy of chunk i-1 run on their own streams while chunk i
     // computes on the context stream (each chunk has its own slice of the
-    // staging buffers, so no slice is reused within a call).
+    // staging buffers, so no slice is reused within a call).  Equal chunks of
+    // about 32 bands (a ramp of small first and last chunks measured no gain
+    // for the mixed path and 14 % slower for FP64, whose op_H outweighs the
+    // copies).
     const int nch = std::max(1, std::min(8, nb / 32));
     const int cb = (nb + nch - 1) / nch;
     if (!c->cp_in) {

@@ -4,7 +4,7 @@
 // pw_fft_tmpl.cuh, but a stage may use a composite radix R = R1*R2 whose
 // R-point DFT runs inside one thread (Cooley-Tukey split: R2 DFTs of size R1,
 // twiddles W_R^(n2 k1), R1 DFTs of size R2).  Fewer stages means fewer
-// shared-memory round trips per line: 75 = 15*5 and 120 = 24*5 take two
+// shared-memory round trips per line: 75 = 15*5 and 120 = 15*8 take two
 // passes instead of three, 27 takes one.
 #pragma once
 #include "pw_fft.cuh"
@@ -92,7 +92,9 @@ template <typename T> struct Dft<T, 27> { static __device__ __forceinline__ void
 template <int N> struct FPlan;
 template <> struct FPlan<27> { static constexpr int nst = 1; static __host__ __device__ constexpr int r(int) { return 27; } };
 template <> struct FPlan<75> { static constexpr int nst = 2; static __host__ __device__ constexpr int r(int s) { return s == 0 ? 15 : 5; } };
-template <> struct FPlan<120> { static constexpr int nst = 2; static __host__ __device__ constexpr int r(int s) { return s == 0 ? 24 : 5; } };
+// 120 = 15 * 8: 91-110 registers in the z and plane kernels (24 * 5 needed 128 and spilled
+// 72-432 bytes); measured Si216 FFT round trip 7.95 -> 6.52 ms
+template <> struct FPlan<120> { static constexpr int nst = 2; static __host__ __device__ constexpr int r(int s) { return s == 0 ? 15 : 8; } };
 
 template <int N> __host__ __device__ constexpr int fp_ns(int s) {
     int p = 1;
@@ -136,20 +138,19 @@ template <int N, int S> __host__ __device__ constexpr int tw_step() {
     return (FPlan<N>::nst == 2 && S == 0) ? 1 : N / FPlan<N>::r(S);
 }
 // twiddle of element r of stage-S butterfly jm (jm < N_S, the stage's span)
-// Padded element positions of a line held in shared memory.  With R0 = 24
-// (120 = 24 * 5) the first stage's outputs x = 24 j + r put lanes j = 0, 2,
-// 4 of a line on one bank; one spare word after every R0 elements
-// (pos(x) = x + x / R0) and a line stride fp_xs = 125 (13 mod 16) put the 16
-// lanes of a half-warp on 16 bank pairs in the first stage and cost at most
-// a 2-way conflict in the second.  Other plans are unpadded.
-template <int N> __host__ __device__ constexpr int fp_pad() { return N == 120 ? 1 : 0; }
+// Padded element positions of a line held in shared memory: pos(x) = x +
+// (x / R0) * fp_pad, line stride fp_xs.  A plan whose first-stage outputs put
+// several lanes of a half-warp on one bank can pad here (the earlier
+// 120 = 24 * 5 plan needed one spare word per 24 elements and stride 125);
+// the current plans are unpadded.
+template <int N> __host__ __device__ constexpr int fp_pad() { return 0; }
 template <int N> __host__ __device__ constexpr int fp_pos(int x) {
     if constexpr (fp_pad<N>() == 0)
         return x;
     else
         return x + (x / FPlan<N>::r(0)) * fp_pad<N>();
 }
-template <int N> __host__ __device__ constexpr int fp_xs() { return fp_pad<N>() == 0 ? N : 125; }
+template <int N> __host__ __device__ constexpr int fp_xs() { return fp_pad<N>() == 0 ? N : N + N / FPlan<N>::r(0) * fp_pad<N>() + 1; }
 static_assert(fp_xs<120>() >= fp_pos<120>(119) + 1, "padded line fits its stride");
 
 template <int N, int S> __device__ __forceinline__ int tw_at(int r, int jm) {

@@ -21,6 +21,8 @@
 //
 // HBM traffic per band: psi once in, Hpsi once out, A (Ncol*N3 complex)
 // written/read twice, V once per plane batch (L2-resident across bands).
+#include <algorithm>
+
 #include "pw_fft.cuh"
 #include "pw_fft_tmpl.cuh"
 #include "pw_fft_fused.cuh"
@@ -304,9 +306,9 @@ template <typename T, int N> __host__ __device__ constexpr int zrow(int Cg) {
 template <typename T> struct MinBlocks;
 template <> struct MinBlocks<float> { static constexpr int v = 2; };
 template <> struct MinBlocks<double> { static constexpr int v = 2; };
-// z passes: three CTAs per SM (80 registers, no spills) where the radix
-// allows it; the radix-24 butterflies of the 120-point lines would spill
-template <typename T, int N3> struct ZBlocks { static constexpr int v = (sizeof(T) == 4 && N3 <= 75) ? 3 : 2; };
+// z passes: three CTAs per SM for every FP32 line length (80 registers, no
+// spills; measured: Si216 FFT round trip 6.51 -> 6.31 ms against two CTAs)
+template <typename T, int N3> struct ZBlocks { static constexpr int v = sizeof(T) == 4 ? 3 : 2; };
 
 // z-pass bodies for one band: ps / hs its sphere coefficients, Ab its
 // [z][column] block of the intermediate, column group blockIdx.x
@@ -334,11 +336,11 @@ template <typename T> __device__ __forceinline__ void cp_async_cx(Cx<T> *smem, c
 }
 template <typename T, int N3>
 __device__ __forceinline__ void zinv_band(const KPlan &kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ ps,
-                                          Cx<T> *__restrict__ Ab, int Cg) {
+                                          Cx<T> *__restrict__ Ab, int Cg, int gx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *Z = tw + N3;
-    const int c0 = blockIdx.x * Cg;
+    const int c0 = gx * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int Zs = zrow<T, N3>(Cg);
@@ -382,16 +384,16 @@ __global__ void __launch_bounds__(FFT_THREADS, ZBlocks<T, N3>::v)
 kf_zinv(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ psi, int64_t ld, Cx<T> *__restrict__ A,
         int Cg) {
     const int b = blockIdx.y;
-    zinv_band<T, N3>(kp, twz, psi + (size_t)b * ld, A + (size_t)b * N3 * kp.Ncol, Cg);
+    zinv_band<T, N3>(kp, twz, psi + (size_t)b * ld, A + (size_t)b * N3 * kp.Ncol, Cg, blockIdx.x);
 }
 
 template <typename T, int N3>
 __device__ __forceinline__ void zfwd_band(const KPlan &kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ Ab,
-                                          const Cx<T> *__restrict__ ps, Cx<T> *__restrict__ hs, int Cg, int flags) {
+                                          const Cx<T> *__restrict__ ps, Cx<T> *__restrict__ hs, int Cg, int flags, int gx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *Z = tw + N3;
-    const int c0 = blockIdx.x * Cg;
+    const int c0 = gx * Cg;
     const int cn = min(Cg, kp.Ncol - c0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int Zs = zrow<T, N3>(Cg);
@@ -445,7 +447,8 @@ __global__ void __launch_bounds__(FFT_THREADS, ZBlocks<T, N3>::v)
 kf_zfwd(KPlan kp, const Cx<T> *__restrict__ twz, const Cx<T> *__restrict__ A, const Cx<T> *__restrict__ psi,
         Cx<T> *__restrict__ Hpsi, int64_t ld, int Cg, int flags) {
     const int b = blockIdx.y;
-    zfwd_band<T, N3>(kp, twz, A + (size_t)b * N3 * kp.Ncol, psi + (size_t)b * ld, Hpsi + (size_t)b * ld, Cg, flags);
+    zfwd_band<T, N3>(kp, twz, A + (size_t)b * N3 * kp.Ncol, psi + (size_t)b * ld, Hpsi + (size_t)b * ld, Cg, flags,
+                     blockIdx.x);
 }
 
 template <typename T, int N1, int N2>
@@ -464,14 +467,14 @@ __device__ __forceinline__ void plane_to_real(const KPlan &kp, Cx<T> *S, Cx<T> *
 template <typename T, int N1, int N2>
 __device__ __forceinline__ void plane_vloc_band(const KPlan &kp, const Cx<T> *__restrict__ twx,
                                                 const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
-                                                Cx<T> *__restrict__ Ab, int Jc) {
+                                                Cx<T> *__restrict__ Ab, int Jc, int kz) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int Nxa = kp.Nxa, Ncol = kp.Ncol;
     Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
     Cx<T> *ty = tx + N1;
     Cx<T> *S = ty + N2;
     Cx<T> *X = S + Nxa * N2;
-    const int kz = blockIdx.x;
+    
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int i = threadIdx.x; i < N1; i += blockDim.x) tx[i] = twx[tw_src<T, N1>(i)];
     for (int i = threadIdx.x; i < N2; i += blockDim.x) ty[i] = twy[tw_src<T, N2>(i)];
@@ -502,7 +505,7 @@ template <typename T, int N1, int N2>
 __global__ void __launch_bounds__(FFT_THREADS, MinBlocks<T>::v)
 kf_plane_vloc(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
               Cx<T> *__restrict__ A, int Jc) {
-    plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + (size_t)blockIdx.y * kp.N3 * kp.Ncol, Jc);
+    plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + (size_t)blockIdx.y * kp.N3 * kp.Ncol, Jc, blockIdx.x);
 }
 
 template <typename T, int N1, int N2>
@@ -567,16 +570,16 @@ struct PlaneXSmem {
 // A) go through every phase together: each block barrier then separates
 // twice the line FFTs, and V(r), the twiddles and the active-x map are
 // loaded once for all of them.
-// Row stride of the sub-plane S: the padded line stride of the fused plan
-// (elements of row ia at ia * LD + fp_pos(y)); 125 on the 120-point grid,
-// unpadded elsewhere (on the 75-point grid padding would cost the third
-// sub-plane per CTA).
+// Row stride of the sub-plane S: the line stride of the fused plan (elements
+// of row ia at ia * LD + fp_pos(y)); the current plans are unpadded (on the
+// 75-point grid padding would cost the third sub-plane per CTA).
 template <int N> __host__ __device__ constexpr int plane_ld() { return pwf::fp_xs<N>(); }
 
 template <int N1, int N2, bool VS, int BPC = 1>
 __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 *__restrict__ twx,
                                                   const float2 *__restrict__ twy, const float *__restrict__ Vr,
-                                                  float2 *__restrict__ Ab, int nbh = 1, size_t astr = 0) {
+                                                  float2 *__restrict__ Ab, int kz, int nbh = 1,
+                                                  size_t astr = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = float;
     constexpr int G = pwf::fp_group<N1>();
@@ -592,7 +595,7 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
     Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * XS;
     float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * XS);
     short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
-    const int kz = blockIdx.x;
+    
     const float *Vp = Vr + (size_t)kz * N1 * N2;
     if constexpr (VS)
         for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[i], &Vp[i]);
@@ -651,7 +654,7 @@ kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict
               float2 *__restrict__ A, int nb) {
     const int b0 = blockIdx.y * BPC;
     const size_t astr = (size_t)kp.N3 * kp.Ncol;
-    plane_vloc_x_band<N1, N2, VS, BPC>(kp, twx, twy, Vr, A + b0 * astr, min(BPC, nb - b0), astr);
+    plane_vloc_x_band<N1, N2, VS, BPC>(kp, twx, twy, Vr, A + b0 * astr, blockIdx.x, min(BPC, nb - b0), astr);
 }
 
 // calc_rhoe: bands [g*Bg, min(nb, (g+1)*Bg)) of plane kz; the weighted
@@ -724,7 +727,8 @@ mk_zinv(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> 
     const KPlan kp = K.kp;
     if (blockIdx.x * Cg >= kp.Ncol) return;
     const int b = blockIdx.y - K.band0;
-    zinv_band<T, N3>(kp, twz, (const Cx<T> *)K.psi + (size_t)b * K.ld, A + K.a_off + (size_t)b * N3 * kp.Ncol, Cg);
+    zinv_band<T, N3>(kp, twz, (const Cx<T> *)K.psi + (size_t)b * K.ld, A + K.a_off + (size_t)b * N3 * kp.Ncol, Cg,
+                     blockIdx.x);
 }
 
 template <typename T, int N3>
@@ -736,7 +740,7 @@ mk_zfwd(const MkK *__restrict__ ks, const int *__restrict__ band_k, const Cx<T> 
     if (blockIdx.x * Cg >= kp.Ncol) return;
     const int b = blockIdx.y - K.band0;
     zfwd_band<T, N3>(kp, twz, A + K.a_off + (size_t)b * N3 * kp.Ncol, (const Cx<T> *)K.psi + (size_t)b * K.ld,
-                     (Cx<T> *)K.Hpsi + (size_t)b * K.ld, Cg, flags);
+                     (Cx<T> *)K.Hpsi + (size_t)b * K.ld, Cg, flags, blockIdx.x);
 }
 
 template <int N1, int N2, bool VS>
@@ -746,7 +750,7 @@ mk_plane_vloc_x(const MkK *__restrict__ ks, const int *__restrict__ band_k, cons
     const MkK &K = ks[band_k[blockIdx.y]];
     const KPlan kp = K.kp;
     const int b = blockIdx.y - K.band0;
-    plane_vloc_x_band<N1, N2, VS>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol);
+    plane_vloc_x_band<N1, N2, VS>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, blockIdx.x);
 }
 
 template <typename T, int N1, int N2>
@@ -756,7 +760,7 @@ mk_plane_vloc(const MkK *__restrict__ ks, const int *__restrict__ band_k, const 
     const MkK &K = ks[band_k[blockIdx.y]];
     const KPlan kp = K.kp;
     const int b = blockIdx.y - K.band0;
-    plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, Jc);
+    plane_vloc_band<T, N1, N2>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, Jc, blockIdx.x);
 }
 
 // Small cube grids whose lines fit one lane (single-stage register FFT, a
@@ -766,10 +770,10 @@ mk_plane_vloc(const MkK *__restrict__ ks, const int *__restrict__ band_k, const 
 // of the sub-plane S, x lines its columns), so no lane reads what another
 // writes within a pass.
 template <int N>
-__global__ void __launch_bounds__(FFT_THREADS)
-mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nbands, int nxa_max,
-                const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
-                float2 *__restrict__ A) {
+__device__ __forceinline__ void plane_vloc_w_body(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nbands,
+                                                  int nxa_max, const float2 *__restrict__ twx,
+                                                  const float2 *__restrict__ twy, const float *__restrict__ Vr,
+                                                  float2 *__restrict__ A, int kz, int bgroup) {
     static_assert(pwf::FPlan<N>::nst == 1 && pwf::fp_group<N>() >= N && pwf::fp_xs<N>() == N, "one line per lane");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = float;
@@ -783,14 +787,13 @@ mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int 
     Cx<T> *S = wbase + (size_t)warp * wsz;
     Cx<T> *Xw = S + (size_t)nxa_max * N;
     short *iax = reinterpret_cast<short *>(Xw + N * N);
-    const int kz = blockIdx.x;
     for (int i = threadIdx.x; i < N * N; i += FFT_THREADS) Vs[i] = Vr[(size_t)kz * N * N + i];
     for (int i = threadIdx.x; i < N; i += FFT_THREADS) {
         tx[i] = twx[tw_src<float, N>(i)];
         ty[i] = twy[tw_src<float, N>(i)];
     }
     __syncthreads();
-    const int gb = blockIdx.y * NW + warp;
+    const int gb = bgroup * NW + warp;
     if (gb >= nbands) return;
     const MkK &K = ks[band_k[gb]];
     const KPlan kp = K.kp;
@@ -822,18 +825,26 @@ mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int 
     for (int c = lane; c < Ncol; c += 32) Ap[c] = S[kp.col_ia[c] * N + kp.col_j[c]];
 }
 
+template <int N>
+__global__ void __launch_bounds__(FFT_THREADS)
+mk_plane_vloc_w(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nbands, int nxa_max,
+                const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float *__restrict__ Vr,
+                float2 *__restrict__ A) {
+    plane_vloc_w_body<N>(ks, band_k, nbands, nxa_max, twx, twy, Vr, A, blockIdx.x, blockIdx.y);
+}
+
 // op_V_Ps_nloc for small projector sets, one CTA per band of the batch:
 // P = betaNL' psi (FP64 sums, one warp per projector), P2 = D P (the
 // (ibeta, jbeta, h) list as CSR), Hpsi += betaNL P2
 template <typename T>
-__global__ void __launch_bounds__(256)
-mk_vnl(const MkK *__restrict__ ks, const int *__restrict__ band_k, const int *__restrict__ Drow,
-       const int *__restrict__ Dcol, const double *__restrict__ Dval, int nbeta) {
+__device__ __forceinline__ void vnl_body(const MkK *__restrict__ ks, const int *__restrict__ band_k,
+                                         const int *__restrict__ Drow, const int *__restrict__ Dcol,
+                                         const double *__restrict__ Dval, int nbeta, int band) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *P = reinterpret_cast<double2 *>(smem_raw);
     double2 *P2 = P + nbeta;
-    const MkK &K = ks[band_k[blockIdx.x]];
-    const int b = blockIdx.x - K.band0;
+    const MkK &K = ks[band_k[band]];
+    const int b = band - K.band0;
     const int ngw = K.kp.Ngw;
     const Cx<T> *beta = (const Cx<T> *)K.beta;
     const Cx<T> *ps = (const Cx<T> *)K.psi + (size_t)b * K.ld;
@@ -896,6 +907,111 @@ mk_vnl(const MkK *__restrict__ ks, const int *__restrict__ band_k, const int *__
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256)
+mk_vnl(const MkK *__restrict__ ks, const int *__restrict__ band_k, const int *__restrict__ Drow,
+       const int *__restrict__ Dcol, const double *__restrict__ Dval, int nbeta) {
+    vnl_body<T>(ks, band_k, Drow, Dcol, Dval, nbeta, blockIdx.x);
+}
+
+
+// ------------------------------------ batched op_H in one persistent launch
+// Every stage of the batched op_H (z inverse, plane pass, z forward, and the
+// nonlocal part) in one cooperative launch: each phase is a grid-stride loop
+// over its work items with the bodies of the per-stage kernels above, and a
+// bounded grid barrier separates the phases (the plane pass needs every
+// column of its z-plane, the forward z pass every plane of its columns, and
+// the nonlocal part adds into the finished Hpsi).  The barrier counter is
+// zeroed before the launch; a wait that gives up after PB_LIMIT polls records
+// 3 in *err (read by pw_check_device) and the kernel runs to completion.
+constexpr long long PB_LIMIT = 1ll << 22;
+__device__ __forceinline__ void grid_bar(unsigned *ctr, unsigned &tgt, int *err) {
+    __syncthreads();
+    tgt += gridDim.x;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctr, 1u);
+        if (!*(volatile int *)err) {
+            long long it = 0;
+            unsigned v;
+            do {
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+                if (++it > PB_LIMIT) {
+                    atomicExch(err, 3);
+                    break;
+                }
+            } while (v < tgt);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <typename T, int NN>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+mk_persistent(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nbands, int nxa_max, int max_ncol, int Cg,
+              int Jc, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ twy, const Cx<T> *__restrict__ twz,
+              const T *__restrict__ Vr, Cx<T> *__restrict__ A, int flags, const int *__restrict__ Drow,
+              const int *__restrict__ Dcol, const double *__restrict__ Dval, int nbeta, unsigned *ctr, int *err) {
+    unsigned tgt = 0;
+    const int ngx = (max_ncol + Cg - 1) / Cg;
+    // z inverse: (column group, band)
+#pragma unroll 1
+    for (int q = blockIdx.x; q < ngx * nbands; q += gridDim.x) {
+        const int gx = q % ngx, band = q / ngx;
+        const MkK &K = ks[band_k[band]];
+        const int b = band - K.band0;
+        if (gx * Cg < K.kp.Ncol)
+            zinv_band<T, NN>(K.kp, twz, (const Cx<T> *)K.psi + (size_t)b * K.ld, A + K.a_off + (size_t)b * NN * K.kp.Ncol,
+                             Cg, gx);
+        __syncthreads();
+    }
+    grid_bar(ctr, tgt, err);
+    // plane pass: (z-plane, band) or, for one-lane lines, (z-plane, group of 8 bands)
+    if constexpr (sizeof(T) == 4 && pwf::FPlan<NN>::nst == 1 && pwf::fp_group<NN>() >= NN) {
+        constexpr int NW = FFT_THREADS / 32;
+        const int ngroups = (nbands + NW - 1) / NW;
+    #pragma unroll 1
+    for (int q = blockIdx.x; q < NN * ngroups; q += gridDim.x) {
+            plane_vloc_w_body<NN>(ks, band_k, nbands, nxa_max, twx, twy, Vr, A, q % NN, q / NN);
+            __syncthreads();
+        }
+    } else {
+    #pragma unroll 1
+    for (int q = blockIdx.x; q < NN * nbands; q += gridDim.x) {
+            const int kz = q % NN, band = q / NN;
+            const MkK &K = ks[band_k[band]];
+            Cx<T> *Ab = A + K.a_off + (size_t)(band - K.band0) * NN * K.kp.Ncol;
+            if constexpr (sizeof(T) == 4) {
+                constexpr bool VS = NN * NN * 4 <= 32 * 1024;
+                plane_vloc_x_band<NN, NN, VS>(K.kp, twx, twy, Vr, Ab, kz);
+            } else {
+                plane_vloc_band<T, NN, NN>(K.kp, twx, twy, Vr, Ab, Jc, kz);
+            }
+            __syncthreads();
+        }
+    }
+    grid_bar(ctr, tgt, err);
+    // z forward with op_K and the gather into Hpsi
+#pragma unroll 1
+    for (int q = blockIdx.x; q < ngx * nbands; q += gridDim.x) {
+        const int gx = q % ngx, band = q / ngx;
+        const MkK &K = ks[band_k[band]];
+        const int b = band - K.band0;
+        if (gx * Cg < K.kp.Ncol)
+            zfwd_band<T, NN>(K.kp, twz, A + K.a_off + (size_t)b * NN * K.kp.Ncol, (const Cx<T> *)K.psi + (size_t)b * K.ld,
+                             (Cx<T> *)K.Hpsi + (size_t)b * K.ld, Cg, flags, gx);
+        __syncthreads();
+    }
+    if (nbeta > 0) {
+        grid_bar(ctr, tgt, err);
+#pragma unroll 1
+        for (int band = blockIdx.x; band < nbands; band += gridDim.x) {
+            vnl_body<T>(ks, band_k, Drow, Dcol, Dval, nbeta, band);
+            __syncthreads();
+        }
+    }
+}
 }  // namespace pwk
 
 // ----------------------------------------------------------- host launchers
@@ -992,9 +1108,9 @@ static cudaError_t launch_plane_vloc_xb(const FftLaunch &L, const void *Vr, void
     return cudaGetLastError();
 }
 // sub-planes per CTA (L.bpc), measured defaults: 3 on the 75-point grid
-// (Si64 round trip 0.996 -> 0.843 ms); 1 on the 120-point grid, where two
-// CTAs per SM (103 KB each) beat two sub-planes in one CTA once the padded
-// layout removed the bank conflicts (Si216 10.0 -> 8.7 ms)
+// (Si64 round trip 0.996 -> 0.843 ms); 1 on the 120-point grid (two CTAs per
+// SM beat two sub-planes in one CTA: Si216 10.0 -> 8.7 ms with the earlier
+// 24 * 5 plan); pw_autotune tries 1-3
 template <int NN>
 static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
     switch (L.bpc) {
@@ -1076,6 +1192,60 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
         mk_vnl<T><<<nbands, 256, vsm, st>>>(ks, band_k, Drow, Dcol, Dval, nbeta);
         e = cudaGetLastError();
     }
+    return e;
+}
+
+
+// The batched op_H of launch_multik as one cooperative launch of
+// mk_persistent (as many CTAs as fit on the GPU at once, each looping over
+// work items).  ctr: a device counter (zeroed here), err: the context's
+// error word.  cudaErrorCooperativeLaunchTooLarge when one CTA per SM does
+// not fit (the caller then runs launch_multik).
+template <typename T>
+cudaError_t launch_multik_persistent(const FftLaunch &L, const MkK *ks, const int *band_k, int nbands, int max_ncol,
+                                     const void *Vr, void *A, int flags, const int *Drow, const int *Dcol,
+                                     const double *Dval, int nbeta, unsigned *ctr, int *err, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    if (kp.N1 != kp.N2 || kp.N2 != kp.N3) return cudaErrorNotSupported;
+    const int Cg = L.Cg;
+    cudaError_t e = cudaErrorNotSupported;
+#define PW_CASE(NN)                                                                                                  \
+    if (kp.N1 == NN) {                                                                                               \
+        size_t sm = (size_t)(NN + NN * zrow<T, NN>(Cg)) * sizeof(Cx<T>);                                             \
+        if constexpr (sizeof(T) == 4 && pwf::FPlan<NN>::nst == 1 && pwf::fp_group<NN>() >= NN) {                    \
+            sm = std::max(sm, (2 * NN + (NN * NN + 1) / 2) * sizeof(float2) +                                         \
+                                  (FFT_THREADS / 32) * ((size_t)kp.Nxa * NN + NN * NN + (NN + 3) / 4) * sizeof(float2)); \
+        } else if constexpr (sizeof(T) == 4) {                                                                       \
+            constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
+            PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};       \
+            ps.xs = pwf::fp_xs<NN>();                                                                                \
+            sm = std::max(sm, ps.elems() * sizeof(float2));                                                          \
+        } else {                                                                                                     \
+            const PlaneSmem ps{NN, NN, kp.Nxa, L.Jc};                                                                \
+            sm = std::max(sm, ps.elems() * sizeof(Cx<T>));                                                           \
+        }                                                                                                            \
+        sm = std::max(sm, 2 * (size_t)nbeta * sizeof(double2));                                                      \
+        const void *fn = (const void *)mk_persistent<T, NN>;                                                         \
+        if ((e = set_smem<T>(fn, sm)) != cudaSuccess) return e;                                                      \
+        int dev = 0, sms = 0, per = 0;                                                                               \
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;                                                      \
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;        \
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, FFT_THREADS, sm)) != cudaSuccess) return e; \
+        if (per < 1) return cudaErrorCooperativeLaunchTooLarge;                                                      \
+        if ((e = cudaMemsetAsync(ctr, 0, sizeof(unsigned), st)) != cudaSuccess) return e;                            \
+        const int ngx = (max_ncol + Cg - 1) / Cg;                                                                    \
+        const int nblk = std::max(1, std::min(sms * per, ngx * nbands));                                            \
+        const int nxa = kp.Nxa, Jc = L.Jc;                                                                           \
+        const Cx<T> *tx = (const Cx<T> *)L.twx, *ty = (const Cx<T> *)L.twy, *tz = (const Cx<T> *)L.twz;             \
+        const T *V = (const T *)Vr;                                                                                  \
+        Cx<T> *Ap = (Cx<T> *)A;                                                                                      \
+        void *args[] = {(void *)&ks, (void *)&band_k, (void *)&nbands, (void *)&nxa, (void *)&max_ncol, (void *)&Cg, \
+                        (void *)&Jc, (void *)&tx, (void *)&ty, (void *)&tz, (void *)&V, (void *)&Ap, (void *)&flags, \
+                        (void *)&Drow, (void *)&Dcol, (void *)&Dval, (void *)&nbeta, (void *)&ctr, (void *)&err};    \
+        return cudaLaunchCooperativeKernel(fn, nblk, FFT_THREADS, args, sm, st);                                     \
+    }
+    FIXED_SIZES(PW_CASE)
+#undef PW_CASE
     return e;
 }
 
@@ -1186,6 +1356,9 @@ cudaError_t launch_zero(void *p, int Ngw, int nb, int64_t ld, cudaStream_t st) {
     template cudaError_t launch_zfwd<T>(const FftLaunch &, const void *, const void *, void *, int64_t, int, int,  \
                                         cudaStream_t);                                                               \
     template cudaError_t launch_plane_vloc<T>(const FftLaunch &, const void *, void *, int, cudaStream_t);          \
+    template cudaError_t launch_multik_persistent<T>(const FftLaunch &, const MkK *, const int *, int, int,          \
+                                                     const void *, void *, int, const int *, const int *,          \
+                                                     const double *, int, unsigned *, int *, cudaStream_t);         \
     template cudaError_t launch_multik<T>(const FftLaunch &, const MkK *, const int *, int, int, int, int,           \
                                           const void *, void *, int, const int *, const int *, const double *, int,  \
                                           cudaStream_t);                                                             \

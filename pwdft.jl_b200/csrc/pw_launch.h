@@ -58,6 +58,10 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
                           int max_ncol, const void *Vr, void *A, int flags, const int *Drow, const int *Dcol,
                           const double *Dval, int nbeta, cudaStream_t st);
 template <typename T>
+cudaError_t launch_multik_persistent(const FftLaunch &L, const MkK *ks, const int *band_k, int nbands, int max_ncol,
+                                     const void *Vr, void *A, int flags, const int *Drow, const int *Dcol,
+                                     const double *Dval, int nbeta, unsigned *ctr, int *err, cudaStream_t st);
+template <typename T>
 cudaError_t launch_plane_rho(const FftLaunch &, const void *A, int nb, int G, int Bg, const double *w, void *rho_part,
                              cudaStream_t);
 template <typename T> cudaError_t launch_rho_reduce(const void *part, int G, size_t N, double *rho, int acc, cudaStream_t);

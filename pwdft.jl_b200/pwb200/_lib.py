@@ -16,6 +16,7 @@ PW_C128, PW_C64 = 0, 1
 PW_OP_K, PW_OP_VLOC, PW_OP_VNL, PW_OP_H = 1, 2, 4, 7
 PW_ACCUMULATE = 0x100
 PW_GRAPH = 0x200
+PW_PERSISTENT = 0x400
 PW_XC_VWN, PW_XC_PBE = 0, 1
 
 STATUS_NAMES = {0: "PW_OK", 1: "PW_ERR_ARG", 2: "PW_ERR_CUDA", 3: "PW_ERR_NOMEM", 4: "PW_ERR_NOT_POSDEF",

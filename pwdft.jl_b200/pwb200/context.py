@@ -9,7 +9,8 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (lib, check, pw_grid_desc, pw_tuning, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE, PW_GRAPH)
+from ._lib import (lib, check, pw_grid_desc, pw_tuning, PW_C128, PW_C64, PW_OP_H, PW_ACCUMULATE, PW_GRAPH,
+                   PW_PERSISTENT)
 
 TUNING_FIELDS = ("band_chunk_bytes", "plane_bands", "z_columns", "gemm_splits")
 
@@ -162,7 +163,7 @@ class Context:
         self._chk(self._L.pw_apply(self.h, ik, ispin, dtype_code(psi), C.c_void_p(psi.data_ptr()),
                                    C.c_void_p(Hpsi.data_ptr()), ld, nb, ops))
 
-    def apply_multi(self, iks, ispin, psis, Hpsis, ops=PW_OP_H, graph=False):
+    def apply_multi(self, iks, ispin, psis, Hpsis, ops=PW_OP_H, graph=False, persistent=False):
         """pw_apply_multi: Hpsis[i] (+)= H(k = iks[i]) psis[i] for every k-point
         in one launch per stage; psis / Hpsis: lists of torch (nb, Ngw)
         blocks of one dtype.  graph=True replays a captured CUDA graph when
@@ -179,7 +180,8 @@ class Context:
         self.use_torch_stream()
         self._chk(self._L.pw_apply_multi(self.h, n, k.ctypes.data_as(C.POINTER(C.c_int32)), ispin,
                                          dtype_code(psis[0]), P, H, ld.ctypes.data_as(C.POINTER(C.c_int64)),
-                                         nb.ctypes.data_as(C.POINTER(C.c_int32)), ops | (PW_GRAPH if graph else 0)))
+                                         nb.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         ops | (PW_GRAPH if graph else 0) | (PW_PERSISTENT if persistent else 0)))
 
     def lobpcg_multi(self, iks, ispin, Xs, tol=1e-5, nitermax=100, nconv=0):
         """pw_lobpcg_multi: the blocks Xs (torch (nb, Ngw) per k-point, one

@@ -99,6 +99,32 @@ def test_apply_multi_accumulate_subset_and_graph(al4):
     ctx.check_device()
 
 
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_apply_multi_persistent_matches_oracle(al4, prec):
+    """PW_PERSISTENT: every stage in one cooperative launch (bounded grid
+    barriers between the stages): the oracle's op_H per k-point, one launch
+    per call, and a CUDA-graph capture of it replays."""
+    import torch
+    from oracle import ops
+    Ho, ctx, psis = al4
+    dt = torch.complex128 if prec == "c128" else torch.complex64
+    X = _dev(psis, dt)
+    HX = [torch.empty_like(x) for x in X]
+    nk = len(X)
+    n0 = ctx.launch_count()
+    ctx.apply_multi(list(range(nk)), 0, X, HX, persistent=True)
+    assert ctx.launch_count() - n0 == 1
+    tol = 1e-11 if prec == "c128" else 2e-5
+    for ik in range(nk):
+        assert _rel(HX[ik].cpu().numpy().T.astype(np.complex128), ops.op_H(Ho, psis[ik], ik)) < tol, ik
+    HY = [torch.zeros_like(x) for x in X]
+    ctx.apply_multi(list(range(nk)), 0, X, HY, graph=True, persistent=True)
+    ctx.apply_multi(list(range(nk)), 0, X, HY, graph=True, persistent=True)
+    for ik in range(nk):
+        assert _rel(HY[ik].cpu().numpy().T.astype(np.complex128), HX[ik].cpu().numpy().T.astype(np.complex128)) < 1e-12
+    ctx.check_device()
+
+
 def test_apply_multi_errors(al4):
     import torch
     import pwb200
