@@ -163,6 +163,56 @@ template <int N, int S> __device__ __forceinline__ int tw_at(int r, int jm) {
     }
 }
 
+// Lane assignment of round t of a stage with NBF butterflies per line and
+// G lines per warp group.  Shared memory serves an 8-byte access one
+// half-warp at a time, so with NBF <= 16 every half-warp takes whole lines
+// (H = 16 / NBF of them, the rest of its lanes idle): its accesses are then H
+// runs of NBF consecutive elements, one per line, instead of runs that
+// straddle a line boundary onto banks the half-warp already uses (measured
+// model of the 75-point plane kernel: 27 % of its shared-memory wavefronts
+// were such conflicts).  The number of rounds equals the packed mapping's
+// for every plan here (75: 5 and 15 butterflies, 6 lines; 120: 8 and 15, 4;
+// 27: 1, 32).
+template <int NBF, int G> struct LaneMap {
+    static constexpr int H = NBF <= 16 ? 16 / NBF : 0;
+    static constexpr int ROUNDS = H ? (G + 2 * H - 1) / (2 * H) : (G * NBF + 31) / 32;
+    static __device__ __forceinline__ bool at(int lane, int t, int nl, int &line, int &j) {
+        if constexpr (H > 0) {
+            const int sub = lane & 15, li = sub / NBF;
+            j = sub - li * NBF;
+            line = (2 * t + (lane >> 4)) * H + li;
+            return li < H && line < nl;
+        } else {
+            const int id = lane + 32 * t;
+            line = id / NBF;
+            j = id - line * NBF;
+            return id < nl * NBF;
+        }
+    }
+};
+
+// w[r] = w1^r for r < R, w[r] = w[r / 2] w[r - r / 2] (about log2(r) + 1
+// roundings): the stage twiddles of one butterfly from a single table read.
+template <typename T, int R> __device__ __forceinline__ void tw_pow(Cx<T> w1, Cx<T> (&w)[R]) {
+    w[0] = cmake((T)1, (T)0);
+    if constexpr (R > 1) w[1] = w1;
+#pragma unroll
+    for (int r = 2; r < R; ++r) w[r] = cmul(w[r / 2], w[r - r / 2]);
+}
+
+// Twiddles of butterfly jm of stage S (conjugated for the inverse, sign > 0)
+// applied to v[1 .. R).  Only the second stage of a two-stage plan has any;
+// its table entry tw_at(1, jm) is exp(-2 pi i jm / N).
+template <typename T, int N, int S, int R>
+__device__ __forceinline__ void apply_tw(Cx<T> (&v)[R], const Cx<T> *tw, int jm, int sign) {
+    Cx<T> w1 = tw[tw_at<N, S>(1, jm)];
+    if (sign > 0) w1.y = -w1.y;
+    Cx<T> w[R];
+    tw_pow<T, R>(w1, w);
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+}
+
 // PAD: elements at fp_pos(x) (es must be 1)
 template <typename T, int N, int S, bool JFAST, bool PAD>
 __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int ls, const Cx<T> *tw, int sign, int lane) {
@@ -170,38 +220,41 @@ __device__ __forceinline__ void fstage(Cx<T> *buf, int l0, int nl, int es, int l
     constexpr int NS = fp_ns<N>(S);
     constexpr int NBF = N / R;
     constexpr int G = fp_group<N>();
-    constexpr int MAXB = (G * NBF + 31) / 32;
-    const int total = nl * NBF;
+    using LM = LaneMap<NBF, G>;
+    // JFAST lines: whole lines per half-warp; otherwise (z columns, line
+    // index fastest) the packed order, whose strides the callers choose
+    constexpr int MAXB = JFAST ? LM::ROUNDS : (G * NBF + 31) / 32;
+    auto slot = [&](int t, int &line, int &j) -> bool {
+        if constexpr (JFAST) {
+            const bool ok = LM::at(lane, t, nl, line, j);
+            line += l0;
+            return ok;
+        } else {
+            const int id = lane + 32 * t;
+            line = l0 + id % nl;
+            j = id / nl;
+            return id < nl * NBF;
+        }
+    };
     const T sg = (T)sign;
     Cx<T> v[MAXB][R];
 #pragma unroll
     for (int t = 0; t < MAXB; ++t) {
-        const int id = lane + 32 * t;
-        if (id < total) {
-            const int line = JFAST ? l0 + id / NBF : l0 + id % nl;
-            const int j = JFAST ? id % NBF : id / nl;
+        int line, j;
+        if (slot(t, line, j)) {
             const int jm = j % NS;
             const Cx<T> *p = buf + line * ls + j * es;
 #pragma unroll
             for (int r = 0; r < R; ++r) v[t][r] = PAD ? buf[line * ls + fp_pos<N>(j + r * NBF)] : p[r * NBF * es];
-            if (NS > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    Cx<T> w = tw[tw_at<N, S>(r, jm)];
-                    if (sign > 0) w.y = -w.y;
-                    v[t][r] = cmul(v[t][r], w);
-                }
-            }
+            if constexpr (NS > 1) apply_tw<T, N, S, R>(v[t], tw, jm, sign);
             Dft<T, R>::run(v[t], sg, tw, tw_step<N, S>());
         }
     }
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < MAXB; ++t) {
-        const int id = lane + 32 * t;
-        if (id < total) {
-            const int line = JFAST ? l0 + id / NBF : l0 + id % nl;
-            const int j = JFAST ? id % NBF : id / nl;
+        int line, j;
+        if (slot(t, line, j)) {
             const int jm = j % NS;
             const int x0 = (j / NS) * NS * R + jm;
             Cx<T> *q = buf + line * ls + x0 * es;
@@ -235,46 +288,40 @@ __device__ __forceinline__ void lines(Cx<T> *buf, int nlines, int es, int ls, co
 namespace pwf {
 
 // Stage S of the N-point line FFT for lines [0, nl) of one warp group, with
-// element access through functors ld(line, x) -> Cx<T> and st(line, x, v):
-// the first stage of a line can read its input straight from another
-// layout, the last can scale or scatter its output, with no extra pass.
+// element access through functors ld(line, x, r) -> Cx<T> and
+// st(line, x, r, v) (x the element, r the compile-time slot of the lane's
+// butterfly it sits in): the first stage of a line can read its input
+// straight from another layout, the last can scale or scatter its output,
+// with no extra pass.
 template <typename T, int N, int S, class LD, class ST>
 __device__ __forceinline__ void fstage_io(int nl, const Cx<T> *tw, int sign, int lane, LD &ld, ST &st) {
     constexpr int R = FPlan<N>::r(S);
     constexpr int NS = fp_ns<N>(S);
     constexpr int NBF = N / R;
     constexpr int G = fp_group<N>();
-    constexpr int MAXB = (G * NBF + 31) / 32;
-    const int total = nl * NBF;
+    using LM = LaneMap<NBF, G>;
     const T sg = (T)sign;
-    Cx<T> v[MAXB][R];
+    Cx<T> v[LM::ROUNDS][R];
 #pragma unroll
-    for (int t = 0; t < MAXB; ++t) {
-        const int id = lane + 32 * t;
-        if (id < total) {
-            const int line = id / NBF, j = id % NBF, jm = j % NS;
+    for (int t = 0; t < LM::ROUNDS; ++t) {
+        int line, j;
+        if (LM::at(lane, t, nl, line, j)) {
+            const int jm = j % NS;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[t][r] = ld(line, j + r * NBF);
-            if (NS > 1) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    Cx<T> w = tw[tw_at<N, S>(r, jm)];
-                    if (sign > 0) w.y = -w.y;
-                    v[t][r] = cmul(v[t][r], w);
-                }
-            }
+            for (int r = 0; r < R; ++r) v[t][r] = ld(line, j + r * NBF, r);
+            if constexpr (NS > 1) apply_tw<T, N, S, R>(v[t], tw, jm, sign);
             Dft<T, R>::run(v[t], sg, tw, tw_step<N, S>());
         }
     }
     __syncwarp();
 #pragma unroll
-    for (int t = 0; t < MAXB; ++t) {
-        const int id = lane + 32 * t;
-        if (id < total) {
-            const int line = id / NBF, j = id % NBF, jm = j % NS;
+    for (int t = 0; t < LM::ROUNDS; ++t) {
+        int line, j;
+        if (LM::at(lane, t, nl, line, j)) {
+            const int jm = j % NS;
             const int x0 = (j / NS) * NS * R + jm;
 #pragma unroll
-            for (int r = 0; r < R; ++r) st(line, x0 + r * NS, v[t][r]);
+            for (int r = 0; r < R; ++r) st(line, x0 + r * NS, r, v[t][r]);
         }
     }
     __syncwarp();
@@ -286,8 +333,8 @@ __device__ __forceinline__ void fstage_io(int nl, const Cx<T> *tw, int sign, int
 template <typename T, int N, class LD0, class STL>
 __device__ __forceinline__ void group_fft(Cx<T> *buf, int nl, const Cx<T> *tw, int sign, int lane, LD0 &ld0, STL &stl) {
     constexpr int XS = fp_xs<N>();
-    auto bld = [&](int line, int x) { return buf[line * XS + fp_pos<N>(x)]; };
-    auto bst = [&](int line, int x, Cx<T> v) { buf[line * XS + fp_pos<N>(x)] = v; };
+    auto bld = [&](int line, int x, int) { return buf[line * XS + fp_pos<N>(x)]; };
+    auto bst = [&](int line, int x, int, Cx<T> v) { buf[line * XS + fp_pos<N>(x)] = v; };
     constexpr int NST = FPlan<N>::nst;
     static_assert(NST == 1 || NST == 2, "fused plans have one or two stages");
     if constexpr (NST == 1) {
@@ -305,7 +352,7 @@ __device__ __forceinline__ void group_fft(Cx<T> *buf, int nl, const Cx<T> *tw, i
 //   F[k2 + R1 k1] = sum_j w_R0^(j k1) [w_N^(j k2) sum_r f[j + R0 r] w_R1^(r k2)],
 // so the scale (vsc(line, x)), the forward radix-R1 DFT and its twiddles
 // stay in registers and one shared-memory exchange (buf) precedes the
-// radix-R0 DFTs, whose outputs go out through st(line, x, v).  One-stage
+// radix-R0 DFTs, whose outputs go out through st(line, x, r, v).  One-stage
 // plans (one line per lane) never touch buf.
 template <typename T, int N, class LD0, class VS, class ST>
 __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> *tw, int lane, LD0 &ld0, VS &vsc,
@@ -316,69 +363,58 @@ __device__ __forceinline__ void group_fft_vpair(Cx<T> *buf, int nl, const Cx<T> 
         if (lane < nl) {
             Cx<T> v[N];
 #pragma unroll
-            for (int r = 0; r < N; ++r) v[r] = ld0(lane, r);
+            for (int r = 0; r < N; ++r) v[r] = ld0(lane, r, r);
             Dft<T, N>::run(v, (T)1, tw, 1);
 #pragma unroll
             for (int r = 0; r < N; ++r) v[r] = cscale(v[r], vsc(lane, r));
             Dft<T, N>::run(v, (T)-1, tw, 1);
 #pragma unroll
-            for (int k = 0; k < N; ++k) st(lane, k, v[k]);
+            for (int k = 0; k < N; ++k) st(lane, k, k, v[k]);
         }
         __syncwarp();
     } else {
         constexpr int R0 = FPlan<N>::r(0), R1 = FPlan<N>::r(1);
         constexpr int G = fp_group<N>();
         constexpr int XS = fp_xs<N>(), RP = R0 + fp_pad<N>();   // fp_pos(j + R0 r) = j + RP r for j < R0
-        auto bst = [&](int line, int x, Cx<T> v) { buf[line * XS + fp_pos<N>(x)] = v; };
+        auto bst = [&](int line, int x, int, Cx<T> v) { buf[line * XS + fp_pos<N>(x)] = v; };
         fstage_io<T, N, 0>(nl, tw, 1, lane, ld0, bst);   // inverse stage 0 into buf
-        constexpr int MAXB = (G * R0 + 31) / 32;          // stage-1 butterflies: R0 per line
-        const int total = nl * R0;
-        Cx<T> v[MAXB][R1];
+        using L1 = LaneMap<R0, G>;                         // stage-1 butterflies: R0 per line
+        Cx<T> v[L1::ROUNDS][R1];
 #pragma unroll
-        for (int t = 0; t < MAXB; ++t) {
-            const int id = lane + 32 * t;
-            if (id < total) {
-                const int line = id / R0, j = id % R0;
+        for (int t = 0; t < L1::ROUNDS; ++t) {
+            int line, j;
+            if (L1::at(lane, t, nl, line, j)) {
 #pragma unroll
                 for (int r = 0; r < R1; ++r) v[t][r] = buf[line * XS + j + r * RP];
-#pragma unroll
-                for (int r = 1; r < R1; ++r) {
-                    Cx<T> w = tw[tw_at<N, 1>(r, j)];
-                    w.y = -w.y;
-                    v[t][r] = cmul(v[t][r], w);
-                }
+                apply_tw<T, N, 1, R1>(v[t], tw, j, +1);
                 Dft<T, R1>::run(v[t], (T)1, tw, N / R1);      // v[r] = f[j + R0 r]
 #pragma unroll
                 for (int r = 0; r < R1; ++r) v[t][r] = cscale(v[t][r], vsc(line, j + R0 * r));
                 Dft<T, R1>::run(v[t], (T)-1, tw, N / R1);     // sum_r f[j + R0 r] w_R1^(r k2)
-#pragma unroll
-                for (int k2 = 1; k2 < R1; ++k2) v[t][k2] = cmul(v[t][k2], tw[tw_at<N, 1>(k2, j)]);
+                apply_tw<T, N, 1, R1>(v[t], tw, j, -1);
             }
         }
         __syncwarp();
 #pragma unroll
-        for (int t = 0; t < MAXB; ++t) {
-            const int id = lane + 32 * t;
-            if (id < total) {
-                const int line = id / R0, j = id % R0;
+        for (int t = 0; t < L1::ROUNDS; ++t) {
+            int line, j;
+            if (L1::at(lane, t, nl, line, j)) {
 #pragma unroll
                 for (int k2 = 0; k2 < R1; ++k2) buf[line * XS + k2 * RP + j] = v[t][k2];
             }
         }
         __syncwarp();
-        constexpr int MAXB2 = (G * R1 + 31) / 32;
-        const int total2 = nl * R1;
+        using L2 = LaneMap<R1, G>;                         // radix-R0 butterflies: R1 per line
 #pragma unroll
-        for (int t = 0; t < MAXB2; ++t) {
-            const int id = lane + 32 * t;
-            if (id < total2) {
-                const int line = id / R1, k2 = id % R1;
+        for (int t = 0; t < L2::ROUNDS; ++t) {
+            int line, k2;
+            if (L2::at(lane, t, nl, line, k2)) {
                 Cx<T> u[R0];
 #pragma unroll
                 for (int j = 0; j < R0; ++j) u[j] = buf[line * XS + k2 * RP + j];
                 Dft<T, R0>::run(u, (T)-1, tw, tw_step<N, 0>());
 #pragma unroll
-                for (int k1 = 0; k1 < R0; ++k1) st(line, k2 + R1 * k1, u[k1]);
+                for (int k1 = 0; k1 < R0; ++k1) st(line, k2 + R1 * k1, k1, u[k1]);
             }
         }
         __syncwarp();

@@ -557,14 +557,31 @@ kf_plane_rho(KPlan kp, const Cx<T> *__restrict__ twx, const Cx<T> *__restrict__ 
 
 // shared-memory layout of the x-fused plane kernels (in float2 units)
 struct PlaneXSmem {
-    int N1, N2, Nxa, nwarps, group, plane_f;  // plane_f: floats of a full plane kept in shared memory (0 or N1*N2)
+    int N1, N2, Nxa, nwarps, group, plane_f;  // plane_f: floats of a full plane kept in shared memory (0 if none)
     int bands = 1;                            // sub-planes held at once (bands of the same z-plane)
     int xs = 0;                               // line stride of the per-warp x-line buffers (0: N1)
+    int twn = -1;                             // twiddle entries (-1: N1 + N2)
     __host__ __device__ size_t elems() const {
-        return (size_t)N1 + N2 + (size_t)bands * Nxa * N2 + (size_t)nwarps * group * (xs ? xs : N1) + (plane_f + 1) / 2 +
-               (N1 + 3) / 4;
+        return (size_t)(twn >= 0 ? twn : N1 + N2) + (size_t)bands * Nxa * N2 + (size_t)nwarps * group * (xs ? xs : N1) +
+               (plane_f + 1) / 2 + (N1 + 3) / 4;
     }
 };
+
+// Twiddle entries the x-fused op_V_loc kernel keeps: the fused plans read
+// only exp(-2 pi i j / N), j < R0, at [R0, 2 R0) of the two-stage table
+// (the radix DFTs hold their roots as constants, the other powers come from
+// pwf::tw_pow); one-stage plans read none.  One table serves x and y.
+template <int N> __host__ __device__ constexpr int xtw_lo() { return pwf::FPlan<N>::nst == 2 ? pwf::FPlan<N>::r(0) : 0; }
+template <int N> __host__ __device__ constexpr int xtw_len() { return pwf::FPlan<N>::nst == 2 ? 2 * pwf::FPlan<N>::r(0) : 1; }
+
+// Row y of the V(r) plane in shared memory starts at float vrow(y): rows 2m
+// and 2m + 1 begin 15 words apart modulo 32, so the R0 = 15 consecutive x
+// that the two half-warps of one x-pass read from two adjacent rows fall on
+// 30 different banks (measured model of the 75-point kernel: 2 wavefronts
+// per read with rows N1 apart, 1 with the gap).
+template <int N1> __host__ __device__ constexpr int vgap() { return (15 - N1 % 32 + 32) % 32; }
+template <int N1> __host__ __device__ constexpr int vrow(int y) { return y * N1 + vgap<N1>() * ((y + 1) >> 1); }
+template <int N1, int N2> __host__ __device__ constexpr int vplane_floats() { return (vrow<N1>(N2) + 1) & ~1; }
 
 // BPC sub-planes (nbh <= BPC bands of the same z-plane, band stride astr in
 // A) go through every phase together: each block barrier then separates
@@ -582,28 +599,26 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
                                                   size_t astr = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using T = float;
+    static_assert(N1 == N2, "one twiddle table serves x and y");
+    (void)twy;
     constexpr int G = pwf::fp_group<N1>();
     const int Nxa = kp.Nxa, Ncol = kp.Ncol;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = FFT_THREADS / 32;
-    Cx<T> *tx = reinterpret_cast<Cx<T> *>(smem_raw);
-    Cx<T> *ty = tx + N1;
-    Cx<T> *S = ty + N2;
+    Cx<T> *tw = reinterpret_cast<Cx<T> *>(smem_raw);
+    Cx<T> *S = tw + xtw_len<N1>();
     constexpr int LD = plane_ld<N2>();
     constexpr int XS = pwf::fp_xs<N1>();
     const size_t SP = (size_t)Nxa * LD;   // one sub-plane
     Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * XS;
     float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * XS);
-    short *iax = reinterpret_cast<short *>(Vs + (VS ? N1 * N2 + (N1 * N2 & 1) : 0));
-    
+    short *iax = reinterpret_cast<short *>(Vs + (VS ? vplane_floats<N1, N2>() : 0));
+
     const float *Vp = Vr + (size_t)kz * N1 * N2;
     if constexpr (VS)
-        for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[i], &Vp[i]);
-    for (int i = threadIdx.x; i < N1; i += FFT_THREADS) {
-        tx[i] = twx[tw_src<float, N1>(i)];
-        iax[i] = -1;
-    }
-    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[tw_src<float, N2>(i)];
+        for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[vrow<N1>(i / N1) + i % N1], &Vp[i]);
+    for (int i = threadIdx.x; i < N1; i += FFT_THREADS) iax[i] = -1;
+    for (int i = xtw_lo<N1>() + threadIdx.x; i < xtw_len<N1>(); i += FFT_THREADS) tw[i] = twx[tw_src<float, N1>(i)];
     for (int i = threadIdx.x; i < nbh * (int)SP; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
     __syncthreads();
     for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
@@ -614,7 +629,41 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) Sb[kp.col_ia[c] * LD + pwf::fp_pos<N2>(kp.col_j[c])] = Ap[c];
     }
     __syncthreads();
-    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, ty, +1);  // ends with __syncthreads
+    // Two-stage plans: the R0 elements x = j + R1 r (r < R0) that this lane
+    // reads in the first inverse x stage are the ones it writes in the last
+    // forward stage (the same butterfly j = lane's slot in both), so their
+    // active-x rows are looked up once, one byte each (255: x not active).
+    constexpr bool TWO = pwf::FPlan<N1>::nst == 2;
+    constexpr int XR0 = pwf::FPlan<N1>::r(0), XR1 = TWO ? pwf::FPlan<N1>::r(1) : 1;
+    constexpr int NPK = TWO ? (XR0 + 3) / 4 : 1;
+    unsigned pk[NPK];
+    if constexpr (TWO) {
+        static_assert(XR1 <= 16 && pwf::LaneMap<XR1, G>::ROUNDS == 1, "one x butterfly slot per lane");
+        int ln, jl;
+        pwf::LaneMap<XR1, G>::at(lane, 0, G, ln, jl);
+#pragma unroll
+        for (int w = 0; w < NPK; ++w) {
+            unsigned u = 0;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = 4 * w + b;
+                const int ia = r < XR0 ? iax[jl + XR1 * r] : -1;
+                u |= (unsigned)(ia >= 0 ? ia : 255) << (8 * b);
+            }
+            pk[w] = u;
+        }
+    }
+    auto iax_at = [&](int x, int r) -> int {
+        if constexpr (TWO) {
+            (void)x;
+            const int v = (pk[r >> 2] >> (8 * (r & 3))) & 255;
+            return v == 255 ? -1 : v;
+        } else {
+            (void)r;
+            return iax[x];
+        }
+    };
+    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, tw, +1);  // ends with __syncthreads
     if constexpr (VS) {
         cp_async_wait_all();
         __syncthreads();
@@ -627,19 +676,19 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         // rows g0 .. g0 + G - 1 lie in one padding block (G divides R0)
         static_assert(pwf::fp_pad<N2>() == 0 || pwf::FPlan<N2>::r(0) % G == 0, "row groups inside a padding block");
         const int yp = pwf::fp_pos<N2>(g0);
-        auto ld_s = [&](int line, int x) {
-            const int ia = iax[x];
+        auto ld_s = [&](int line, int x, int r) {
+            const int ia = iax_at(x, r);
             return ia >= 0 ? Sb[ia * LD + yp + line] : cmake((T)0, (T)0);
         };
-        auto vsc = [&](int line, int x) { return VS ? Vs[(g0 + line) * N1 + x] : __ldg(&Vp[(g0 + line) * N1 + x]); };
-        auto st_s = [&](int line, int x, Cx<T> v) {
-            const int ia = iax[x];
+        auto vsc = [&](int line, int x) { return VS ? Vs[vrow<N1>(g0 + line) + x] : __ldg(&Vp[(g0 + line) * N1 + x]); };
+        auto st_s = [&](int line, int x, int r, Cx<T> v) {
+            const int ia = iax_at(x, r);
             if (ia >= 0) Sb[ia * LD + yp + line] = v;
         };
-        pwf::group_fft_vpair<T, N1>(Xw, nl, tx, lane, ld_s, vsc, st_s);
+        pwf::group_fft_vpair<T, N1>(Xw, nl, tw, lane, ld_s, vsc, st_s);
     }
     __syncthreads();
-    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, ty, -1);
+    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, tw, -1);
     for (int bb = 0; bb < nbh; ++bb) {
         Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
         const Cx<T> *Sb = S + bb * SP;
@@ -701,11 +750,11 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
         line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);
         for (int g0 = warp * G; g0 < N2; g0 += NW * G) {
             const int nl = min(G, N2 - g0);
-            auto ld_s = [&](int line, int x) {
+            auto ld_s = [&](int line, int x, int) {
                 const int ia = iax[x];
                 return ia >= 0 ? S[ia * N2 + g0 + line] : cmake((T)0, (T)0);
             };
-            auto st_r = [&](int line, int x, Cx<T> v) { acc[(g0 + line) * N1 + x] += wb * (v.x * v.x + v.y * v.y); };
+            auto st_r = [&](int line, int x, int, Cx<T> v) { acc[(g0 + line) * N1 + x] += wb * (v.x * v.x + v.y * v.y); };
             pwf::group_fft<T, N1>(Xw, nl, tx, +1, lane, ld_s, st_r);
         }
         __syncthreads();
@@ -805,16 +854,16 @@ __device__ __forceinline__ void plane_vloc_w_body(const MkK *__restrict__ ks, co
     for (int i = lane; i < Nxa; i += 32) iax[kp.xa[i]] = (short)i;
     for (int c = lane; c < Ncol; c += 32) S[kp.col_ia[c] * N + kp.col_j[c]] = Ap[c];
     __syncwarp();
-    auto ld_row = [&](int line, int x) { return S[line * N + x]; };
-    auto st_row = [&](int line, int x, Cx<T> v) { S[line * N + x] = v; };
+    auto ld_row = [&](int line, int x, int) { return S[line * N + x]; };
+    auto st_row = [&](int line, int x, int, Cx<T> v) { S[line * N + x] = v; };
     pwf::group_fft<T, N>(Xw, Nxa, ty, +1, lane, ld_row, st_row);
     __syncwarp();
-    auto ld_s = [&](int line, int x) {
+    auto ld_s = [&](int line, int x, int) {
         const int ia = iax[x];
         return ia >= 0 ? S[ia * N + line] : cmake((T)0, (T)0);
     };
     auto vsc = [&](int line, int x) { return Vs[line * N + x]; };
-    auto st_s = [&](int line, int x, Cx<T> v) {
+    auto st_s = [&](int line, int x, int, Cx<T> v) {
         const int ia = iax[x];
         if (ia >= 0) S[ia * N + line] = v;
     };
@@ -1095,9 +1144,10 @@ template <int NN, int BPC>
 static cudaError_t launch_plane_vloc_xb(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
     const KPlan &kp = L.kp;
     constexpr bool VS = NN * NN * 4 <= 32 * 1024;
-    PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};
+    PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? vplane_floats<NN, NN>() : 0};
     ps.bands = BPC;
     ps.xs = pwf::fp_xs<NN>();
+    ps.twn = xtw_len<NN>();
     const size_t smem = ps.elems() * sizeof(float2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = set_smem<float>((const void *)kx_plane_vloc<NN, NN, VS, BPC>, smem);
@@ -1164,8 +1214,10 @@ cudaError_t launch_multik(const FftLaunch &L, const MkK *ks, const int *band_k, 
                                         (const float *)Vr, (float2 *)A);                                             \
         } else if constexpr (sizeof(T) == 4) {                                                                       \
             constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
-            PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};       \
+            PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(),                         \
+                          VS ? vplane_floats<NN, NN>() : 0};                                                         \
             ps.xs = pwf::fp_xs<NN>();                                                                                \
+            ps.twn = xtw_len<NN>();                                                                                  \
             const size_t psm = ps.elems() * sizeof(float2);                                                          \
             if ((e = set_smem<float>((const void *)mk_plane_vloc_x<NN, NN, VS>, psm)) != cudaSuccess) return e;     \
             mk_plane_vloc_x<NN, NN, VS><<<dim3(NN, nbands), FFT_THREADS, psm, st>>>(                                 \
@@ -1217,8 +1269,10 @@ cudaError_t launch_multik_persistent(const FftLaunch &L, const MkK *ks, const in
                                   (FFT_THREADS / 32) * ((size_t)kp.Nxa * NN + NN * NN + (NN + 3) / 4) * sizeof(float2)); \
         } else if constexpr (sizeof(T) == 4) {                                                                       \
             constexpr bool VS = NN * NN * 4 <= 32 * 1024;                                                            \
-            PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? NN * NN : 0};       \
+            PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(),                         \
+                          VS ? vplane_floats<NN, NN>() : 0};                                                         \
             ps.xs = pwf::fp_xs<NN>();                                                                                \
+            ps.twn = xtw_len<NN>();                                                                                  \
             sm = std::max(sm, ps.elems() * sizeof(float2));                                                          \
         } else {                                                                                                     \
             const PlaneSmem ps{NN, NN, kp.Nxa, L.Jc};                                                                \
