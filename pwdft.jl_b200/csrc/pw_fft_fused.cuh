@@ -82,8 +82,43 @@ template <typename T, int R1, int R2> struct CompDft {
         }
     }
 };
+// R = R1*R2 with gcd(R1, R2) = 1 (Good-Thomas prime-factor split): input
+// n = (R2 n1 + R1 n2) mod R and output k = CRT(k1 mod R1, k2 mod R2) turn
+// W_R^(nk) into W_R1^(n1 k1) W_R2^(n2 k2), so no twiddles sit between the
+// R2 DFTs of size R1 and the R1 DFTs of size R2 (both index maps are
+// compile-time register permutations).
+template <int A, int M> __host__ __device__ constexpr int inv_mod() {
+    int r = 1;
+    while ((A * r) % M != 1) ++r;
+    return r;
+}
+template <typename T, int R1, int R2> struct PfaDft {
+    static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
+        constexpr int R = R1 * R2;
+        constexpr int E1 = R2 * inv_mod<R2 % R1, R1>(), E2 = R1 * inv_mod<R1 % R2, R2>();   // CRT idempotents
+        Cx<T> a[R];
+#pragma unroll
+        for (int n2 = 0; n2 < R2; ++n2) {
+            Cx<T> t[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; ++n1) t[n1] = v[(R2 * n1 + R1 * n2) % R];
+            Dft<T, R1>::run(t, s, tw, step);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) a[n2 * R1 + k1] = t[k1];
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < R1; ++k1) {
+            Cx<T> t[R2];
+#pragma unroll
+            for (int n2 = 0; n2 < R2; ++n2) t[n2] = a[n2 * R1 + k1];
+            Dft<T, R2>::run(t, s, tw, step);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2) v[(E1 * k1 + E2 * k2) % R] = t[k2];
+        }
+    }
+};
 template <typename T> struct Dft<T, 9> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 3, 3>::run(v, s, tw, st); } };
-template <typename T> struct Dft<T, 15> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 3, 5>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 15> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { PfaDft<T, 3, 5>::run(v, s, tw, st); } };
 template <typename T> struct Dft<T, 24> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 8, 3>::run(v, s, tw, st); } };
 template <typename T> struct Dft<T, 25> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 5, 5>::run(v, s, tw, st); } };
 template <typename T> struct Dft<T, 27> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 9, 3>::run(v, s, tw, st); } };
