@@ -291,6 +291,9 @@ def time_rayleigh_ritz(ctx, psi32, nb, steps, flush):
     res = {}
     for name, fn, flops in (("gram", lambda: ctx.gram(Q, Q, G), 8.0 * (3 * nb) ** 2 * ngw),
                             ("rotate", lambda: ctx.rotate(Q, U, out), 8.0 * 3 * nb * nb * ngw)):
+        # an NVTX range per product, so that a profiler can select its launches
+        # (ncu --nvtx --nvtx-include "rr_gram/")
+        torch.cuda.nvtx.range_push("rr_" + name)
         for _ in range(2):
             fn()
         torch.cuda.synchronize()
@@ -303,6 +306,7 @@ def time_rayleigh_ritz(ctx, psi32, nb, steps, flush):
             e.record()
             torch.cuda.synchronize()
             ts.append(s.elapsed_time(e))
+        torch.cuda.nvtx.range_pop()
         ms = sum(ts) / len(ts)
         res[name] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
     return res

@@ -378,15 +378,21 @@ int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, cons
             int64_t ldc, int acc, int upper = 0) {
     UmmaOperand A, B;
     int s;
-    if ((s = umma_scratch(c, c->um_a_hi, c->um_a_lo, 2 * (int64_t)m, K, A)) ||
-        (s = umma_scratch(c, c->um_b_hi, c->um_b_lo, n, K, B)))
-        return s;
-    CK(c, umma_prep_tn_a<float2>(Z, ldz, K, m, A, c->stream));
-    CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
-    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp, c->gemm_splits)))) return s;
     const int same = (Z == Wm && ldz == ldw && m == n);   // Z^H Z: add the lo*lo product
+    if ((s = umma_scratch(c, c->um_a_hi, c->um_a_lo, 2 * (int64_t)m, K, A))) return s;
+    CK(c, umma_prep_tn_a<float2>(Z, ldz, K, m, A, c->stream));
+    if (same) {
+        // the B' rows [Re z_j, Im z_j] of Z^H Z are the even rows of A'
+        B = A;
+        B.rows = n;
+        B.rstride = 2;
+    } else {
+        if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, n, K, B))) return s;
+        CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
+    }
+    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp, c->gemm_splits)))) return s;
     CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper, same, c->gemm_splits));
-    c->launches += 4;
+    c->launches += (same ? 2 : 3) + (acc || umma_splits(A.rows, n, A.Kp, c->gemm_splits) > 1 ? 1 : 0);
     return PW_OK;
 }
 
@@ -407,7 +413,7 @@ int umma_nn(pw_ctx *c, int64_t M, int n, int k, const void *A, int64_t lda, cons
     if ((s = ensure(c, c->um_ws, umma_ws_bytes(Ao.rows, n, Ao.Kp, c->gemm_splits)))) return s;
     CK(c, umma_gemm<float2>(Ao, B, (int)M, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, 0, 0,
                             c->gemm_splits));
-    c->launches += 3;
+    c->launches += 2 + (acc || umma_splits(Ao.rows, n, Ao.Kp, c->gemm_splits) > 1 ? 1 : 0);
     return PW_OK;
 }
 
@@ -433,7 +439,7 @@ int apply_T(pw_ctx *c, int ik, int ispin, const void *psi, void *Hpsi, int64_t l
             CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
             if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
             CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, c->P.p, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
-            c->launches += 3;
+            c->launches += 2 + (umma_splits(kd.beta_tn.rows, nb, kd.beta_tn.Kp) > 1 ? 1 : 0);
         } else {
             if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb)))) return s;
             CK(c, (gemm_tn<T>(kd.Ngw, c->nbeta, nb, beta, kd.Ngw, psi, ld, (double2 *)c->P.p, c->nbeta, 0, c->gemm_ws.p, st)));
@@ -1296,7 +1302,7 @@ int pwk_beta_dot(pw_ctx *c, int ik, int dtype, const void *psi, int64_t ld, int 
         CK(c, umma_prep_tn_b<float2>(psi, ld, kd.Ngw, nb, B, st));
         if ((s = ensure(c, c->um_ws, umma_ws_bytes(kd.beta_tn.rows, nb, kd.beta_tn.Kp)))) return s;
         CK(c, umma_gemm<double2>(kd.beta_tn, B, c->nbeta, nb, out, c->nbeta, 0, (float *)c->um_ws.p, c->d_err, st));
-        c->launches += 3;
+        c->launches += 2 + (umma_splits(kd.beta_tn.rows, nb, kd.beta_tn.Kp) > 1 ? 1 : 0);
     } else {
         if ((s = ensure(c, c->gemm_ws, gemm_tn_ws_bytes(kd.Ngw, c->nbeta, nb)))) return s;
         if (dtype == PW_C128)

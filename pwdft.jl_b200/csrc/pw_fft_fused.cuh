@@ -211,7 +211,7 @@ template <int N, int S> __device__ __forceinline__ int tw_at(int r, int jm) {
 template <int NBF, int G> struct LaneMap {
     static constexpr int H = NBF <= 16 ? 16 / NBF : 0;
     static constexpr int ROUNDS = H ? (G + 2 * H - 1) / (2 * H) : (G * NBF + 31) / 32;
-    static __device__ __forceinline__ bool at(int lane, int t, int nl, int &line, int &j) {
+    static __host__ __device__ __forceinline__ bool at(int lane, int t, int nl, int &line, int &j) {
         if constexpr (H > 0) {
             const int sub = lane & 15, li = sub / NBF;
             j = sub - li * NBF;

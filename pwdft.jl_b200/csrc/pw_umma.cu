@@ -40,20 +40,37 @@
 namespace pwk {
 namespace umma {
 
-constexpr int BM = 128, BN = 128, BK = 64;
-constexpr int TILE_BYTES = BM * BK * 2;   // 16 KB per operand tile (BM == BN)
+constexpr int BM = 128, BK = 64;
+constexpr int TILE_A_BYTES = BM * BK * 2;   // 16 KB per A operand tile
 constexpr int THREADS = 192;
-constexpr uint32_t TMEM_COLS = 2 * BN;   // two accumulator tiles (double buffer)
 constexpr long long WAIT_LIMIT = 1ll << 26;
 constexpr int MAX_STAGES = 3;
+// k-blocks accumulated in one TMEM tile before the epilogue drains it (each
+// tile is one accumulation chain of the tensor core's truncating FP32 adds;
+// measured: 2 to 8 k-blocks per chain gain at most 6 % on the Si216 Gram and
+// bias its diagonal by -6e-7 to -3e-6, one k-block by -1e-7)
+#ifndef PW_UMMA_CHAIN
+#define PW_UMMA_CHAIN 1
+#endif
+constexpr int CHAIN = PW_UMMA_CHAIN;
 
 // NS = number of BF16 pieces per FP32 value: 2 (hi, lo: 3 products, ~2^-17)
 // or 3 (hi, mid, lo: 6 products, ~2^-24, for products with heavy
-// cancellation such as betaNL' psi).  Three pieces need 6 tiles per stage,
-// so the pipeline keeps 2 stages instead of 3.
-template <int NS> struct Cfg {
-    static constexpr int STAGES = NS == 2 ? 3 : 2;
-    static constexpr int STAGE_BYTES = 2 * NS * TILE_BYTES;
+// cancellation such as betaNL' psi).  BN = output tile width (complex
+// columns): 128, or 160 when it pads n less (n = 160, 480, 1440 bands: one
+// MMA of N = 160 instead of two of N = 128 with 96 columns of padding, and
+// the A tiles read once per 160 columns).  Stages: as many as fit in 227 KB.
+template <int NS, int BN> struct Cfg {
+    static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "tcgen05 N for M = 128, whole 32-column TMEM loads");
+    static constexpr int TILE_B_BYTES = BN * BK * 2;
+    static constexpr int STAGE_BYTES = NS * (TILE_A_BYTES + TILE_B_BYTES);
+    static constexpr int STAGES = (225 * 1024) / STAGE_BYTES < MAX_STAGES ? (225 * 1024) / STAGE_BYTES : MAX_STAGES;
+    static_assert(STAGES >= 2, "at least a double-buffered pipeline");
+    // two accumulator tiles (double buffer), allocation a power of two >= 32
+    static constexpr uint32_t TMEM_COLS = 2 * BN <= 256 ? 256u : 512u;
+    // kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = BN
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 };
 
 struct __align__(8) Bars {
@@ -64,7 +81,9 @@ struct __align__(8) Bars {
     uint32_t tmem_base;
     int failed;
 };
-template <int NS> constexpr size_t smem_bytes() { return 1024 + (size_t)Cfg<NS>::STAGES * Cfg<NS>::STAGE_BYTES + sizeof(Bars); }
+template <int NS, int BN> constexpr size_t smem_bytes() {
+    return 1024 + (size_t)Cfg<NS, BN>::STAGES * Cfg<NS, BN>::STAGE_BYTES + sizeof(Bars);
+}
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -100,13 +119,10 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
     return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
            ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
-// kind::f16, A = B = BF16, D = F32, both K-major, M = 128, N = 128
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t accum) {
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(IDESC), "r"(accum));
+        "l"(a), "l"(b), "r"(idesc), "r"(accum));
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *b) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
@@ -136,15 +152,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 // D (Mp x Np) = sum over the split's k-blocks of the piece products
 //   NS = 2:  A0 B0^T + A0 B1^T + A1 B0^T
 //   NS = 3:  A0 B0^T + A0 B1^T + A1 B0^T + A0 B2^T + A1 B1^T + A2 B0^T
-// written to W[z][n][m] (fp32, column-major, ld = Mp).
-template <int NS>
+// written to W[z][n][m] (fp32, column-major, ld = Mp), or, with a single
+// split (gridDim.z == 1) and C given, straight into the complex result C
+// (element (i, j) at C[j ldc + i], rows 2i and 2i + 1 of D its real and
+// imaginary parts; cdouble: C is complex128; accumulate: C += D; upper: only
+// i <= j written).
+template <int NS, int BN>
 __global__ void __launch_bounds__(THREADS, 1)
 k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
             const __grid_constant__ CUtensorMap tA2, const __grid_constant__ CUtensorMap tB0,
             const __grid_constant__ CUtensorMap tB1, const __grid_constant__ CUtensorMap tB2, int Mp, int Np, int KB,
-            int kb_per, float *__restrict__ W, int *__restrict__ err, int upper, int lolo) {
-    constexpr int STAGES = Cfg<NS>::STAGES;
-    constexpr int STAGE_BYTES = Cfg<NS>::STAGE_BYTES;
+            int kb_per, float *__restrict__ W, int *__restrict__ err, int upper, int lolo, void *__restrict__ C,
+            int64_t ldc, int cdouble, int accumulate) {
+    using CF = Cfg<NS, BN>;
+    constexpr int STAGES = CF::STAGES;
+    constexpr int STAGE_BYTES = CF::STAGE_BYTES;
+    constexpr int TB = CF::TILE_B_BYTES;
+    constexpr int TA = TILE_A_BYTES;
     // upper: C = Z^H W is Hermitian and only its upper triangle is read; a
     // tile whose complex rows (m0/2 ..) all lie below its columns is skipped
     // before any barrier or TMEM allocation
@@ -172,7 +196,7 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUt
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&bars->tmem_base)),
-                     "r"(TMEM_COLS));
+                     "r"(CF::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     fence_before();
@@ -194,11 +218,11 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUt
             const int kc = (kb0 + i) * BK;
             // stage layout: A pieces 0..NS-1, then B pieces 0..NS-1
             tma_load_2d(st, &tA0, &bars->full[s], kc, m0);
-            tma_load_2d(st + TILE_BYTES, &tA1, &bars->full[s], kc, m0);
-            if constexpr (NS == 3) tma_load_2d(st + 2 * TILE_BYTES, &tA2, &bars->full[s], kc, m0);
-            tma_load_2d(st + NS * TILE_BYTES, &tB0, &bars->full[s], kc, n0);
-            tma_load_2d(st + (NS + 1) * TILE_BYTES, &tB1, &bars->full[s], kc, n0);
-            if constexpr (NS == 3) tma_load_2d(st + (NS + 2) * TILE_BYTES, &tB2, &bars->full[s], kc, n0);
+            tma_load_2d(st + TA, &tA1, &bars->full[s], kc, m0);
+            if constexpr (NS == 3) tma_load_2d(st + 2 * TA, &tA2, &bars->full[s], kc, m0);
+            tma_load_2d(st + NS * TA, &tB0, &bars->full[s], kc, n0);
+            tma_load_2d(st + NS * TA + TB, &tB1, &bars->full[s], kc, n0);
+            if constexpr (NS == 3) tma_load_2d(st + NS * TA + 2 * TB, &tB2, &bars->full[s], kc, n0);
         }
         // wait (bounded) for the loads still in flight before leaving
         for (int i = max(0, nkb - STAGES); i < nkb; ++i) {
@@ -206,58 +230,63 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUt
             if (!mbar_wait(&bars->full[s], (uint32_t)((i / STAGES) & 1))) bars->failed = 1;
         }
     } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer: every k-block accumulates into a fresh
-        // TMEM tile (b = i & 1), the correction products first while the
-        // tile is still small and the main product last, so that the
-        // tensor core's truncating FP32 accumulation touches each value only
-        // a few times; the epilogue sums the tiles with round-to-nearest adds
+        // ---------------- MMA issuer: every CHAIN k-blocks accumulate into a
+        // fresh TMEM tile (b = chain & 1), within a k-block the correction
+        // products first and the main product last, so that the tensor
+        // core's truncating FP32 accumulation touches each value only a few
+        // times; the epilogue sums the tiles with round-to-nearest adds
         for (int i = 0; i < nkb; ++i) {
             const int s = i % STAGES;
             const uint32_t ph = (uint32_t)((i / STAGES) & 1);
-            const int b = i & 1;
-            const uint32_t tu = (uint32_t)((i >> 1) & 1);
-            if (!mbar_wait(&bars->tempty[b], tu ^ 1) || !mbar_wait(&bars->full[s], ph)) {
+            const int ch = i / CHAIN;
+            const bool first = i % CHAIN == 0;
+            const int b = ch & 1;
+            const uint32_t tu = (uint32_t)((ch >> 1) & 1);
+            if ((first && !mbar_wait(&bars->tempty[b], tu ^ 1)) || !mbar_wait(&bars->full[s], ph)) {
                 bars->failed = 1;
                 break;
             }
             fence_after();
             const uint32_t base = su32(smem + (size_t)s * STAGE_BYTES);
             const uint32_t d = tmem + (uint32_t)(b * BN);
+            constexpr uint32_t ID = CF::IDESC;
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
                 const uint32_t off = kk * 32;
-                const uint64_t a0 = sdesc(base + off), a1 = sdesc(base + TILE_BYTES + off);
-                const uint64_t b0 = sdesc(base + NS * TILE_BYTES + off), b1 = sdesc(base + (NS + 1) * TILE_BYTES + off);
+                const uint64_t a0 = sdesc(base + off), a1 = sdesc(base + TA + off);
+                const uint64_t b0 = sdesc(base + NS * TA + off), b1 = sdesc(base + NS * TA + TB + off);
+                const bool fresh = first && kk == 0;
                 // lolo (two pieces, A and B the same block): the lo*lo term
                 // too, whose omission would bias every |z|^2 on the diagonal low
-                if (NS == 2 && lolo) mma_bf16(d, a1, b1, kk > 0 ? 1u : 0u);
-                mma_bf16(d, a0, b1, (kk > 0 || (NS == 2 && lolo)) ? 1u : 0u);
-                mma_bf16(d, a1, b0, 1u);
+                if (NS == 2 && lolo) mma_bf16(d, a1, b1, ID, fresh ? 0u : 1u);
+                mma_bf16(d, a0, b1, ID, (!fresh || (NS == 2 && lolo)) ? 1u : 0u);
+                mma_bf16(d, a1, b0, ID, 1u);
                 if constexpr (NS == 3) {
-                    const uint64_t a2 = sdesc(base + 2 * TILE_BYTES + off), b2 = sdesc(base + (NS + 2) * TILE_BYTES + off);
-                    mma_bf16(d, a0, b2, 1u);
-                    mma_bf16(d, a1, b1, 1u);
-                    mma_bf16(d, a2, b0, 1u);
+                    const uint64_t a2 = sdesc(base + 2 * TA + off), b2 = sdesc(base + NS * TA + 2 * TB + off);
+                    mma_bf16(d, a0, b2, ID, 1u);
+                    mma_bf16(d, a1, b1, ID, 1u);
+                    mma_bf16(d, a2, b0, ID, 1u);
                 }
             }
 #pragma unroll
             for (int kk = 0; kk < BK / 16; ++kk) {
                 const uint32_t off = kk * 32;
-                mma_bf16(d, sdesc(base + off), sdesc(base + NS * TILE_BYTES + off), 1u);
+                mma_bf16(d, sdesc(base + off), sdesc(base + NS * TA + off), ID, 1u);
             }
             mma_commit(&bars->empty[s]);
-            mma_commit(&bars->tfull[b]);
+            if (i % CHAIN == CHAIN - 1 || i == nkb - 1) mma_commit(&bars->tfull[b]);
         }
     } else if (warp >= 2) {
         // ---------------- epilogue: TMEM lanes [32q, 32q+32) -> rows m0 + 32q + lane,
-        // the k-block tiles summed in registers
+        // the chain tiles summed in registers
         const int q = warp & 3;
         const int m = m0 + 32 * q + lane;
         float acc[BN];
 #pragma unroll
         for (int t = 0; t < BN; ++t) acc[t] = 0.f;
         bool ok = true;
-        for (int i = 0; i < nkb; ++i) {
+        const int nch = (nkb + CHAIN - 1) / CHAIN;
+        for (int i = 0; i < nch; ++i) {
             const int b = i & 1;
             const uint32_t tu = (uint32_t)((i >> 1) & 1);
             if (!mbar_wait(&bars->tfull[b], tu)) {
@@ -277,12 +306,39 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUt
             if (lane == 0) mbar_arrive(&bars->tempty[b]);
         }
         if (!ok) atomicExch(err, 2);
-        float *Wz = W + (size_t)blockIdx.z * Mp * (size_t)Np;
         if (m < Mp) {
+            if (gridDim.z == 1 && C) {
+                // lanes hold consecutive rows of D = alternating Re / Im of
+                // consecutive complex rows: coalesced component stores
+                const int i = m >> 1, part = m & 1;
+                if (cdouble) {
+                    double *Cd = (double *)C;
 #pragma unroll
-            for (int t = 0; t < BN; ++t) {
-                const int n = n0 + t;
-                if (n < Np) Wz[(size_t)n * Mp + m] = acc[t];
+                    for (int t = 0; t < BN; ++t) {
+                        const int n = n0 + t;
+                        if (n < Np && !(upper && i > n)) {
+                            double *p = Cd + 2 * ((size_t)n * ldc + i) + part;
+                            *p = accumulate ? *p + (double)acc[t] : (double)acc[t];
+                        }
+                    }
+                } else {
+                    float *Cf = (float *)C;
+#pragma unroll
+                    for (int t = 0; t < BN; ++t) {
+                        const int n = n0 + t;
+                        if (n < Np && !(upper && i > n)) {
+                            float *p = Cf + 2 * ((size_t)n * ldc + i) + part;
+                            *p = accumulate ? *p + acc[t] : acc[t];
+                        }
+                    }
+                }
+            } else {
+                float *Wz = W + (size_t)blockIdx.z * Mp * (size_t)Np;
+#pragma unroll
+                for (int t = 0; t < BN; ++t) {
+                    const int n = n0 + t;
+                    if (n < Np) Wz[(size_t)n * Mp + m] = acc[t];
+                }
             }
         }
     }
@@ -291,7 +347,7 @@ k_umma_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUt
     if (threadIdx.x == 0 && bars->failed) atomicExch(err, 1);
     if (warp == 1) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(CF::TMEM_COLS));
     }
 }
 
@@ -447,9 +503,10 @@ cudaError_t get_encoder() {
     return cudaSuccess;
 }
 
-cudaError_t make_map(CUtensorMap *map, const void *base, int64_t rows, int Kp, int box_rows) {
+// rows of Kp BF16 values, row r at base + r * rstride * Kp
+cudaError_t make_map(CUtensorMap *map, const void *base, int64_t rows, int Kp, int box_rows, int rstride) {
     cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+    cuuint64_t strides[1] = {(cuuint64_t)Kp * 2 * (cuuint64_t)rstride};
     cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, es,
@@ -511,12 +568,20 @@ cudaError_t umma_prep_nn_a(const void *A, int64_t lda, int64_t M, int k, UmmaOpe
     return e;
 }
 
+// Output tile width for n complex columns: 160 when it pads n less than 128
+// does (n = 160, 320, 480, 1440), else 128.
+static int pick_bn(int n) {
+    const int p128 = (n + 127) / 128 * 128, p160 = (n + 159) / 160 * 160;
+    return p160 < p128 ? 160 : 128;
+}
+
 // Split-K count: enough CTAs to fill the GPU.  (Accuracy does not depend
-// on it: each k-block is its own accumulation chain in TMEM.)
-int umma_splits(int64_t Mp, int Np, int Kp, int splits = 0) {
+// on it: every CHAIN k-blocks are their own accumulation chain in TMEM.)
+int umma_splits(int64_t Mp, int Np, int Kp, int splits) {
     const int KB = Kp / BK;
     if (splits > 0) return std::max(1, std::min(splits, KB));
-    const int tiles = (int)((Mp + BM - 1) / BM) * ((Np + BN - 1) / BN);
+    const int bn = pick_bn(Np);
+    const int tiles = (int)((Mp + BM - 1) / BM) * ((Np + bn - 1) / bn);
     int S = (2 * 148 + tiles - 1) / tiles;
     return std::max(1, std::min(S, KB / 4 > 0 ? KB / 4 : 1));
 }
@@ -525,17 +590,20 @@ size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits) {
     return (size_t)umma_splits(Mp, Np, Kp, splits) * Mp * Np * sizeof(float);
 }
 
-template <int NS>
+template <int NS, int BN>
 static cudaError_t launch_umma(const CUtensorMap *mA, const CUtensorMap *mB, dim3 grid, int Mp, int n, int KB, int kb_per,
-                               float *ws, int *err, int upper, int lolo, cudaStream_t st) {
+                               float *ws, int *err, int upper, int lolo, void *C, int64_t ldc, int cdouble, int accumulate,
+                               cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_umma_gemm<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes<NS>());
+        cudaError_t e = cudaFuncSetAttribute(k_umma_gemm<NS, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_bytes<NS, BN>());
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_umma_gemm<NS><<<grid, THREADS, smem_bytes<NS>(), st>>>(mA[0], mA[1], mA[2], mB[0], mB[1], mB[2], Mp, n, KB, kb_per,
-                                                              ws, err, upper, lolo);
+    k_umma_gemm<NS, BN><<<grid, THREADS, smem_bytes<NS, BN>(), st>>>(mA[0], mA[1], mA[2], mB[0], mB[1], mB[2], Mp, n, KB,
+                                                                      kb_per, ws, err, upper, lolo, C, ldc, cdouble,
+                                                                      accumulate);
     return cudaGetLastError();
 }
 
@@ -547,20 +615,30 @@ cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, 
     if (A.Kp != B.Kp || A.rows != 2 * (int64_t)m || B.rows != n) return cudaErrorInvalidValue;
     // three BF16 pieces only when both operands carry them
     const int ns = (A.lo2 && B.lo2) ? 3 : 2;
+    const int bn = pick_bn(n);
     CUtensorMap mA[3], mB[3];
     const __nv_bfloat16 *pa[3] = {A.hi, A.lo, ns == 3 ? A.lo2 : A.lo};
     const __nv_bfloat16 *pb[3] = {B.hi, B.lo, ns == 3 ? B.lo2 : B.lo};
     for (int q = 0; q < 3; ++q) {
-        if ((e = make_map(&mA[q], pa[q], A.rows, A.Kp, BM)) != cudaSuccess) return e;
-        if ((e = make_map(&mB[q], pb[q], B.rows, B.Kp, BN)) != cudaSuccess) return e;
+        if ((e = make_map(&mA[q], pa[q], A.rows, A.Kp, BM, A.rstride)) != cudaSuccess) return e;
+        if ((e = make_map(&mB[q], pb[q], B.rows, B.Kp, bn, B.rstride)) != cudaSuccess) return e;
     }
     const int KB = A.Kp / BK;
     const int S = umma_splits(A.rows, n, A.Kp, splits);
     const int kb_per = (KB + S - 1) / S;
-    dim3 grid((unsigned)((A.rows + BM - 1) / BM), (n + BN - 1) / BN, S);
-    e = ns == 3 ? launch_umma<3>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, 0, st)
-                : launch_umma<2>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, lolo, st);
-    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned)((A.rows + BM - 1) / BM), (n + bn - 1) / bn, S);
+    // one split and no accumulation: the epilogue writes C itself, no
+    // workspace pass (accumulating, its read-modify-write of C measured
+    // slower than the workspace + finalize pass: Si64 op_H 0.78 -> 0.95 ms)
+    void *Cd = (S == 1 && !accumulate) ? C : nullptr;
+    const int cd = sizeof(CT) == 16 ? 1 : 0;
+    if (ns == 3)
+        e = bn == 160 ? launch_umma<3, 160>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, 0, Cd, ldc, cd, accumulate, st)
+                      : launch_umma<3, 128>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, 0, Cd, ldc, cd, accumulate, st);
+    else
+        e = bn == 160 ? launch_umma<2, 160>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, lolo, Cd, ldc, cd, accumulate, st)
+                      : launch_umma<2, 128>(mA, mB, grid, (int)A.rows, n, KB, kb_per, ws, err, upper, lolo, Cd, ldc, cd, accumulate, st);
+    if (e != cudaSuccess || Cd) return e;
     k_finalize<CT><<<blocks_for((size_t)m * n), 256, 0, st>>>(ws, S, m, n, (CT *)C, ldc, accumulate, upper);
     return cudaGetLastError();
 }

@@ -16,11 +16,16 @@ struct UmmaOperand {
     __nv_bfloat16 *lo2 = nullptr;
     int64_t rows = 0;
     int Kp = 0;
+    int rstride = 1;   // row r of a piece at r * rstride * Kp (2: the even rows of
+                       // an A' operand, which are the B' rows of the same block)
 };
 
 int umma_kpad(int64_t K);                          // padded 2K (multiple of 64)
 size_t umma_operand_bytes(int64_t rows, int64_t K);  // hi + lo bytes for `rows` rows (one piece: half)
-// split-K workspace; splits > 0 overrides the automatic split count
+// split-K count (splits > 0 overrides the automatic choice) and its
+// workspace; a single split that does not accumulate writes the result
+// directly (no finalize launch)
+int umma_splits(int64_t Mp, int Np, int Kp, int splits = 0);
 size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits = 0);
 
 // Operand builders (CT = float2 or double2 input element).

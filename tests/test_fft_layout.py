@@ -2,10 +2,11 @@
 pw_fft_kernels.cu), checked on the CPU with the header's own constexpr
 functions (compiled by nvcc into a host-only program):
 
-  fp_pos / fp_xs   padded element positions: injective, inside the line
-                   stride; on the 120-point lines every first-stage access
-                   pattern of a warp touches each bank pair of a half-warp
-                   once and the second stage at most twice
+  fp_pos / fp_xs   element positions: injective, inside the line stride
+  LaneMap          whole lines per half-warp: every load and store of both
+                   stages of the 75- and 120-point lines (line stride N)
+                   touches each bank pair of a half-warp once, where the
+                   packed lane order conflicts
   tw_src           the shared twiddle table holds exp(-2 pi i m / R0) then
                    the stage-1 twiddles at (r, j), N entries
   zrow             the z-tile row stride = lines per warp group (mod 16)
@@ -25,6 +26,18 @@ CSRC = os.path.join(ROOT, "pwdft.jl_b200", "csrc")
 PROG = r'''
 #include <cstdio>
 #include "pw_fft_fused.cuh"
+// LaneMap<NBF, G>: "LM NBF G ROUNDS" then (t lane ok line j) for every slot
+template <int NBF, int G> void lanes() {
+    using LM = pwf::LaneMap<NBF, G>;
+    std::printf("LM %d %d %d", NBF, G, LM::ROUNDS);
+    for (int t = 0; t < LM::ROUNDS; ++t)
+        for (int lane = 0; lane < 32; ++lane) {
+            int line = -1, j = -1;
+            const bool ok = LM::at(lane, t, G, line, j);
+            std::printf(" %d,%d,%d,%d,%d", t, lane, ok ? 1 : 0, line, j);
+        }
+    std::printf("\n");
+}
 template <int N> void dump() {
     constexpr int R0 = pwf::FPlan<N>::r(0);
     constexpr int R1 = pwf::FPlan<N>::nst == 2 ? pwf::FPlan<N>::r(1) : 1;
@@ -34,6 +47,8 @@ template <int N> void dump() {
     std::printf("\nTW");
     for (int i = 0; i < N; ++i) std::printf(" %d", pwf::tw_src<N>(i));
     std::printf("\n");
+    lanes<N / R0, pwf::fp_group<N>()>();
+    lanes<N / R1, pwf::fp_group<N>()>();
 }
 int main() { dump<27>(); dump<75>(); dump<120>(); return 0; }
 '''
@@ -50,11 +65,16 @@ def layouts(tmp_path_factory):
     subprocess.run(["nvcc", "-std=c++17", "-I", CSRC, str(src), "-o", exe], check=True, capture_output=True)
     out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
     res = {}
-    for i in range(0, len(out) - 2, 3):
+    for i in range(0, len(out) - 4, 5):
         f = out[i].split()
         N = int(f[1])
         res[N] = dict(G=int(f[3]), XS=int(f[5]), R0=int(f[7]), R1=int(f[9]),
-                      pos=[int(v) for v in out[i + 1].split()[1:]], tw=[int(v) for v in out[i + 2].split()[1:]])
+                      pos=[int(v) for v in out[i + 1].split()[1:]], tw=[int(v) for v in out[i + 2].split()[1:]],
+                      lanes={})
+        for k in (3, 4):
+            g = out[i + k].split()
+            slots = [tuple(int(v) for v in x.split(",")) for x in g[4:]]
+            res[N]["lanes"][int(g[1])] = dict(G=int(g[2]), rounds=int(g[3]), slots=slots)
     return res
 
 
@@ -78,25 +98,63 @@ def test_positions_fit_and_are_injective(layouts):
             assert L["pos"] == list(range(N)) and L["XS"] == N
 
 
-def test_120_first_stage_conflict_free(layouts):
-    L = layouts[120]
-    G, XS, R0, R1, pos = L["G"], L["XS"], L["R0"], L["R1"], L["pos"]
-    ideal = got1 = got2 = 0
-    for r in range(R0):                      # stage-0 outputs x = R0 j + r, lane (line, j)
-        ids = list(range(G * R1))
-        a = [(i // R1) * XS + pos[(i % R1) * R0 + r] for i in ids]
-        got1 += wavefronts(a)
-        ideal += (len(a) + 15) // 16
-    assert got1 == ideal
-    for r in range(R1):                      # stage-1 inputs x = j + R0 r, lane (line, j)
-        for t in range((G * R0 + 31) // 32):
-            ids = [i for i in range(32 * t, 32 * t + 32) if i < G * R0]
-            a = [(i // R0) * XS + pos[(i % R0) + R0 * r] for i in ids]
-            assert wavefronts(a) <= 2 * ((len(a) + 15) // 16)
-            got2 += wavefronts(a)
-    # the unpadded stride-120 layout: 8-way conflicts in stage 0
-    bad = sum(wavefronts([(i // R1) * 120 + (i % R1) * R0 + r for i in range(G * R1)]) for r in range(R0))
-    assert bad >= 7 * ideal
+def stage_patterns(L, nbf, packed=False):
+    """Per warp instruction of the two stages of a warp group's lines: element
+    indices within the lines (line stride XS) for every (round, r)."""
+    N, XS, R0 = len(L["pos"]), L["XS"], L["R0"]
+    lm = L["lanes"][nbf]
+    R = N // nbf
+    out = []
+    rounds = (lm["G"] * nbf + 31) // 32 if packed else lm["rounds"]
+    for t in range(rounds):
+        slots = []
+        for lane in range(32):
+            if packed:
+                i = lane + 32 * t
+                slots.append((i // nbf, i % nbf) if i < lm["G"] * nbf else None)
+            else:
+                _, _, ok, line, j = lm["slots"][t * 32 + lane]
+                slots.append((line, j) if ok else None)
+        for r in range(R):
+            if nbf == N // R0:      # first stage: reads j + nbf r, writes R0 j + r
+                ld = [s[0] * XS + L["pos"][s[1] + nbf * r] if s else None for s in slots]
+                st = [s[0] * XS + L["pos"][R0 * s[1] + r] if s else None for s in slots]
+            else:                   # second stage: reads and writes j + R0 r
+                ld = st = [s[0] * XS + L["pos"][s[1] + R0 * r] if s else None for s in slots]
+            out += [ld, st]
+    return out
+
+
+def wavefronts_lanes(act):
+    """wavefronts() with explicit lane numbers (idle lanes left out)."""
+    tot = 0
+    for half in (0, 1):
+        h = [x for k, x in act if (k >= 16) == bool(half)]
+        if h:
+            banks = {}
+            for x in h:
+                banks.setdefault(x % 16, set()).add(x)
+            tot += max(len(v) for v in banks.values())
+    return tot
+
+
+def test_line_stages_conflict_free(layouts):
+    for N in (75, 120):
+        L = layouts[N]
+        for nbf in L["lanes"]:
+            got = ideal = packed = 0
+            for a in stage_patterns(L, nbf):
+                act = [(k, x) for k, x in enumerate(a) if x is not None]
+                got += wavefronts_lanes(act)
+                ideal += (1 if any(k < 16 for k, _ in act) else 0) + (1 if any(k >= 16 for k, _ in act) else 0)
+            for a in stage_patterns(L, nbf, packed=True):
+                packed += wavefronts_lanes([(k, x) for k, x in enumerate(a) if x is not None])
+            assert got == ideal, (N, nbf, got, ideal)
+            assert got <= packed, (N, nbf, got, packed)
+        # every slot of a group is taken exactly once over the rounds
+        for nbf, lm in L["lanes"].items():
+            seen = [(line, j) for t, lane, ok, line, j in lm["slots"] if ok]
+            assert sorted(seen) == [(l, j) for l in range(lm["G"]) for j in range(nbf)], (N, nbf)
 
 
 def test_twiddle_table(layouts):
