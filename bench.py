@@ -50,12 +50,12 @@ DIAMOND = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes (read + write) of one FP32 pruned-FFT round trip of the Si64
-# op_H (160 bands: kf_zinv + kx_plane_vloc + kf_zfwd over two band batches),
-# from one --set full capture of each kernel of the first batch (83 bands)
-# scaled by 160/83:
-#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 PW_BENCH_NO_MULTIK=1 PW_BENCH_NO_AUTOTUNE=1 ncu --set full
-#     --clock-control none -k regex:<kernel> -s 6 -c 1 python bench.py --steps 3 --warmup 3
-FFT_TRAFFIC_BYTES = {"si64": 267.7e6}
+# op_H (160 bands: kf_zinv + kx_plane_vloc + kf_zfwd over both band batches),
+# summed over the six launches of the first timed op_H:
+#   PW_BENCH_NO_SCF=1 PW_BENCH_NO_CPU=1 PW_BENCH_NO_MULTIK=1 PW_BENCH_NO_AUTOTUNE=1 ncu --metrics
+#     dram__bytes_read.sum,dram__bytes_write.sum --clock-control none
+#     -k "regex:kf_zinv|kx_plane_vloc|kf_zfwd" -s 18 -c 6 python bench.py --steps 3 --warmup 3
+FFT_TRAFFIC_BYTES = {"si64": 260.6e6}
 FALLBACK_HBM_GBS = 6650.0
 
 
