@@ -390,9 +390,9 @@ int umma_tn(pw_ctx *c, int64_t K, int m, int n, const void *Z, int64_t ldz, cons
         if ((s = umma_scratch(c, c->um_b_hi, c->um_b_lo, n, K, B))) return s;
         CK(c, umma_prep_tn_b<float2>(Wm, ldw, K, n, B, c->stream));
     }
-    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp, c->gemm_splits)))) return s;
+    if ((s = ensure(c, c->um_ws, umma_ws_bytes(A.rows, n, A.Kp, c->gemm_splits, upper)))) return s;
     CK(c, umma_gemm<CT>(A, B, m, n, C, ldc, acc, (float *)c->um_ws.p, c->d_err, c->stream, upper, same, c->gemm_splits));
-    c->launches += (same ? 2 : 3) + (acc || umma_splits(A.rows, n, A.Kp, c->gemm_splits) > 1 ? 1 : 0);
+    c->launches += (same ? 2 : 3) + (acc || umma_splits(A.rows, n, A.Kp, c->gemm_splits, upper) > 1 ? 1 : 0);
     return PW_OK;
 }
 

@@ -78,19 +78,30 @@ __global__ void k_splitk_reduce(const double2 *__restrict__ W, int S, int m, int
 
 constexpr int NN_BM = 64, NN_BN = 32, NN_BK = 16;
 
+// tri: triangular structure the caller guarantees (the k-loop skips the
+// zero blocks, whole tiles are skipped where no needed output lies):
+//   1  A lower triangular (A[g][l] = 0 for l > g)
+//   2  B upper triangular (B[l][j] = 0 for l > j) and only C[g][j], g <= j,
+//      needed (tiles entirely below the diagonal are not formed)
+//   3  A upper triangular (A[g][l] = 0 for l < g)
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_gemm_nn(int64_t M, int n, int k, const Cx<T> *__restrict__ A, int64_t lda, const double2 *__restrict__ B, int64_t ldb,
-          Cx<T> *__restrict__ C, int64_t ldc, int accumulate) {
+          Cx<T> *__restrict__ C, int64_t ldc, int accumulate, int tri) {
     __shared__ Cx<T> As[NN_BK][NN_BM];
     __shared__ Cx<T> Bs[NN_BK][NN_BN];
     const int64_t g0 = (int64_t)blockIdx.x * NN_BM;
     const int n0 = blockIdx.y * NN_BN;
+    if (tri == 2 && g0 > n0 + NN_BN - 1) return;   // the whole CTA: before any barrier
+    int jbeg = 0, jend = k;
+    if (tri == 1) jend = (int)min((int64_t)k, g0 + NN_BM);
+    if (tri == 2) jend = min(k, n0 + NN_BN);
+    if (tri == 3) jbeg = (int)min((int64_t)k, (g0 / NN_BK) * NN_BK);
     const int tg = threadIdx.x & 63, tn = threadIdx.x >> 6;  // 64 rows x 4 column groups of 8
     Cx<T> acc[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) acc[q] = cmake((T)0, (T)0);
-    for (int j0 = 0; j0 < k; j0 += NN_BK) {
+    for (int j0 = jbeg; j0 < jend; j0 += NN_BK) {
         for (int e = threadIdx.x; e < NN_BK * NN_BM; e += 256) {
             const int gg = e % NN_BM, jj = e / NN_BM;
             As[jj][gg] = (g0 + gg < M && j0 + jj < k) ? A[(size_t)(j0 + jj) * lda + g0 + gg] : cmake((T)0, (T)0);
@@ -192,10 +203,10 @@ cudaError_t gemm_tn(int64_t K, int m, int n, const void *A, int64_t lda, const v
 
 template <typename T>
 cudaError_t gemm_nn(int64_t M, int n, int k, const void *A, int64_t lda, const double2 *B, int64_t ldb, void *C,
-                    int64_t ldc, int accumulate, cudaStream_t st) {
+                    int64_t ldc, int accumulate, cudaStream_t st, int tri) {
     if (M <= 0 || n <= 0) return cudaSuccess;
     dim3 grid((unsigned)((M + NN_BM - 1) / NN_BM), (n + NN_BN - 1) / NN_BN);
-    k_gemm_nn<T><<<grid, 256, 0, st>>>(M, n, k, (const Cx<T> *)A, lda, B, ldb, (Cx<T> *)C, ldc, accumulate);
+    k_gemm_nn<T><<<grid, 256, 0, st>>>(M, n, k, (const Cx<T> *)A, lda, B, ldb, (Cx<T> *)C, ldc, accumulate, tri);
     return cudaGetLastError();
 }
 
@@ -204,9 +215,9 @@ template cudaError_t gemm_tn<float>(int64_t, int, int, const void *, int64_t, co
 template cudaError_t gemm_tn<double>(int64_t, int, int, const void *, int64_t, const void *, int64_t, double2 *, int64_t,
                                      int, void *, cudaStream_t, int);
 template cudaError_t gemm_nn<float>(int64_t, int, int, const void *, int64_t, const double2 *, int64_t, void *, int64_t,
-                                    int, cudaStream_t);
+                                    int, cudaStream_t, int);
 template cudaError_t gemm_nn<double>(int64_t, int, int, const void *, int64_t, const double2 *, int64_t, void *, int64_t,
-                                     int, cudaStream_t);
+                                     int, cudaStream_t, int);
 
 cudaError_t apply_dcsr(int nbeta, int nb, const int *rowptr, const int *col, const double *val, const double2 *P,
                        double2 *P2, cudaStream_t st) {

@@ -82,10 +82,12 @@ template <typename T>
 // the diagonal are skipped.
 cudaError_t gemm_tn(int64_t K, int m, int n, const void *A, int64_t lda, const void *B, int64_t ldb, double2 *C,
                     int64_t ldc, int accumulate, void *ws, cudaStream_t, int upper = 0);
-// C (M x n, Cx<T>, ldc) (+)= A (M x k, Cx<T>) * B (k x n, double2)
+// C (M x n, Cx<T>, ldc) (+)= A (M x k, Cx<T>) * B (k x n, double2); tri: 1 = A
+// lower triangular, 2 = B upper triangular and only C's upper triangle
+// needed, 3 = A upper triangular (zero blocks skipped)
 template <typename T>
 cudaError_t gemm_nn(int64_t M, int n, int k, const void *A, int64_t lda, const double2 *B, int64_t ldb, void *C,
-                    int64_t ldc, int accumulate, cudaStream_t);
+                    int64_t ldc, int accumulate, cudaStream_t, int tri = 0);
 // P2[i][b] = sum_j D[i][j] P[j][b]  (CSR D; P, P2 are nbeta x nb, ld = nbeta)
 cudaError_t apply_dcsr(int nbeta, int nb, const int *rowptr, const int *col, const double *val, const double2 *P,
                        double2 *P2, cudaStream_t);

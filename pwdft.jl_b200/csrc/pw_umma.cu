@@ -575,19 +575,43 @@ static int pick_bn(int n) {
     return p160 < p128 ? 160 : 128;
 }
 
-// Split-K count: enough CTAs to fill the GPU.  (Accuracy does not depend
-// on it: every CHAIN k-blocks are their own accumulation chain in TMEM.)
-int umma_splits(int64_t Mp, int Np, int Kp, int splits) {
+// Split-K count.  One CTA fits on an SM (222 KB of shared memory); the
+// count minimises a model of the run time in k-block units: waves of the
+// active tiles (those on or above the diagonal for a Hermitian product) x
+// splits over 148 SMs, times the k-blocks per split plus ~8 for a CTA's
+// pipeline fill and epilogue, plus the split-K workspace pass.  (Measured:
+// the Si64 betaNL' psi at 5 tiles x 60 splits ran as 2 waves plus 4 CTAs;
+// the Si216 Gram, 115 active tiles, was slower unsplit than at 2 splits.)
+// Accuracy does not depend on it: every CHAIN k-blocks are their own
+// accumulation chain in TMEM.
+int umma_splits(int64_t Mp, int Np, int Kp, int splits, int upper) {
     const int KB = Kp / BK;
     if (splits > 0) return std::max(1, std::min(splits, KB));
     const int bn = pick_bn(Np);
-    const int tiles = (int)((Mp + BM - 1) / BM) * ((Np + bn - 1) / bn);
-    int S = (2 * 148 + tiles - 1) / tiles;
-    return std::max(1, std::min(S, KB / 4 > 0 ? KB / 4 : 1));
+    const int mt = (int)((Mp + BM - 1) / BM), nt = (Np + bn - 1) / bn;
+    int active = mt * nt;
+    if (upper) {
+        active = 0;
+        for (int by = 0; by < nt; ++by)
+            for (int bx = 0; bx < mt; ++bx) active += (bx * BM) / 2 > by * bn + bn - 1 ? 0 : 1;
+    }
+    active = std::max(1, active);
+    const int smax = std::max(1, std::min(64, KB / 4));
+    int best = 1;
+    double tbest = 1e300;
+    for (int S = 1; S <= smax; ++S) {
+        const double waves = (double)((active * S + 147) / 148);
+        const double t = waves * ((double)(KB + S - 1) / S + 8.0) + (S > 1 ? (double)S * Mp * Np / 1.6e6 : 0.0);
+        if (t < tbest * (1.0 - 1e-9)) {
+            tbest = t;
+            best = S;
+        }
+    }
+    return best;
 }
 
-size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits) {
-    return (size_t)umma_splits(Mp, Np, Kp, splits) * Mp * Np * sizeof(float);
+size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits, int upper) {
+    return (size_t)umma_splits(Mp, Np, Kp, splits, upper) * Mp * Np * sizeof(float);
 }
 
 template <int NS, int BN>
@@ -624,7 +648,7 @@ cudaError_t umma_gemm(const UmmaOperand &A, const UmmaOperand &B, int m, int n, 
         if ((e = make_map(&mB[q], pb[q], B.rows, B.Kp, bn, B.rstride)) != cudaSuccess) return e;
     }
     const int KB = A.Kp / BK;
-    const int S = umma_splits(A.rows, n, A.Kp, splits);
+    const int S = umma_splits(A.rows, n, A.Kp, splits, upper);
     const int kb_per = (KB + S - 1) / S;
     dim3 grid((unsigned)((A.rows + BM - 1) / BM), (n + bn - 1) / bn, S);
     // one split and no accumulation: the epilogue writes C itself, no

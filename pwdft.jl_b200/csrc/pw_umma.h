@@ -25,8 +25,9 @@ size_t umma_operand_bytes(int64_t rows, int64_t K);  // hi + lo bytes for `rows`
 // split-K count (splits > 0 overrides the automatic choice) and its
 // workspace; a single split that does not accumulate writes the result
 // directly (no finalize launch)
-int umma_splits(int64_t Mp, int Np, int Kp, int splits = 0);
-size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits = 0);
+// (upper: the product is Hermitian and only tiles on or above the diagonal run)
+int umma_splits(int64_t Mp, int Np, int Kp, int splits = 0, int upper = 0);
+size_t umma_ws_bytes(int64_t Mp, int Np, int Kp, int splits = 0, int upper = 0);
 
 // Operand builders (CT = float2 or double2 input element).
 //   tn_a: A' (2m rows) from Z (K x m)          for C = Z^H W
