@@ -490,6 +490,13 @@ def main():
         flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
         print(json.dumps({"multik": multik_comparison(local, max(5, args.steps // 20), flush)}))
         return
+    if os.environ.get("PW_BENCH_ONLY_EIGH") == "1":
+        # the FP64 generalized eigensolver alone at this workload's size (a
+        # short command for profiling it)
+        torch.cuda.set_device(local)
+        H, _ = build_workload(local, args.workload)
+        print(json.dumps({"eigh_fp64": time_eigh(H.ctx, WORKLOADS[args.workload], max(1, args.steps))}))
+        return
     dist = None
     if world > 1:
         import torch.distributed as dist
