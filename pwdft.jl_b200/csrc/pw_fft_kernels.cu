@@ -582,6 +582,14 @@ template <int N> __host__ __device__ constexpr int xtw_len() { return pwf::FPlan
 template <int N1> __host__ __device__ constexpr int vgap() { return (15 - N1 % 32 + 32) % 32; }
 template <int N1> __host__ __device__ constexpr int vrow(int y) { return y * N1 + vgap<N1>() * ((y + 1) >> 1); }
 template <int N1, int N2> __host__ __device__ constexpr int vplane_floats() { return (vrow<N1>(N2) + 1) & ~1; }
+// FP64 planes: the half-warps of an x-pass read 8-byte values, served one
+// half-warp (one row) at a time, so no gap
+template <typename T, int N1> __host__ __device__ constexpr int vrow_t(int y) {
+    return sizeof(T) == 4 ? vrow<N1>(y) : y * N1;
+}
+template <typename T, int N1, int N2> __host__ __device__ constexpr int vplane_elems() {
+    return sizeof(T) == 4 ? vplane_floats<N1, N2>() : N1 * N2;
+}
 
 // BPC sub-planes (nbh <= BPC bands of the same z-plane, band stride astr in
 // A) go through every phase together: each block barrier then separates
@@ -592,13 +600,12 @@ template <int N1, int N2> __host__ __device__ constexpr int vplane_floats() { re
 // 75-point grid padding would cost the third sub-plane per CTA).
 template <int N> __host__ __device__ constexpr int plane_ld() { return pwf::fp_xs<N>(); }
 
-template <int N1, int N2, bool VS, int BPC = 1>
-__device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 *__restrict__ twx,
-                                                  const float2 *__restrict__ twy, const float *__restrict__ Vr,
-                                                  float2 *__restrict__ Ab, int kz, int nbh = 1,
+template <typename T, int N1, int N2, bool VS, int BPC = 1>
+__device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const Cx<T> *__restrict__ twx,
+                                                  const Cx<T> *__restrict__ twy, const T *__restrict__ Vr,
+                                                  Cx<T> *__restrict__ Ab, int kz, int nbh = 1,
                                                   size_t astr = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using T = float;
     static_assert(N1 == N2, "one twiddle table serves x and y");
     (void)twy;
     constexpr int G = pwf::fp_group<N1>();
@@ -611,14 +618,22 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
     constexpr int XS = pwf::fp_xs<N1>();
     const size_t SP = (size_t)Nxa * LD;   // one sub-plane
     Cx<T> *Xw = S + BPC * SP + (size_t)warp * G * XS;
-    float *Vs = reinterpret_cast<float *>(S + BPC * SP + (size_t)NW * G * XS);
-    short *iax = reinterpret_cast<short *>(Vs + (VS ? vplane_floats<N1, N2>() : 0));
+    T *Vs = reinterpret_cast<T *>(S + BPC * SP + (size_t)NW * G * XS);
+    short *iax = reinterpret_cast<short *>(Vs + (VS ? vplane_elems<T, N1, N2>() : 0));
 
-    const float *Vp = Vr + (size_t)kz * N1 * N2;
-    if constexpr (VS)
-        for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) cp_async4(&Vs[vrow<N1>(i / N1) + i % N1], &Vp[i]);
+    const T *Vp = Vr + (size_t)kz * N1 * N2;
+    if constexpr (VS) {
+        for (int i = threadIdx.x; i < N1 * N2; i += FFT_THREADS) {
+            T *dst = &Vs[vrow_t<T, N1>(i / N1) + i % N1];
+            if constexpr (sizeof(T) == 4)
+                cp_async4(dst, &Vp[i]);
+            else
+                cp_async_cx<float>(reinterpret_cast<Cx<float> *>(dst), reinterpret_cast<const Cx<float> *>(&Vp[i]));
+        }
+    }
     for (int i = threadIdx.x; i < N1; i += FFT_THREADS) iax[i] = -1;
-    for (int i = xtw_lo<N1>() + threadIdx.x; i < xtw_len<N1>(); i += FFT_THREADS) tw[i] = twx[tw_src<float, N1>(i)];
+    // the table of twx is in natural order: entry i of the fused layout is exp(-2 pi i tw_src(i) / N)
+    for (int i = xtw_lo<N1>() + threadIdx.x; i < xtw_len<N1>(); i += FFT_THREADS) tw[i] = twx[pwf::tw_src<N1>(i)];
     for (int i = threadIdx.x; i < nbh * (int)SP; i += FFT_THREADS) S[i] = cmake((T)0, (T)0);
     __syncthreads();
     for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
@@ -663,7 +678,7 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
             return iax[x];
         }
     };
-    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, tw, +1);  // ends with __syncthreads
+    pwf::lines<T, N2, true>(S, nbh * Nxa, 1, LD, tw, +1);  // ends with __syncthreads
     if constexpr (VS) {
         cp_async_wait_all();
         __syncthreads();
@@ -680,7 +695,7 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
             const int ia = iax_at(x, r);
             return ia >= 0 ? Sb[ia * LD + yp + line] : cmake((T)0, (T)0);
         };
-        auto vsc = [&](int line, int x) { return VS ? Vs[vrow<N1>(g0 + line) + x] : __ldg(&Vp[(g0 + line) * N1 + x]); };
+        auto vsc = [&](int line, int x) { return VS ? Vs[vrow_t<T, N1>(g0 + line) + x] : __ldg(&Vp[(g0 + line) * N1 + x]); };
         auto st_s = [&](int line, int x, int r, Cx<T> v) {
             const int ia = iax_at(x, r);
             if (ia >= 0) Sb[ia * LD + yp + line] = v;
@@ -688,7 +703,7 @@ __device__ __forceinline__ void plane_vloc_x_band(const KPlan &kp, const float2 
         pwf::group_fft_vpair<T, N1>(Xw, nl, tw, lane, ld_s, vsc, st_s);
     }
     __syncthreads();
-    line_fft<T, N2, true, true>(S, nbh * Nxa, 1, LD, tw, -1);
+    pwf::lines<T, N2, true>(S, nbh * Nxa, 1, LD, tw, -1);
     for (int bb = 0; bb < nbh; ++bb) {
         Cx<T> *Ap = Ab + bb * astr + (size_t)kz * Ncol;
         const Cx<T> *Sb = S + bb * SP;
@@ -703,7 +718,18 @@ kx_plane_vloc(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict
               float2 *__restrict__ A, int nb) {
     const int b0 = blockIdx.y * BPC;
     const size_t astr = (size_t)kp.N3 * kp.Ncol;
-    plane_vloc_x_band<N1, N2, VS, BPC>(kp, twx, twy, Vr, A + b0 * astr, blockIdx.x, min(BPC, nb - b0), astr);
+    plane_vloc_x_band<float, N1, N2, VS, BPC>(kp, twx, twy, Vr, A + b0 * astr, blockIdx.x, min(BPC, nb - b0), astr);
+}
+
+// The same x-fused plane pass in FP64 (the reference's precision): the fused
+// radix plans in double registers, one CTA per SM (up to 255 registers).
+template <int N1, int N2, bool VS, int BPC>
+__global__ void __launch_bounds__(FFT_THREADS, 1)
+kx_plane_vloc64(KPlan kp, const double2 *__restrict__ twx, const double2 *__restrict__ twy,
+                const double *__restrict__ Vr, double2 *__restrict__ A, int nb) {
+    const int b0 = blockIdx.y * BPC;
+    const size_t astr = (size_t)kp.N3 * kp.Ncol;
+    plane_vloc_x_band<double, N1, N2, VS, BPC>(kp, twx, twy, Vr, A + b0 * astr, blockIdx.x, min(BPC, nb - b0), astr);
 }
 
 // calc_rhoe: bands [g*Bg, min(nb, (g+1)*Bg)) of plane kz; the weighted
@@ -799,7 +825,7 @@ mk_plane_vloc_x(const MkK *__restrict__ ks, const int *__restrict__ band_k, cons
     const MkK &K = ks[band_k[blockIdx.y]];
     const KPlan kp = K.kp;
     const int b = blockIdx.y - K.band0;
-    plane_vloc_x_band<N1, N2, VS>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, blockIdx.x);
+    plane_vloc_x_band<float, N1, N2, VS>(kp, twx, twy, Vr, A + K.a_off + (size_t)b * kp.N3 * kp.Ncol, blockIdx.x);
 }
 
 template <typename T, int N1, int N2>
@@ -1033,7 +1059,7 @@ mk_persistent(const MkK *__restrict__ ks, const int *__restrict__ band_k, int nb
             Cx<T> *Ab = A + K.a_off + (size_t)(band - K.band0) * NN * K.kp.Ncol;
             if constexpr (sizeof(T) == 4) {
                 constexpr bool VS = NN * NN * 4 <= 32 * 1024;
-                plane_vloc_x_band<NN, NN, VS>(K.kp, twx, twy, Vr, Ab, kz);
+                plane_vloc_x_band<float, NN, NN, VS>(K.kp, twx, twy, Vr, Ab, kz);
             } else {
                 plane_vloc_band<T, NN, NN>(K.kp, twx, twy, Vr, Ab, Jc, kz);
             }
@@ -1169,6 +1195,25 @@ static cudaError_t launch_plane_vloc_x(const FftLaunch &L, const void *Vr, void 
         case 3: return launch_plane_vloc_xb<NN, 3>(L, Vr, A, nb, st);
         default: return cudaErrorInvalidValue;
     }
+}
+// FP64 x-fused plane pass on the two-stage grids (75, 120): V(r) in shared
+// memory when the plane takes at most 48 KB, one band per CTA
+template <int NN>
+static cudaError_t launch_plane_vloc64_x(const FftLaunch &L, const void *Vr, void *A, int nb, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    constexpr bool VS = NN * NN * 8 <= 48 * 1024;
+    PlaneXSmem ps{NN, plane_ld<NN>(), kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), VS ? vplane_elems<double, NN, NN>() : 0};
+    ps.bands = 1;
+    ps.xs = pwf::fp_xs<NN>();
+    ps.twn = xtw_len<NN>();
+    const size_t smem = ps.elems() * sizeof(double2);
+    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    cudaError_t e = set_smem<double>((const void *)kx_plane_vloc64<NN, NN, VS, 1>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(kp.N3, nb);
+    kx_plane_vloc64<NN, NN, VS, 1><<<grid, FFT_THREADS, smem, st>>>(kp, (const double2 *)L.twx, (const double2 *)L.twy,
+                                                                    (const double *)Vr, (double2 *)A, nb);
+    return cudaGetLastError();
 }
 template <int NN>
 static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb, int G, int Bg, const double *w,
@@ -1313,6 +1358,9 @@ cudaError_t launch_plane_vloc(const FftLaunch &L, const void *Vr, void *A, int n
             FIXED_SIZES(PW_CASE)
 #undef PW_CASE
         }
+    } else {
+        if (kp.N1 == kp.N2 && kp.N1 == 75) return launch_plane_vloc64_x<75>(L, Vr, A, nb, st);
+        if (kp.N1 == kp.N2 && kp.N1 == 120) return launch_plane_vloc64_x<120>(L, Vr, A, nb, st);
     }
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
