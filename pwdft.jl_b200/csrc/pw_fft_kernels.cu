@@ -268,7 +268,9 @@ __global__ void k_zero(Cx<T> *p, int Ngw, int nb, int64_t ld) {
 // pw_fft_tmpl.cuh); used for the grid sizes listed in FIXED_SIZES below,
 // the run-time kernels above serve every other {2,3,5}-smooth size.
 // FP32 lines use the register-fused composite radices (fewer shared-memory
-// passes); FP64 lines keep the 2/3/4/5/8 stages (register pressure).
+// passes); FP64 lines here keep the 2/3/4/5/8 stages (register pressure in
+// the z passes); the FP64 x-fused plane pass (kx_plane_vloc64) calls the
+// fused plans directly with one CTA per SM.
 template <typename T, int N, bool JF, bool PAD = false>
 __device__ __forceinline__ void line_fft(Cx<T> *buf, int nl, int es, int ls, const Cx<T> *tw, int sign) {
     static_assert(!PAD || sizeof(T) == 4, "padded lines are FP32 only");
