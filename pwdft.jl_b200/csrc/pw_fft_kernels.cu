@@ -737,12 +737,11 @@ kx_plane_vloc64(KPlan kp, const double2 *__restrict__ twx, const double2 *__rest
 // calc_rhoe: bands [g*Bg, min(nb, (g+1)*Bg)) of plane kz; the weighted
 // |psi(r)|^2 accumulate in shared memory when the plane fits (RS), else in
 // the global partial sums directly.
-template <int N1, int N2, bool RS>
-__global__ void __launch_bounds__(FFT_THREADS, 2)
-kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float2 *__restrict__ A,
-             int nb, int Bg, const double *__restrict__ w, float *__restrict__ rho_part) {
+template <typename T, int N1, int N2, bool RS>
+__device__ __forceinline__ void plane_rho_x_body(const KPlan &kp, const Cx<T> *__restrict__ twx,
+                                                 const Cx<T> *__restrict__ twy, const Cx<T> *__restrict__ A, int nb,
+                                                 int Bg, const double *__restrict__ w, T *__restrict__ rho_part) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using T = float;
     constexpr int G = pwf::fp_group<N1>();
     constexpr int N12 = N1 * N2;
     const int N3 = kp.N3, Nxa = kp.Nxa, Ncol = kp.Ncol;
@@ -753,17 +752,18 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
     Cx<T> *S = ty + N2;
     constexpr int XS = pwf::fp_xs<N1>();
     Cx<T> *Xw = S + Nxa * N2 + (size_t)warp * G * XS;
-    float *Rs = reinterpret_cast<float *>(S + Nxa * N2 + (size_t)NW * G * XS);
+    T *Rs = reinterpret_cast<T *>(S + Nxa * N2 + (size_t)NW * G * XS);
     short *iax = reinterpret_cast<short *>(Rs + (RS ? N12 + (N12 & 1) : 0));
     const int kz = blockIdx.x, g = blockIdx.y;
-    float *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
+    T *rp = rho_part + (size_t)g * N12 * N3 + (size_t)kz * N12;
+    // the tables of twx, twy are in natural order (entry i of the fused layout: tw_src(i))
     for (int i = threadIdx.x; i < N1; i += FFT_THREADS) {
-        tx[i] = twx[tw_src<float, N1>(i)];
+        tx[i] = twx[pwf::tw_src<N1>(i)];
         iax[i] = -1;
     }
-    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[tw_src<float, N2>(i)];
-    float *acc = RS ? Rs : rp;
-    for (int i = threadIdx.x; i < N12; i += FFT_THREADS) acc[i] = 0.0f;
+    for (int i = threadIdx.x; i < N2; i += FFT_THREADS) ty[i] = twy[pwf::tw_src<N2>(i)];
+    T *acc = RS ? Rs : rp;
+    for (int i = threadIdx.x; i < N12; i += FFT_THREADS) acc[i] = (T)0;
     __syncthreads();
     for (int i = threadIdx.x; i < Nxa; i += FFT_THREADS) iax[kp.xa[i]] = (short)i;
     const int b0 = g * Bg, b1 = min(nb, b0 + Bg);
@@ -775,7 +775,7 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
 #pragma unroll 4
         for (int c = threadIdx.x; c < Ncol; c += FFT_THREADS) S[kp.col_ia[c] * N2 + kp.col_j[c]] = Ap[c];
         __syncthreads();
-        line_fft<T, N2, true>(S, Nxa, 1, N2, ty, +1);
+        pwf::lines<T, N2, true>(S, Nxa, 1, N2, ty, +1);
         for (int g0 = warp * G; g0 < N2; g0 += NW * G) {
             const int nl = min(G, N2 - g0);
             auto ld_s = [&](int line, int x, int) {
@@ -789,6 +789,21 @@ kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict_
     }
     if constexpr (RS)
         for (int i = threadIdx.x; i < N12; i += FFT_THREADS) rp[i] = Rs[i];
+}
+
+template <int N1, int N2, bool RS>
+__global__ void __launch_bounds__(FFT_THREADS, 2)
+kx_plane_rho(KPlan kp, const float2 *__restrict__ twx, const float2 *__restrict__ twy, const float2 *__restrict__ A,
+             int nb, int Bg, const double *__restrict__ w, float *__restrict__ rho_part) {
+    plane_rho_x_body<float, N1, N2, RS>(kp, twx, twy, A, nb, Bg, w, rho_part);
+}
+
+// The same x-fused density pass in FP64, one CTA per SM.
+template <int N1, int N2, bool RS>
+__global__ void __launch_bounds__(FFT_THREADS, 1)
+kx_plane_rho64(KPlan kp, const double2 *__restrict__ twx, const double2 *__restrict__ twy, const double2 *__restrict__ A,
+               int nb, int Bg, const double *__restrict__ w, double *__restrict__ rho_part) {
+    plane_rho_x_body<double, N1, N2, RS>(kp, twx, twy, A, nb, Bg, w, rho_part);
 }
 
 // ------------------------------------------ batched op_H over k-points
@@ -1209,7 +1224,7 @@ static cudaError_t launch_plane_vloc64_x(const FftLaunch &L, const void *Vr, voi
     ps.xs = pwf::fp_xs<NN>();
     ps.twn = xtw_len<NN>();
     const size_t smem = ps.elems() * sizeof(double2);
-    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+    if (smem > 227 * 1024) return cudaErrorNotSupported;   // the caller takes the plane-wide kernel
     cudaError_t e = set_smem<double>((const void *)kx_plane_vloc64<NN, NN, VS, 1>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid(kp.N3, nb);
@@ -1230,6 +1245,25 @@ static cudaError_t launch_plane_rho_x(const FftLaunch &L, const void *A, int nb,
     dim3 grid(kp.N3, G);
     kx_plane_rho<NN, NN, RS><<<grid, FFT_THREADS, smem, st>>>(kp, (const float2 *)L.twx, (const float2 *)L.twy,
                                                              (const float2 *)A, nb, Bg, w, (float *)rho_part);
+    return cudaGetLastError();
+}
+
+// FP64 x-fused density pass on the two-stage grids: the density plane in
+// shared memory when it takes at most 48 KB, else the global partial sums
+template <int NN>
+static cudaError_t launch_plane_rho64_x(const FftLaunch &L, const void *A, int nb, int G, int Bg, const double *w,
+                                        void *rho_part, cudaStream_t st) {
+    const KPlan &kp = L.kp;
+    constexpr bool RS = NN * NN * 8 <= 48 * 1024;
+    PlaneXSmem ps{NN, NN, kp.Nxa, FFT_THREADS / 32, pwf::fp_group<NN>(), RS ? NN * NN : 0};
+    ps.xs = pwf::fp_xs<NN>();
+    const size_t smem = ps.elems() * sizeof(double2);
+    if (smem > 227 * 1024) return cudaErrorNotSupported;   // the caller takes the plane-wide kernel
+    cudaError_t e = set_smem<double>((const void *)kx_plane_rho64<NN, NN, RS>, smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(kp.N3, G);
+    kx_plane_rho64<NN, NN, RS><<<grid, FFT_THREADS, smem, st>>>(kp, (const double2 *)L.twx, (const double2 *)L.twy,
+                                                               (const double2 *)A, nb, Bg, w, (double *)rho_part);
     return cudaGetLastError();
 }
 
@@ -1360,9 +1394,11 @@ cudaError_t launch_plane_vloc(const FftLaunch &L, const void *Vr, void *A, int n
             FIXED_SIZES(PW_CASE)
 #undef PW_CASE
         }
-    } else {
-        if (kp.N1 == kp.N2 && kp.N1 == 75) return launch_plane_vloc64_x<75>(L, Vr, A, nb, st);
-        if (kp.N1 == kp.N2 && kp.N1 == 120) return launch_plane_vloc64_x<120>(L, Vr, A, nb, st);
+    } else if (kp.N1 == kp.N2 && (kp.N1 == 75 || kp.N1 == 120)) {
+        // x-fused when its sub-plane fits in shared memory (active x up to ~80 of 120)
+        const cudaError_t e = kp.N1 == 75 ? launch_plane_vloc64_x<75>(L, Vr, A, nb, st)
+                                          : launch_plane_vloc64_x<120>(L, Vr, A, nb, st);
+        if (e != cudaErrorNotSupported) return e;
     }
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
@@ -1398,6 +1434,10 @@ cudaError_t launch_plane_rho(const FftLaunch &L, const void *A, int nb, int G, i
             FIXED_SIZES(PW_CASE)
 #undef PW_CASE
         }
+    } else if (kp.N1 == kp.N2 && (kp.N1 == 75 || kp.N1 == 120)) {
+        const cudaError_t e = kp.N1 == 75 ? launch_plane_rho64_x<75>(L, A, nb, G, Bg, w, rho_part, st)
+                                          : launch_plane_rho64_x<120>(L, A, nb, G, Bg, w, rho_part, st);
+        if (e != cudaErrorNotSupported) return e;
     }
     PlaneSmem ps{kp.N1, kp.N2, kp.Nxa, L.Jc};
     size_t smem = ps.elems() * sizeof(Cx<T>);
