@@ -95,6 +95,118 @@ template <typename T> struct SmallDft<T, 8> {
     }
 };
 
+// FP32 butterflies on the paired FP32 pipe of sm_100 (one FFMA2 / FADD2 /
+// FMUL2 per complex add, real-constant multiply-add or real scale, where
+// the scalar formulas above take two).  A product by +-i is folded into
+// the FFMA2 that consumes it: r + i s u = (r.x - s u.y, r.y + s u.x) is one
+// FFMA2 of the swapped pair (u.y, u.x) with (-s, s); where the operand is
+// a difference, the swapped pair is formed directly by two scalar
+// subtractions.  Host builds take the same lane-wise formulas with fmaf.
+namespace pk {
+__host__ __device__ __forceinline__ float2 bc(float c) { return make_float2(c, c); }
+__host__ __device__ __forceinline__ float2 add(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    return __fadd2_rn(a, b);
+#else
+    return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 mul(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    return __fmul2_rn(a, b);
+#else
+    return make_float2(a.x * b.x, a.y * b.y);
+#endif
+}
+// a * b + c per lane, one rounding
+__host__ __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
+    return __ffma2_rn(a, b, c);
+#else
+    return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+#endif
+}
+// a - b (exact product by -1, one rounding: the same value as a scalar subtraction)
+__host__ __device__ __forceinline__ float2 sub(float2 a, float2 b) { return fma(b, bc(-1.0f), a); }
+// (a - b) with its lanes swapped: (a.y - b.y, a.x - b.x)
+__host__ __device__ __forceinline__ float2 subsw(float2 a, float2 b) { return make_float2(a.y - b.y, a.x - b.x); }
+__host__ __device__ __forceinline__ float2 swp(float2 a) { return make_float2(a.y, a.x); }
+}  // namespace pk
+
+template <> struct SmallDft<float, 2> {
+    static __host__ __device__ __forceinline__ void run(float2 *v, float) {
+        const float2 a = v[0], b = v[1];
+        v[0] = pk::add(a, b);
+        v[1] = pk::sub(a, b);
+    }
+};
+
+template <> struct SmallDft<float, 3> {
+    static __host__ __device__ __forceinline__ void run(float2 *v, float s) {
+        const float sc = s * (float)PW_SQRT3_2;
+        const float2 t1 = pk::add(v[1], v[2]);
+        const float2 t2 = pk::fma(t1, pk::bc(-0.5f), v[0]);
+        const float2 ds = pk::subsw(v[1], v[2]);        // i s sqrt3/2 (v1 - v2) = (-sc ds.x, sc ds.y)
+        v[0] = pk::add(v[0], t1);
+        v[1] = pk::fma(ds, make_float2(-sc, sc), t2);
+        v[2] = pk::fma(ds, make_float2(sc, -sc), t2);
+    }
+};
+
+template <> struct SmallDft<float, 4> {
+    static __host__ __device__ __forceinline__ void run(float2 *v, float s) {
+        const float2 a = pk::add(v[0], v[2]), b = pk::sub(v[0], v[2]);
+        const float2 c = pk::add(v[1], v[3]);
+        const float2 ds = pk::subsw(v[1], v[3]);        // i s (v1 - v3) = (-s ds.x, s ds.y)
+        v[0] = pk::add(a, c);
+        v[2] = pk::sub(a, c);
+        v[1] = pk::fma(ds, make_float2(-s, s), b);
+        v[3] = pk::fma(ds, make_float2(s, -s), b);
+    }
+};
+
+template <> struct SmallDft<float, 5> {
+    static __host__ __device__ __forceinline__ void run(float2 *v, float s) {
+        const float2 x0 = v[0];
+        const float2 a1 = pk::add(v[1], v[4]), a2 = pk::add(v[2], v[3]);
+        const float2 b1 = pk::subsw(v[1], v[4]), b2 = pk::subsw(v[2], v[3]);   // swapped differences
+        const float2 r1 = pk::fma(a2, pk::bc((float)PW_C5_2), pk::fma(a1, pk::bc((float)PW_C5_1), x0));
+        const float2 r2 = pk::fma(a2, pk::bc((float)PW_C5_1), pk::fma(a1, pk::bc((float)PW_C5_2), x0));
+        // swapped u1 = b1 S1 + b2 S2 and u2 = b1 S2 - b2 S1; r -+ i s u
+        const float2 u1 = pk::fma(b2, pk::bc((float)PW_S5_2), pk::mul(b1, pk::bc((float)PW_S5_1)));
+        const float2 u2 = pk::fma(b2, pk::bc(-(float)PW_S5_1), pk::mul(b1, pk::bc((float)PW_S5_2)));
+        const float2 pm = make_float2(-s, s), mp = make_float2(s, -s);
+        v[0] = pk::add(x0, pk::add(a1, a2));
+        v[1] = pk::fma(u1, pm, r1);
+        v[4] = pk::fma(u1, mp, r1);
+        v[2] = pk::fma(u2, pm, r2);
+        v[3] = pk::fma(u2, mp, r2);
+    }
+};
+
+template <> struct SmallDft<float, 8> {
+    static __host__ __device__ __forceinline__ void run(float2 *v, float s) {
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        SmallDft<float, 4>::run(e, s);
+        SmallDft<float, 4>::run(o, s);
+        const float h = (float)PW_RSQRT2;
+        const float2 pm = make_float2(-s, s), mp = make_float2(s, -s);
+        // w8 o1 = h (o1 + i s o1); w8^3 o3 = -h (o3 - i s o3); w8^2 o2 = i s o2
+        const float2 t1 = pk::fma(pk::swp(o[1]), pm, o[1]);
+        const float2 q3 = pk::fma(pk::swp(o[3]), mp, o[3]);
+        const float2 o2 = pk::swp(o[2]);
+        v[0] = pk::add(e[0], o[0]);
+        v[4] = pk::sub(e[0], o[0]);
+        v[1] = pk::fma(t1, pk::bc(h), e[1]);
+        v[5] = pk::fma(t1, pk::bc(-h), e[1]);
+        v[2] = pk::fma(o2, pm, e[2]);
+        v[6] = pk::fma(o2, mp, e[2]);
+        v[3] = pk::fma(q3, pk::bc(-h), e[3]);
+        v[7] = pk::fma(q3, pk::bc(h), e[3]);
+    }
+};
+
 // One radix-R stage over `nlines` lines of length n; element (line, idx)
 // lives at buf[line*ls + idx*es].  Threads are mapped line-fastest.
 template <typename T, int R, int MAXV>
