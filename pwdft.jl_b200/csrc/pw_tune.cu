@@ -17,6 +17,7 @@
 
 #include "../../include/pwb200.h"
 #include "pw_launch.h"
+#include "pw_tune_cache.h"
 
 cudaStream_t pwk_stream(pw_ctx *c);
 int pwk_device(const pw_ctx *c);
@@ -81,41 +82,6 @@ double time_ms(cudaStream_t st, F &&f, int warm = 2, int reps = 5) {
     return ts[ts.size() / 2];
 }
 
-bool read_cache(const char *path, const std::string &key, pw_tuning *t) {
-    if (!path || !*path) return false;
-    FILE *f = std::fopen(path, "r");
-    if (!f) return false;
-    char line[1024];
-    bool hit = false;
-    while (std::fgets(line, sizeof(line), f)) {
-        char *tab = std::strchr(line, '\t');
-        if (!tab) continue;
-        *tab = 0;
-        if (key != line) continue;
-        long long chunk = 0;
-        int bpc = 0, zc = 0, sp = 0;
-        if (std::sscanf(tab + 1, "%lld %d %d %d", &chunk, &bpc, &zc, &sp) == 4) {
-            std::memset(t, 0, sizeof(*t));
-            t->band_chunk_bytes = chunk;
-            t->plane_bands = bpc;
-            t->z_columns = zc;
-            t->gemm_splits = sp;
-            hit = true;   // the last matching line wins
-        }
-    }
-    std::fclose(f);
-    return hit;
-}
-
-void append_cache(const char *path, const std::string &key, const pw_tuning &t) {
-    if (!path || !*path) return;
-    FILE *f = std::fopen(path, "a");
-    if (!f) return;
-    std::fprintf(f, "%s\t%lld %d %d %d\n", key.c_str(), (long long)t.band_chunk_bytes, t.plane_bands, t.z_columns,
-                 t.gemm_splits);
-    std::fclose(f);
-}
-
 }  // namespace
 
 extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cache_path, pw_tuning *chosen,
@@ -132,13 +98,10 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return pwk_fail_msg(c, PW_ERR_CUDA, "cudaGetDeviceProperties failed");
     const int ngw = pwk_ngw(c, ik);
-    char keyb[512];
-    std::snprintf(keyb, sizeof(keyb), "gpu=%s;Ns=%dx%dx%d;Ngw=%d;Ncol=%d;Nxa=%d;nb=%d;dtype=%d;nbeta=%d", prop.name, Ns[0],
-                  Ns[1], Ns[2], ngw, Ncol, Nxa, nb, dtype, nbeta);
-    const std::string key(keyb);
+    const std::string key = pwk::tune::cache_key(prop.name, Ns, ngw, Ncol, Nxa, nb, dtype, nbeta);
     const char *path = cache_path ? cache_path : std::getenv("PW_AUTOTUNE_CACHE");
     pw_tuning t;
-    if (read_cache(path, key, &t)) {
+    if (pwk::tune::read_cache(path, key, &t)) {
         int s = pw_set_tuning(c, &t);
         if (s) return s;
         pw_get_tuning(c, &t);   // the values in effect (a zero field reads as its default)
@@ -171,15 +134,7 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
     }
     const double tdef = tbest;
     auto try_field = [&](auto setter, const std::vector<int64_t> &vals) {
-        for (int64_t v : vals) {
-            pw_tuning cand = best;
-            setter(cand, v);
-            const double tm = eval(cand);
-            if (tm > 0 && tm < tbest * 0.995) {
-                tbest = tm;
-                best = cand;
-            }
-        }
+        pwk::tune::descend(best, tbest, eval, setter, vals);
     };
     if (f32 && Ns[0] == Ns[1] && (Ns[0] == 27 || Ns[0] == 75 || Ns[0] == 120))
         try_field([](pw_tuning &x, int64_t v) { x.plane_bands = (int32_t)v; }, {1, 2, 3});
@@ -214,7 +169,7 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
                 if (pw_set_tuning(c, &cand) != PW_OK) continue;
                 const double tm = time_ms(st, run_rr);
                 if (sp == 0) gdef = tm;
-                if (tm > 0 && (gbest < 0 || tm < gbest * 0.995)) {
+                if (tm > 0 && (gbest < 0 || pwk::tune::faster(tm, gbest))) {
                     gbest = tm;
                     sbest = sp;
                 }
@@ -231,7 +186,7 @@ extern "C" int pw_autotune(pw_ctx *c, int ik, int nb, int dtype, const char *cac
     int s = pw_set_tuning(c, &best);
     if (s) return s;
     pw_get_tuning(c, &best);    // the values in effect (a zero field reads as its default)
-    append_cache(path, key, best);
+    pwk::tune::append_cache(path, key, best);
     if (chosen) *chosen = best;
     return PW_OK;
 }
