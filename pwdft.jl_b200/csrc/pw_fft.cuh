@@ -27,7 +27,7 @@
 template <typename T, int R> struct SmallDft;
 
 template <typename T> struct SmallDft<T, 2> {
-    static __device__ __forceinline__ void run(Cx<T> *v, T) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T) {
         Cx<T> a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
@@ -35,7 +35,7 @@ template <typename T> struct SmallDft<T, 2> {
 };
 
 template <typename T> struct SmallDft<T, 3> {
-    static __device__ __forceinline__ void run(Cx<T> *v, T s) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s) {
         Cx<T> t1 = cadd(v[1], v[2]);
         Cx<T> t2 = csub(v[0], cscale(t1, (T)0.5));
         Cx<T> t3 = cmul_is(cscale(csub(v[1], v[2]), (T)PW_SQRT3_2), s);
@@ -46,7 +46,7 @@ template <typename T> struct SmallDft<T, 3> {
 };
 
 template <typename T> struct SmallDft<T, 4> {
-    static __device__ __forceinline__ void run(Cx<T> *v, T s) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s) {
         Cx<T> a = cadd(v[0], v[2]), b = csub(v[0], v[2]);
         Cx<T> c = cadd(v[1], v[3]), d = cmul_is(csub(v[1], v[3]), s);
         v[0] = cadd(a, c);
@@ -57,7 +57,7 @@ template <typename T> struct SmallDft<T, 4> {
 };
 
 template <typename T> struct SmallDft<T, 5> {
-    static __device__ __forceinline__ void run(Cx<T> *v, T s) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s) {
         Cx<T> a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
         Cx<T> a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
         Cx<T> x0 = v[0];
@@ -74,7 +74,7 @@ template <typename T> struct SmallDft<T, 5> {
 };
 
 template <typename T> struct SmallDft<T, 8> {
-    static __device__ __forceinline__ void run(Cx<T> *v, T s) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s) {
         Cx<T> e[4] = {v[0], v[2], v[4], v[6]};
         Cx<T> o[4] = {v[1], v[3], v[5], v[7]};
         SmallDft<T, 4>::run(e, s);

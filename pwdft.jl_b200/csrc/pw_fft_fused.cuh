@@ -15,11 +15,11 @@ namespace pwf {
 template <typename T, int R> struct Dft;
 
 // radices with direct formulas
-template <typename T> struct Dft<T, 2> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 2>::run(v, s); } };
-template <typename T> struct Dft<T, 3> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 3>::run(v, s); } };
-template <typename T> struct Dft<T, 4> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 4>::run(v, s); } };
-template <typename T> struct Dft<T, 5> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 5>::run(v, s); } };
-template <typename T> struct Dft<T, 8> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 8>::run(v, s); } };
+template <typename T> struct Dft<T, 2> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 2>::run(v, s); } };
+template <typename T> struct Dft<T, 3> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 3>::run(v, s); } };
+template <typename T> struct Dft<T, 4> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 4>::run(v, s); } };
+template <typename T> struct Dft<T, 5> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 5>::run(v, s); } };
+template <typename T> struct Dft<T, 8> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *, int) { SmallDft<T, 8>::run(v, s); } };
 
 // exp(-2 pi i m / R) evaluated at compile time: Taylor series of sin and
 // cos about 0 after reduction to [-pi, pi] (30 terms: below 1e-17 there).
@@ -41,7 +41,7 @@ template <int M, int R> struct Root {
 };
 
 // compile-time loop: f(std::integral_constant<int, I>) for I in [I0, I1)
-template <int I0, int I1, class F> __device__ __forceinline__ void sfor(F &&f) {
+template <int I0, int I1, class F> __host__ __device__ __forceinline__ void sfor(F &&f) {
     if constexpr (I0 < I1) {
         f(std::integral_constant<int, I0>{});
         sfor<I0 + 1, I1>(f);
@@ -52,7 +52,7 @@ template <int I0, int I1, class F> __device__ __forceinline__ void sfor(F &&f) {
 // (no table reads; tw and step pass through to the sub-DFTs, which ignore
 // them too).
 template <typename T, int R1, int R2> struct CompDft {
-    static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
         constexpr int R = R1 * R2;
         Cx<T> a[R];
         sfor<0, R2>([&](auto n2c) {
@@ -93,7 +93,7 @@ template <int A, int M> __host__ __device__ constexpr int inv_mod() {
     return r;
 }
 template <typename T, int R1, int R2> struct PfaDft {
-    static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
+    static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int step) {
         constexpr int R = R1 * R2;
         constexpr int E1 = R2 * inv_mod<R2 % R1, R1>(), E2 = R1 * inv_mod<R1 % R2, R2>();   // CRT idempotents
         Cx<T> a[R];
@@ -117,11 +117,11 @@ template <typename T, int R1, int R2> struct PfaDft {
         }
     }
 };
-template <typename T> struct Dft<T, 9> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 3, 3>::run(v, s, tw, st); } };
-template <typename T> struct Dft<T, 15> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { PfaDft<T, 3, 5>::run(v, s, tw, st); } };
-template <typename T> struct Dft<T, 24> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 8, 3>::run(v, s, tw, st); } };
-template <typename T> struct Dft<T, 25> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 5, 5>::run(v, s, tw, st); } };
-template <typename T> struct Dft<T, 27> { static __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 9, 3>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 9> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 3, 3>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 15> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { PfaDft<T, 3, 5>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 24> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 8, 3>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 25> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 5, 5>::run(v, s, tw, st); } };
+template <typename T> struct Dft<T, 27> { static __host__ __device__ __forceinline__ void run(Cx<T> *v, T s, const Cx<T> *tw, int st) { CompDft<T, 9, 3>::run(v, s, tw, st); } };
 
 // Fused plans: radices per stage (product = N).
 template <int N> struct FPlan;
