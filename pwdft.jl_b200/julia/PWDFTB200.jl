@@ -203,6 +203,10 @@ function apply!(Ham::B200Hamiltonian, psi::AbstractMatrix{ComplexF64}, Hpsi::Abs
     dev = device(Ham)
     p = dense(psi)
     h = (Hpsi isa StridedMatrix && stride(Hpsi, 1) == 1) ? Hpsi : Matrix(Hpsi)
+    if stride(h, 2) != stride(p, 2)   # pw_op_H_host takes one leading dimension for both blocks
+        p = Matrix(psi)
+        h === Hpsi && (h = Matrix(Hpsi))
+    end
     check(ccall((:pw_op_H_host, libpwb200), Cint,
                 (Ptr{Cvoid}, Cint, Cint, Ptr{ComplexF64}, Ptr{ComplexF64}, Int64, Cint, Cuint, Cint),
                 dev.ctx, Ham.ik - 1, Ham.ispin - 1, p, h, stride(p, 2), size(p, 2), ops, dev.dtype), dev.ctx)
