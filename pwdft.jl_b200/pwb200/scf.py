@@ -1,7 +1,7 @@
 """KS_solve_SCF! with every step of the SCF iteration on the device.
 
-Mirrors KS_solve_SCF.jl:24-373 (Nspin = 1, no smearing, Pulay or simple
-density mixing):
+Mirrors KS_solve_SCF.jl:24-373 (Nspin = 1; simple density mixing by default,
+as there, or Pulay; Fermi-Dirac smearing):
   ethr schedule            KS_solve_SCF.jl:177-185
   diag_LOBPCG!             pw_lobpcg per k-point          (device, update_psi="LOBPCG"), or
                            pw_lobpcg_multi for all k-points together (batched=True, nb <= 16)
@@ -121,7 +121,7 @@ def rand_psiks(Ham, Nstates, seed, dtype, keep=None):
     return out
 
 
-def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay", mixdim=5, etot_conv_thr=1e-6,
+def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="simple", mixdim=5, etot_conv_thr=1e-6,
                  ethr_evals_last=1e-5, NiterMax=100, precision="fp64", fp64_switch=1e-5, seed=1234, psiks=None,
                  verbose=False, lobpcg_maxiter=100, update_psi="LOBPCG", use_smearing=False, kT=1e-3,
                  savewfc=False, wfc_dir=".", batched=False, cheby_degree=8):
@@ -145,6 +145,11 @@ def KS_solve_SCF(Ham, meshk=None, Nstates=None, betamix=0.2, mix_method="pulay",
     Ham.setup_density()
     if update_psi not in ("LOBPCG", "davidson", "davidson_qe", "CheFSI", "PCG"):
         raise ValueError("update_psi must be 'LOBPCG', 'davidson', 'davidson_qe', 'CheFSI' or 'PCG'")
+    if mix_method not in ("simple", "pulay"):
+        # KS_solve_SCF.jl:240-272 also has linear_adaptive, broyden, rpulay,
+        # ppulay and anderson, and raises on any other name
+        raise ValueError("mix_method must be 'simple' or 'pulay' (the reference's linear_adaptive, broyden, "
+                         "rpulay, ppulay and anderson mixers are not built)")
     if update_psi == "PCG" and precision != "fp64":
         raise ValueError("update_psi='PCG' (diag_Emin_PCG!) runs on FP64 blocks only")
     if update_psi == "davidson" and precision != "fp64":

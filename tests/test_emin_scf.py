@@ -213,3 +213,6 @@ def test_scf_rejects_unsupported_choices():
         scf.KS_solve_SCF(Hd, update_psi="nonexistent")
     with pytest.raises(ValueError):
         scf.KS_solve_SCF(Hd, update_psi="davidson", precision="mixed")
+    for m in ("broyden", "anderson", "nonexistent"):
+        with pytest.raises(ValueError):
+            scf.KS_solve_SCF(Hd, mix_method=m)
