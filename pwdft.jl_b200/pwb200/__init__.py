@@ -158,12 +158,33 @@ def diag_davidson_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
 __all__ += ["diag_davidson_"]
 
 
-def diag_Emin_PCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0, tol_ebands=1e-4, alpha_t=3e-5, I_CG_BETA=2):
+# The reference's keyword names that are not ASCII, and its print switches
+# (output only, accepted and ignored)
+_KW_RENAME = {"\u03b1_t": "alpha_t", "\u03b1_max": "alpha_max"}
+_KW_PRINT = ("verbose_last", "print_final_ebands", "print_final_energies")
+
+
+def _reference_kwargs(kwargs):
+    out = {}
+    for k, v in kwargs.items():
+        if k in _KW_PRINT:
+            continue
+        out[_KW_RENAME.get(k, k)] = v
+    return out
+
+
+def diag_Emin_PCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0, tol_ebands=1e-4, alpha_t=3e-5, I_CG_BETA=2,
+                   verbose=False, **kwargs):
     """diag_Emin_PCG!(Ham, psiks; tol, NiterMax, Nstates_conv, tol_ebands, α_t, I_CG_BETA)
     (diag_Emin_PCG.jl:17-47): all-band PCG per k-point on complex128 blocks
-    (pwb200.emin_pcg)."""
+    (pwb200.emin_pcg).  The reference's own keyword names (α_t, verbose,
+    verbose_last) are accepted as well."""
     import numpy as np
     from .emin_pcg import diag_Emin_PCG_k
+    kw = _reference_kwargs(kwargs)
+    alpha_t = kw.pop("alpha_t", alpha_t)
+    if kw:
+        raise TypeError("diag_Emin_PCG_: unexpected keyword arguments %s" % sorted(kw))
     evals = np.zeros((psiks[0].shape[0], len(psiks)))
     for ik, X in enumerate(psiks):
         Ham.ik = ik
@@ -179,16 +200,19 @@ __all__ += ["diag_Emin_PCG_"]
 def KS_solve_SCF_(Ham, **kwargs):
     """KS_solve_SCF!(Ham; ...) (KS_solve_SCF.jl:24-373): pwb200.scf.KS_solve_SCF
     (update_psi "LOBPCG" | "davidson" | "CheFSI" | "PCG", precision "fp64" |
-    "mixed", smearing, symmetry, k-point sharding over a process group)."""
+    "mixed", smearing, symmetry, k-point sharding over a process group).  The
+    reference's print switches are accepted and ignored."""
     from .scf import KS_solve_SCF
-    return KS_solve_SCF(Ham, **kwargs)
+    return KS_solve_SCF(Ham, **_reference_kwargs(kwargs))
 
 
 def KS_solve_Emin_PCG_(Ham, psiks=None, **kwargs):
     """KS_solve_Emin_PCG!(Ham, psiks; ...) (KS_solve_Emin_PCG.jl:27-270):
-    pwb200.emin_scf.KS_solve_Emin_PCG."""
+    pwb200.emin_scf.KS_solve_Emin_PCG.  The reference's keyword names α_t and
+    α_max are accepted for alpha_t and alpha_max, its print switches are
+    ignored."""
     from .emin_scf import KS_solve_Emin_PCG
-    return KS_solve_Emin_PCG(Ham, psiks, **kwargs)
+    return KS_solve_Emin_PCG(Ham, psiks, **_reference_kwargs(kwargs))
 
 
 __all__ += ["KS_solve_SCF_", "KS_solve_Emin_PCG_"]

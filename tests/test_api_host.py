@@ -5,6 +5,7 @@ context: k-point loop, Ham.ik bookkeeping, argument order and the
 (Nstates, Nkpt) eigenvalue layout.  No device code runs here; the device
 paths have their own parity tests (test_lobpcg_gpu, test_chefsi_gpu)."""
 import numpy as np
+import pytest
 
 
 class FakeCtx:
@@ -116,7 +117,22 @@ def test_driver_aliases_forward_arguments(monkeypatch):
     seen = {}
     monkeypatch.setattr(scf, "KS_solve_SCF", lambda Ham, **kw: seen.setdefault("scf", (Ham, kw)))
     monkeypatch.setattr(emin_scf, "KS_solve_Emin_PCG", lambda Ham, psiks, **kw: seen.setdefault("emin", (Ham, psiks, kw)))
-    pwb200.KS_solve_SCF_("H", update_psi="PCG", etot_conv_thr=1e-7)
-    pwb200.KS_solve_Emin_PCG_("H", None, i_cg_beta=3)
+    pwb200.KS_solve_SCF_("H", update_psi="PCG", etot_conv_thr=1e-7, print_final_ebands=True)
+    pwb200.KS_solve_Emin_PCG_("H", None, i_cg_beta=3, **{"\u03b1_t": 1e-5, "\u03b1_max": 1.5})
     assert seen["scf"] == ("H", {"update_psi": "PCG", "etot_conv_thr": 1e-7})
-    assert seen["emin"] == ("H", None, {"i_cg_beta": 3})
+    assert seen["emin"] == ("H", None, {"i_cg_beta": 3, "alpha_t": 1e-5, "alpha_max": 1.5})
+    from pwb200 import emin_pcg
+    import numpy as np
+
+    def fake_k(ctx, ik, ispin, X, **kw):
+        seen.setdefault("pcg", []).append((ik, kw["alpha_t"], kw["I_CG_BETA"]))
+        return np.zeros(X.shape[0]), 1
+    monkeypatch.setattr(emin_pcg, "diag_Emin_PCG_k", fake_k)
+
+    class H:
+        ctx, ispin, ik = None, 0, 0
+    pwb200.diag_Emin_PCG_(H, [np.zeros((2, 4)), np.zeros((2, 4))], verbose_last=True, I_CG_BETA=3,
+                          **{"\u03b1_t": 2e-5})
+    assert seen["pcg"] == [(0, 2e-5, 3), (1, 2e-5, 3)]
+    with pytest.raises(TypeError):
+        pwb200.diag_Emin_PCG_(H, [np.zeros((2, 4))], alpha_typo=1.0)
