@@ -80,9 +80,10 @@ def calc_rhoe_(Ham, psiks, Rhoe, Focc):
 # (Nspin = 1: psiks holds one (Nstates, Ngw) device block per k-point; the
 # returned evals are (Nstates, Nkpt) like the reference's (Nstates, Nkspin).)
 
-def diag_LOBPCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
-    """diag_LOBPCG!(Ham, psiks; tol, NiterMax, Nstates_conv) (diag_LOBPCG.jl:1-28):
-    every block replaced by its Ritz vectors; returns evals."""
+def diag_LOBPCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0, verbose=False, verbose_last=False):
+    """diag_LOBPCG!(Ham, psiks; tol, NiterMax, verbose, verbose_last,
+    Nstates_conv) (diag_LOBPCG.jl:1-28): every block replaced by its Ritz
+    vectors; returns evals (the print switches are ignored)."""
     import numpy as np
     evals = np.zeros((psiks[0].shape[0], len(psiks)))
     for ik, X in enumerate(psiks):
@@ -91,8 +92,11 @@ def diag_LOBPCG_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
     return evals
 
 
-def diag_davidson_qe_(Ham, psiks, tol=1e-5, NiterMax=100):
-    """diag_davidson_qe!(Ham, psiks; tol, NiterMax) (diag_davidson_qe_v2.jl:6-34)."""
+def diag_davidson_qe_(Ham, psiks, tol=1e-5, NiterMax=100, verbose=False, verbose_last=False, Nstates_conv=0):
+    """diag_davidson_qe!(Ham, psiks; tol, NiterMax, verbose, verbose_last,
+    Nstates_conv) (diag_davidson_qe_v2.jl:6-34); like the reference, which
+    passes only tol and NiterMax on to the per-k solver, Nstates_conv and the
+    print switches have no effect."""
     import numpy as np
     evals = np.zeros((psiks[0].shape[0], len(psiks)))
     for ik, X in enumerate(psiks):
@@ -142,9 +146,10 @@ def ortho_sqrt_(Ham, psi):
 __all__ += ["diag_LOBPCG_", "diag_davidson_qe_", "diag_CheFSI_", "chebyfilt", "get_ub_lb_lanczos", "ortho_sqrt_"]
 
 
-def diag_davidson_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0):
-    """diag_davidson!(Ham, psiks; tol, NiterMax, Nstates_conv) (diag_davidson.jl:12-38):
-    the 2-block Davidson per k-point on complex128 blocks (pwb200.davidson)."""
+def diag_davidson_(Ham, psiks, tol=1e-5, NiterMax=100, Nstates_conv=0, verbose=False, verbose_last=False):
+    """diag_davidson!(Ham, psiks; tol, NiterMax, verbose, verbose_last,
+    Nstates_conv) (diag_davidson.jl:12-38): the 2-block Davidson per k-point
+    on complex128 blocks (pwb200.davidson; the print switches are ignored)."""
     import numpy as np
     from .davidson import diag_davidson_k
     evals = np.zeros((psiks[0].shape[0], len(psiks)))
