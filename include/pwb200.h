@@ -186,7 +186,7 @@ int pw_apply_multi(pw_ctx *ctx, int nk, const int *iks, int ispin, int dtype,
                    void *const *psi, void *const *Hpsi, const int64_t *ld,
                    const int *nb, unsigned ops);
 
-/* out = in / (1 + |G+k|^2)  (Kprec.jl:97-111; in == out allowed). */
+/* out = in / (1 + |G+k|^2)  (Kprec.jl:30-44; in == out allowed). */
 int pw_kprec(pw_ctx *ctx, int ik, int dtype, const void *in, void *out,
              int64_t ld, int nb);
 
@@ -276,7 +276,7 @@ int pw_lobpcg(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
 int pw_davidson(pw_ctx *ctx, int ik, int ispin, int dtype, void *X, int64_t ld,
                 int nb, double tol, int nitermax, double *evals, int *niter);
 
-/* chebyfilt(Ham, X, degree, lb, ub) for k-point ik (CheFSI.jl:36-67): the
+/* chebyfilt(Ham, X, degree, lb, ub) for k-point ik (CheFSI.jl:34-64): the
  * scaled Chebyshev filter of the given degree (>= 1) over [lb, ub]
  * (ub > lb), Y = p(H) X with the three-term recurrence of the reference
  * (sigma1 = e / (lb - ub) fixed, sigma_{i+1} = 1 / (2 / sigma1 - sigma_i)).
@@ -287,7 +287,7 @@ int pw_chebyfilt(pw_ctx *ctx, int ik, int ispin, int dtype, const void *X,
                  void *Y, int64_t ld, int nb, int degree, double lb,
                  double ub);
 
-/* get_ub_lb_lanczos(Ham, nlancz) for k-point ik (CheFSI.jl:70-123, with
+/* get_ub_lb_lanczos(Ham, nlancz) for k-point ik (CheFSI.jl:67-125, with
  * norm_matrix_induced of :127-137): nlancz (even, <= Ngw) Lanczos steps
  * from the start vector v0 (device, Ngw ComplexF64; the reference draws it
  * with randn) with one step of full reorthogonalisation, in FP64.
@@ -401,7 +401,7 @@ int pw_ortho_sqrt(pw_ctx *ctx, int dtype, void *psi, int64_t ld, int64_t ngw,
                   int nb);
 
 /* Rinv = inv(cholesky(Hermitian(C)).U): the upper-triangular factor that
- * diag_LOBPCG.jl:118-125,186-194 divides W and P by (W / R).  C (device,
+ * diag_LOBPCG.jl:144-147,170-174,195-199 divides W and P by (W / R).  C (device,
  * n x n ComplexF64, upper triangle read) is overwritten; Rinv (device, n x n
  * column-major).  PW_ERR_NOT_POSDEF when C is not positive definite. */
 int pw_chol_rinv(pw_ctx *ctx, int n, double *C, double *Rinv);

@@ -13,7 +13,7 @@ test/validations_old/Si_fcc.jl:15) and its logged components
 (test/LOG_runtest_v.1.1.1:1171-1181), the Ewald energy
 (test/test_energies.jl:19), the VWN known answers (test/test_xc.jl:3-4), the
 lattice matrices (test/test_gen_lattice.jl) and the free-electron spectrum
-(timing/time_diag_LOBPCG.jl:141-160).  See tests/test_oracle_golden.py.
+(timing/time_diag_LOBPCG.jl:5-84).  See tests/test_oracle_golden.py.
 
 Module map (each function cites the reference file:line it follows):
   pwgrid     PWGrid.jl, fft_support.jl, KPoints.jl, gen_lattice.jl

@@ -21,7 +21,7 @@ from .lobpcg import ortho_sqrt
 
 
 def chebyfilt(Ham, X, degree, lb, ub, ik=None):
-    """CheFSI.jl:36-67."""
+    """CheFSI.jl:34-64."""
     ik = Ham.ik if ik is None else ik
     ee = (ub - lb) / 2
     c = (ub + lb) / 2
@@ -39,14 +39,14 @@ def chebyfilt(Ham, X, degree, lb, ub, ik=None):
 
 
 def norm_matrix_induced(A):
-    """CheFSI.jl:127-137."""
+    """CheFSI.jl:128-138."""
     N = A.shape[0]
     v1 = np.ones(N) / np.sqrt(N)
     return float(np.linalg.norm(A @ v1))
 
 
 def get_ub_lb_lanczos(Ham, nlancz, v0, ik=None):
-    """CheFSI.jl:70-123 from the start vector v0; returns (ub, lb, T)."""
+    """CheFSI.jl:67-125 from the start vector v0; returns (ub, lb, T)."""
     ik = Ham.ik if ik is None else ik
     ngw = v0.shape[0]
     V = np.zeros((ngw, nlancz), dtype=np.complex128)

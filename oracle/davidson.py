@@ -102,7 +102,7 @@ def diag_davidson_qe_all(Ham, psiks, tol=1e-5, NiterMax=100):
 
 
 def diag_davidson(Ham, X, ik=None, tol=1e-5, NiterMax=100, Nstates_conv=0, hop=None):
-    """The 2-block Davidson of diag_davidson.jl:52-206 for one k-point: the
+    """The 2-block Davidson of diag_davidson.jl:50-191 for one k-point: the
     basis is [X, R] with R the Kprec-preconditioned, normalised residuals;
     X (Nbasis, Nstates), orthonormal on entry, is overwritten with the Ritz
     vectors.  Returns (evals, iterations, converged)."""

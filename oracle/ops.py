@@ -6,7 +6,7 @@ Oracle (test infrastructure only).  Restates PWDFT.jl:
   op_V_Ps_nloc.jl:39-78      op_V_Ps_nloc! for GTH (accumulating)
   PsPotNL.jl:242-254         calc_betaNL_psi
   op_H.jl:53-63              op_H!  (zero, then K + V_loc + V_nloc)
-  Kprec.jl:77-95             Kprec
+  Kprec.jl:10-28             Kprec
   calc_rhoe.jl:9-135         calc_rhoe! (no symmetrisation, no dual grid)
 
 psi is a (Ngw, Nstates) complex128 array in the reference's column order;
@@ -70,7 +70,7 @@ def op_H(Ham, psi, ik=None):
 
 
 def Kprec(Ham, psi, ik=None):
-    """Kprec.jl:77-95: psi / (1 + |G+k|^2)."""
+    """Kprec.jl:10-28: psi / (1 + |G+k|^2)."""
     ik = Ham.ik if ik is None else ik
     return psi / (1.0 + Ham.pw.Gk2(ik))[:, None]
 

@@ -1,9 +1,9 @@
 """PBE exchange-correlation with the reference's internal formulas.
 
 Oracle (test infrastructure only).  Restates PWDFT.jl (Nspin = 1):
-  XC_funcs/XC_x_pbe.jl:3-51     XC_x_pbe   (PBE exchange enhancement, no Slater part)
-  XC_funcs/XC_c_pw.jl:1-37      XC_c_pw    (Perdew-Wang 92 correlation)
-  XC_funcs/XC_c_pbe.jl:3-59     XC_c_pbe   (PBE gradient correction to PW92)
+  XC_funcs/XC_x_pbe.jl:3-49     XC_x_pbe   (PBE exchange enhancement, no Slater part)
+  XC_funcs/XC_c_pw.jl:1-31      XC_c_pw    (Perdew-Wang 92 correlation)
+  XC_funcs/XC_c_pbe.jl:3-53     XC_c_pbe   (PBE gradient correction to PW92)
   GGA_PBE_internal.jl:29-53     calc_epsxc_PBE!
   GGA_PBE_internal.jl:98-145    calc_Vxc_PBE!
   PWGrid.jl:351-375             op_nabla
@@ -18,7 +18,7 @@ from .ham import G_to_R, R_to_G, xc_x_slater
 
 
 def xc_x_pbe(rho, grho):
-    """XC_x_pbe.jl:3-51: (sx, v1x, v2x)."""
+    """XC_x_pbe.jl:3-49: (sx, v1x, v2x)."""
     rho = np.asarray(rho, dtype=np.float64)
     grho = np.asarray(grho, dtype=np.float64)
     ok = (rho > 1e-6) & (grho > 1e-10)
@@ -49,7 +49,7 @@ def xc_x_pbe(rho, grho):
 
 
 def xc_c_pw(rho):
-    """XC_c_pw.jl:1-37: (ec, vc)."""
+    """XC_c_pw.jl:1-31: (ec, vc)."""
     rho = np.asarray(rho, dtype=np.float64)
     ok = rho > 1e-10
     r = np.where(ok, rho, 1.0)
@@ -69,7 +69,7 @@ def xc_c_pw(rho):
 
 
 def xc_c_pbe(rho, grho):
-    """XC_c_pbe.jl:3-59: (sc, v1c, v2c)."""
+    """XC_c_pbe.jl:3-53: (sc, v1c, v2c)."""
     rho = np.asarray(rho, dtype=np.float64)
     grho = np.asarray(grho, dtype=np.float64)
     ok = (rho > 1e-6) & (grho > 1e-10)

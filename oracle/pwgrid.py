@@ -7,7 +7,7 @@ Oracle (test infrastructure only).  Restates PWDFT.jl:
   PWGrid.jl:199-242        init_gvec (stable sortperm on G2)
   PWGrid.jl:245-275        init_Gshells
   PWGrid.jl:292-322        init_gvecw
-  KPoints.jl:120-262       gen_kpoint_grid (identity rotation only + time
+  KPoints.jl:121-260       gen_kpoint_grid (identity rotation only + time
                            reversal, i.e. use_symmetry=false)
   gen_lattice.jl:17-28     fcc / cubic lattice vectors (by column)
 
@@ -200,7 +200,7 @@ class PWGrid:
 
 
 def gen_kpoint_grid(LatVecs, nk, shift=(0, 0, 0), time_reversal=True):
-    """KPoints.jl:120-262 with the identity as the only rotation (no
+    """KPoints.jl:121-260 with the identity as the only rotation (no
     symmetry reduction beyond k ~ -k)."""
     nk1, nk2, nk3 = nk
     k1, k2, k3 = shift

@@ -1,9 +1,9 @@
 // The device parts of diag_CheFSI! (CheFSI.jl:1-139):
-//   pw_chebyfilt       chebyfilt (CheFSI.jl:36-67): the scaled Chebyshev filter
+//   pw_chebyfilt       chebyfilt (CheFSI.jl:34-64): the scaled Chebyshev filter
 //                      of degree m applied to a block, m op_H applications and
 //                      one fused three-term combination kernel per step;
-//   pw_lanczos_bounds  get_ub_lb_lanczos (CheFSI.jl:70-123) with
-//                      norm_matrix_induced (CheFSI.jl:127-137): nlancz Lanczos
+//   pw_lanczos_bounds  get_ub_lb_lanczos (CheFSI.jl:67-125) with
+//                      norm_matrix_induced (CheFSI.jl:128-138): nlancz Lanczos
 //                      steps with one step of full reorthogonalisation, in
 //                      FP64, the Lanczos vectors kept on the device.
 // The ortho_sqrt! and the Rayleigh quotient of diag_CheFSI! are pw_ortho_sqrt,

@@ -227,7 +227,7 @@ __global__ void k_opK(int Ngw, int nb, const double *__restrict__ Gk2, const Cx<
     }
 }
 
-// out = in / (1 + |G+k|^2)   (Kprec.jl:97-111)
+// out = in / (1 + |G+k|^2)   (Kprec.jl:30-44)
 template <typename T>
 __global__ void k_kprec(int Ngw, int nb, const double *__restrict__ Gk2, const Cx<T> *in, Cx<T> *out, int64_t ld) {
     const size_t total = (size_t)Ngw * nb;

@@ -300,7 +300,7 @@ extern "C" int pw_ortho_sqrt(pw_ctx *c, int dtype, void *psi, int64_t ld, int64_
 }
 
 // Rinv = inv(cholesky(Hermitian(C)).U) (the W / R and P / R of
-// diag_LOBPCG.jl:118-125,186-194), C read from its upper triangle and
+// diag_LOBPCG.jl:144-147,170-174,195-199), C read from its upper triangle and
 // overwritten; FP64 on the device.
 extern "C" int pw_chol_rinv(pw_ctx *c, int n, double *C, double *Rinv) {
     if (!c) return PW_ERR_ARG;

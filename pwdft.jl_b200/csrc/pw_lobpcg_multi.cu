@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) bk_rot(const BkDesc *__restrict__ ds, int
     }
 }
 
-// dst = src (ncols columns); kprec != 0: dst = src / (1 + |G+k|^2) (Kprec.jl:97-111)
+// dst = src (ncols columns); kprec != 0: dst = src / (1 + |G+k|^2) (Kprec.jl:30-44)
 template <typename C>
 __global__ void bk_copy(const BkDesc *__restrict__ ds, int nb, int ncols, BRef Src, BRef Dst, int kprec) {
     const int k = blockIdx.x;

@@ -56,12 +56,12 @@ def op_V_Ps_nloc_(Ham, psi, Hpsi):
 
 
 def Kprec_(ik, Ham, psi, Kpsi):
-    """Kprec!(ik, pw, psi, Kpsi) (Kprec.jl:97-111)."""
+    """Kprec!(ik, pw, psi, Kpsi) (Kprec.jl:30-44)."""
     Ham.ctx.kprec(ik, psi, Kpsi)
 
 
 def Kprec(ik, Ham, psi):
-    """Kprec(ik, pw, psi) (Kprec.jl:77-95)."""
+    """Kprec(ik, pw, psi) (Kprec.jl:10-28)."""
     out = _torch().empty_like(psi)
     Ham.ctx.kprec(ik, psi, out)
     return out
@@ -119,14 +119,14 @@ def diag_CheFSI_(Ham, psiks, cheby_degree, seed=1234):
 
 
 def chebyfilt(Ham, X, degree, lb, ub):
-    """chebyfilt(Ham, X, degree, lb, ub) -> Y (CheFSI.jl:36-67) at Ham.ik."""
+    """chebyfilt(Ham, X, degree, lb, ub) -> Y (CheFSI.jl:34-64) at Ham.ik."""
     Y = _torch().empty_like(X)
     Ham.ctx.chebyfilt(Ham.ik, Ham.ispin, X, Y, degree, lb, ub)
     return Y
 
 
 def get_ub_lb_lanczos(Ham, nlancz, v0=None, seed=None):
-    """get_ub_lb_lanczos(Ham, nlancz) -> (ub, lb) (CheFSI.jl:70-123) at Ham.ik;
+    """get_ub_lb_lanczos(Ham, nlancz) -> (ub, lb) (CheFSI.jl:67-125) at Ham.ik;
     v0 (complex128 device vector of Ngw) defaults to a seeded normal draw,
     where the reference calls randn."""
     import numpy as np

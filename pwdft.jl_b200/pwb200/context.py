@@ -274,7 +274,7 @@ class Context:
         return lam, S
 
     def chebyfilt(self, ik, ispin, X, Y, degree, lb, ub):
-        """chebyfilt (CheFSI.jl:36-67): Y = p(H) X, the scaled Chebyshev
+        """chebyfilt (CheFSI.jl:34-64): Y = p(H) X, the scaled Chebyshev
         filter of `degree` over [lb, ub]; X, Y distinct (nb, Ngw) device
         blocks of one dtype, X unchanged."""
         assert X.dtype == Y.dtype and X.shape == Y.shape and X.is_contiguous() and Y.is_contiguous()
@@ -284,7 +284,7 @@ class Context:
                                        C.c_void_p(Y.data_ptr()), ld, nb, int(degree), float(lb), float(ub)))
 
     def lanczos_bounds(self, ik, ispin, nlancz, v0):
-        """get_ub_lb_lanczos (CheFSI.jl:70-123) from the start vector v0 (a
+        """get_ub_lb_lanczos (CheFSI.jl:67-125) from the start vector v0 (a
         complex128 device tensor of Ngw); returns (ub, lb) in the
         reference's order."""
         import torch

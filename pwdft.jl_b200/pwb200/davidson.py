@@ -1,4 +1,4 @@
-"""The 2-block diag_davidson! (diag_davidson.jl:52-206) on the device, one
+"""The 2-block diag_davidson! (diag_davidson.jl:50-191) on the device, one
 k-point at a time, assembled from the library's block operations:
 
   H X, H R                  pw_apply

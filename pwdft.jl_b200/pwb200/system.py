@@ -260,7 +260,7 @@ ZATOMS = {"H": 1, "He": 2, "Li": 3, "C": 6, "N": 7, "O": 8, "Na": 11, "Mg": 12, 
 
 def kpoint_grid(LatVecs, mesh, time_reversal=True):
     """Gamma-centred Monkhorst-Pack grid reduced by k ~ -k only
-    (KPoints.jl:120-262 with the identity as the only rotation).
+    (KPoints.jl:121-260 with the identity as the only rotation).
     Returns Cartesian k (3, Nk) and weights summing to one."""
     n1, n2, n3 = mesh
     frac = np.array([[i / n1, j / n2, k / n3] for i in range(n1) for j in range(n2) for k in range(n3)])

@@ -1,4 +1,4 @@
-"""The 2-block diag_davidson! (diag_davidson.jl:52-206).
+"""The 2-block diag_davidson! (diag_davidson.jl:50-191).
 
 CPU: the oracle restatement converges to the exact lowest eigenvalues of
 Si fcc's dense H(Gamma); the device composition (pwb200.davidson) run on a

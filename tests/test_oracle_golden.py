@@ -10,7 +10,7 @@ Every constant below is quoted from the reference's tests or logs:
   test/test_energies.jl:19                 E_NN(Si fcc) = -8.397927400714764
   test/test_xc.jl:3-4                      VWN eps_xc / V_xc at rho = 0.1 .. 0.5 (atol 1e-5)
   test/test_gen_lattice.jl:33-35           lattice matrices
-  timing/time_diag_LOBPCG.jl:26-60         free-electron Hamiltonian known answer
+  timing/time_diag_LOBPCG.jl:5-84         free-electron Hamiltonian known answer
 """
 import numpy as np
 import pytest
@@ -65,7 +65,7 @@ def test_gvec_sphere_sorted_stably():
 
 def test_free_electron_spectrum():
     """With V = 0 and no projectors the LOBPCG eigenvalues are the sorted
-    0.5 |G+k|^2 (timing/time_diag_LOBPCG.jl:26-60)."""
+    0.5 |G+k|^2 (timing/time_diag_LOBPCG.jl:5-84)."""
     H = systems.Ham_Si_fcc(meshk=(1, 1, 1), extra_states=8)
     H.V_Total = np.zeros(H.pw.Npoints)
     H.NbetaNL = 0
