@@ -9,7 +9,7 @@ Quantum ESPRESSO's symm_base):
   copy_sym!                SymmetryInfo.jl:562-611
   SymmetryInfo(atoms)      SymmetryInfo.jl:711-784  (Nsyms, s, inv_s, ft, non_symmorphic, irt)
   symmetrize_vector!       SymmetryInfo.jl:923-966  (forces)
-  gen_kpoint_grid          KPoints.jl:121-261       with the crystal's rotations
+  gen_kpoint_grid          KPoints.jl:121-260       with the crystal's rotations
   RhoeSymmetrizer          RhoeSymmetrizer.jl:14-110  G-vector orbits
   symmetrize_rhoe!         RhoeSymmetrizer.jl:114-236
 
@@ -142,7 +142,7 @@ def symmetrize_vector(LatVecs, sym, v):
 
 
 def gen_kpoint_grid(LatVecs, nk, s, shift=(0, 0, 0), time_reversal=True):
-    """KPoints.jl:121-261: (Nkpt, xk Cartesian (3, Nkpt), wk)."""
+    """KPoints.jl:121-260: (Nkpt, xk Cartesian (3, Nkpt), wk)."""
     nk1, nk2, nk3 = nk
     k1, k2, k3 = shift
     SMALL = 1.0e-5

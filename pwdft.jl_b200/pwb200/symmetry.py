@@ -7,7 +7,7 @@ symmetry-reduced k-point mesh (host, once per geometry).
                      a fractional translation (disabled for supercells), as
                      s (3, 3, Nsyms) acting on reciprocal crystal coordinates
                      and ft (3, Nsyms); an operation maps x -> s^T x - ft
-  kpoint_grid_sym    gen_kpoint_grid (KPoints.jl:121-261) with those rotations
+  kpoint_grid_sym    gen_kpoint_grid (KPoints.jl:121-260) with those rotations
                      and k ~ -k
   symmetrizer_tables RhoeSymmetrizer (RhoeSymmetrizer.jl:14-110) flattened for
                      pw_set_symmetry: per orbit of the density sphere, the
