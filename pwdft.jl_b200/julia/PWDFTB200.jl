@@ -18,17 +18,22 @@ they make to the methods below -- more specific than PWDFT's
     diag_LOBPCG!, diag_davidson_qe!                  (whole solves on the device)
     calc_grad                                        (calc_grad.jl:1-57)
     update!                                          (PWDFT's update!, then V_loc re-uploaded)
-    calc_E_Ps_nloc, op_S!                            (the GTH methods PWDFT types on Hamiltonian{PsPot_GTH})
+    calc_E_Ps_nloc, op_S!, calc_forces_nlcc!,        (the GTH methods PWDFT types on Hamiltonian{PsPot_GTH})
+    calc_forces_scf_corr!
     calc_forces_Ps_loc!, calc_forces_Ps_nloc!        (calc_forces_Ps_loc.jl:13-72, calc_forces_Ps_nloc.jl:291-411)
+
+and the per-species GTH functions (eval_Vloc_G, eval_proj_G, ...) read
+through to the wrapped PsPot_GTH.
 
 Differentiation: `dE_dVloc` (pw_vloc_vjp) and ChainRulesCore rrules for
 `local_band_energy` (gradient in V_loc) and `ionic_energy` (gradient in the
 atomic positions, -F from the device force kernels).
 
 Written against include/pwb200.h.  Julia is not installed in the build
-image, so this file is not exercised by the test suite; the same ABI call
+image, so this file is not run by the test suite: the same ABI call
 sequences are exercised from Python (pwdft.jl_b200/pwb200 and
-tests/test_staging_gpu.py) on every run.
+tests/test_staging_gpu.py), and tests/test_julia_shim.py checks this text
+against PWDFT.jl's declared types, method names and drivers' call sites.
 """
 module PWDFTB200
 
@@ -90,9 +95,24 @@ function Base.getproperty(p::PsPot_GTH_B200, s::Symbol)
     return getproperty(getfield(p, :psp), s)
 end
 Base.propertynames(p::PsPot_GTH_B200) = (:psp, :dev, propertynames(getfield(p, :psp))...)
-# the GTH tables PWDFT dispatches on (PsPot_GTH.jl:164-189, 338-391)
+# the GTH tables PWDFT dispatches on (PsPot_GTH.jl:123-260, 338-391)
 PWDFT.eval_Vloc_G(p::PsPot_GTH_B200, args...) = PWDFT.eval_Vloc_G(p.psp, args...)
+PWDFT.eval_Vloc_G!(p::PsPot_GTH_B200, args...) = PWDFT.eval_Vloc_G!(p.psp, args...)
+PWDFT.eval_Vloc_G_short(p::PsPot_GTH_B200, args...) = PWDFT.eval_Vloc_G_short(p.psp, args...)
+PWDFT.eval_Vloc_R(p::PsPot_GTH_B200, args...) = PWDFT.eval_Vloc_R(p.psp, args...)
 PWDFT.eval_proj_G(p::PsPot_GTH_B200, args...) = PWDFT.eval_proj_G(p.psp, args...)
+PWDFT.eval_proj_R(p::PsPot_GTH_B200, args...) = PWDFT.eval_proj_R(p.psp, args...)
+PWDFT.print(io::IO, p::PsPot_GTH_B200; kw...) = PWDFT.print(io, p.psp; kw...)
+PWDFT.print(p::PsPot_GTH_B200; kw...) = PWDFT.print(p.psp; kw...)
+PWDFT.write_psp10(p::PsPot_GTH_B200; kw...) = PWDFT.write_psp10(p.psp; kw...)
+# the methods PWDFT types on Vector{PsPot_GTH} (PsPot_GTH.jl:394, calc_PspCore_ene.jl:1,
+# PsPotNL.jl:16, calc_forces_Ps_nloc.jl:347) take the wrapped GTH records
+gth(pspots::Vector{PsPot_GTH_B200}) = [p.psp for p in pspots]
+PWDFT.calc_Natomwfc(atoms::Atoms, pspots::Vector{PsPot_GTH_B200}) = PWDFT.calc_Natomwfc(atoms, gth(pspots))
+PWDFT.calc_PspCore_ene(atoms::Atoms, pspots::Vector{PsPot_GTH_B200}) = PWDFT.calc_PspCore_ene(atoms, gth(pspots))
+PWDFT.PsPotNL(atoms::Atoms, pw::PWGrid, pspots::Vector{PsPot_GTH_B200}; kw...) = PWDFT.PsPotNL(atoms, pw, gth(pspots); kw...)
+PWDFT.calc_dbetaNL(atoms::Atoms, pw::PWGrid, pspots::Vector{PsPot_GTH_B200}, args...) =
+    PWDFT.calc_dbetaNL(atoms, pw, gth(pspots), args...)
 
 const B200Hamiltonian = Hamiltonian{PsPot_GTH_B200}
 device(Ham::B200Hamiltonian) = Ham.pspots[1].dev
@@ -437,6 +457,18 @@ function PWDFT.calc_forces_Ps_nloc!(Ham::B200Hamiltonian, psiks::BlochWavefunc, 
                     c, ik - 1, PW_C128, p.ptr, size(psiks[ikspin], 1), size(psiks[ikspin], 2), w, Fk), c)
         F_Ps_nloc .+= Fk
     end
+    return
+end
+
+# GTH pseudopotentials carry no core correction: the nonlinear-core and SCF
+# correction forces are zero, as PWDFT's Hamiltonian{PsPot_GTH} methods
+# (calc_forces_nlcc.jl:20-23, calc_forces_scf_corr.jl:8-11) make them
+function PWDFT.calc_forces_nlcc!(Ham::B200Hamiltonian, F_nlcc)
+    fill!(F_nlcc, 0.0)
+    return
+end
+function PWDFT.calc_forces_scf_corr!(Ham::B200Hamiltonian, F_scf_corr)
+    fill!(F_scf_corr, 0.0)
     return
 end
 

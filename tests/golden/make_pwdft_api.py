@@ -5,6 +5,13 @@
              every struct reachable from them through field types
   functions  for each PWDFT.<name> the binding uses, and for the drivers it
              documents, whether src/ defines a function of that name
+  methods    for each function the binding adds methods to, the positional
+             parameter types of every method src/ defines for it ("Any" where
+             untyped): what the binding's invoke calls must name
+  gth_typed  the functions src/ defines with a parameter typed
+             Hamiltonian{PsPot_GTH}, PsPot_GTH or Vector{PsPot_GTH}: none of
+             them takes the binding's Hamiltonian{PsPot_GTH_B200} or its
+             species, so the binding must add a method for each
   calls      every call in src/ of a function the binding adds methods to:
              file:line, the kind of each positional argument ("bloch": a
              whole BlochWavefunc such as psiks, "block": an indexed one such
@@ -159,6 +166,42 @@ def call_sites(code, name):
     return sites
 
 
+def method_signatures(code, name):
+    """Positional parameter types of each `function name(...)` in code."""
+    sigs = []
+    for m in re.finditer(r"^\s*function\s+(?:PWDFT\.)?" + re.escape(name) + r"\s*\(", code, re.M):
+        depth, j = 1, m.end()
+        while j < len(code) and depth:
+            depth += {"(": 1, ")": -1}.get(code[j], 0)
+            j += 1
+        pos = code[m.end():j - 1].partition(";")[0]
+        types = []
+        for a in split_top(pos):
+            a = " ".join(a.split())
+            if not a:
+                continue
+            tm = re.match(r"^\w+\s*::\s*(.+?)(?:\s*=.*)?$", a)
+            types.append(tm.group(1).replace(" ", "") if tm else "Any")
+        sigs.append(types)
+    return sigs
+
+
+GTH_TYPE = re.compile(r"::\s*(?:Hamiltonian\{PsPot_GTH\}|PsPot_GTH|Vector\{PsPot_GTH\}|Array\{PsPot_GTH,\s*1\})\s*(?:[,;=]|$)")
+
+
+def gth_typed(code):
+    """Names of the functions whose parameters include a GTH-typed one."""
+    out = set()
+    for m in re.finditer(r"^\s*function\s+(?:\w+\.)?([A-Za-z_][\w!]*)\s*\(", code, re.M):
+        depth, j = 1, m.end()
+        while j < len(code) and depth:
+            depth += {"(": 1, ")": -1}.get(code[j], 0)
+            j += 1
+        if any(GTH_TYPE.search(" ".join(a.split())) for a in split_top(code[m.end():j - 1].replace(";", ","))):
+            out.add(m.group(1))
+    return out
+
+
 def arg_kind(expr):
     if "..." in expr:
         return "splat"
@@ -193,19 +236,25 @@ def main(src):
     keep = reachable(structs, ["Hamiltonian", "PsPot_GTH"])
     extended = sorted(set(re.findall(r"^(?:function\s+)?PWDFT\.([A-Za-z_][\w!]*)\(", code, re.M)))
     calls = {n: [] for n in extended}
+    methods = {n: [] for n in extended}
+    typed = set()
     for root, _, files in os.walk(src):
         for fn in sorted(files):
             if fn.endswith(".jl"):
                 with open(os.path.join(root, fn), encoding="utf-8", errors="replace") as f:
                     ref = julia_code(f.read())
                 rel = os.path.relpath(os.path.join(root, fn), os.path.dirname(src.rstrip("/")))
+                typed |= gth_typed(ref)
                 for n in extended:
+                    methods[n] += method_signatures(ref, n)
                     for line, pos, kws in call_sites(ref, n):
                         calls[n].append({"at": "%s:%d" % (rel, line), "positional": [arg_kind(a) for a in pos],
                                          "keywords": kws})
     out = {"structs": {k: structs[k] for k in sorted(keep)},
            "functions": {n: n in functions for n in used if n not in abstract},
            "abstract_types": {n: True for n in used if n in abstract},
+           "methods": methods,
+           "gth_typed": sorted(typed),
            "calls": calls}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pwdft_api.json")
     with open(dst, "w") as f:

@@ -11,6 +11,10 @@ by tests/golden/make_pwdft_api.py from the reference sources):
                field types
   names        every PWDFT.<name> the binding extends or calls, and every
                driver it documents, is defined by PWDFT.jl
+  GTH methods  every function PWDFT.jl types on Hamiltonian{PsPot_GTH},
+               PsPot_GTH or Vector{PsPot_GTH} (none accepts the binding's
+               Hamiltonian{PsPot_GTH_B200} or its species) gets a method from
+               the binding
   dispatch     every call in PWDFT.jl of a function the binding adds methods
                to, whose arguments fit one of those methods (by count and,
                where the argument shows it, whole BlochWavefunc vs one
@@ -253,3 +257,10 @@ def test_driver_calls_dispatch_with_accepted_keywords():
                  ("src/KS_solve_SCF.jl", "update!"), ("src/KS_solve_Emin_PCG.jl", "calc_grad"),
                  ("src/KS_solve_Emin_PCG.jl", "calc_rhoe!")):
         assert (f, n) in reached, (f, n)
+
+
+def test_every_gth_typed_method_is_covered():
+    api, code = load()
+    extended = set(re.findall(r"^(?:function\s+)?PWDFT\.([A-Za-z_][\w!]*)(?:\{[^}]*\})?\(", code, re.M))
+    missing = sorted(set(api["gth_typed"]) - extended)
+    assert not missing, "PWDFT methods typed on the GTH types with no method for the binding's types: %s" % missing
